@@ -1,0 +1,90 @@
+// Device-side data of one nodal-DG discretisation and the kernel interfaces.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dg_physics.cuh"
+
+namespace apollo {
+
+// Per-element geometry, 24 float64 (192 bytes), built on the host from the
+// element's vertices exactly as Apollo's GeometricFactors2d / Normals2d do
+// (src/lib/wxnodaldggeometry2d.cc:382-442).
+struct ElemGeo {
+  double rx, ry, sx, sy;  // dr/dx, dr/dy, ds/dx, ds/dy
+  double J, invJ;
+  double nx[3], ny[3], sJ[3];  // outward unit normal and half edge length per face
+  double vx[3], vy[3];         // vertices (for boundary-condition coordinates)
+  double pad[3];
+};
+
+// Face record: interior (k1, f1, k2, f2) with k1's face f1 paired to k2's face
+// f2; boundary (k, f, -tag, -1).
+struct FaceRec {
+  int k1, f1, k2, f2;
+};
+
+// Time-stepper state kept on the device so whole steps run without the host.
+struct DevState {
+  double t;          // time at the start of the current step
+  double dt;         // dt of the current step
+  double tend;       // end time (<= 0: none)
+  double pad0;
+  unsigned long long lam_bits;  // max numerical-flux speed of the current stage (bits of a double >= 0)
+  int err;           // ErrBits
+  int steps;         // steps completed
+  double last_sugg;  // suggested dt of the last right-hand side
+  double sums[8];
+};
+
+// Operators of one order, float64, row-major, built on the host.
+//   V  [NC][NP]  nodal values -> cubature points (Vand_cub * V^-1)
+//   Dr [NP][NC]  VVT * Dr_cub^T * diag(w_cub)    (VVT = V V^T, reference-element M^-1)
+//   Ds [NP][NC]  VVT * Ds_cub^T * diag(w_cub)
+//   I  [NF][NP]  nodal values -> face Gauss points, NF = 3 NG
+//   L  [NP][NF]  VVT * I^T (surface "LIFT" without the Gauss weights)
+struct DgDev {
+  int K, nfaces, N;
+  const ElemGeo* geo;
+  const FaceRec* faces;
+  const double *V, *Dr, *Ds, *I, *L, *gz, *gw;
+  double *vol, *trace, *flux;  // scratch: [K][NP][M], [K][NF][M], [K][NF][M]
+  DevState* st;
+  EqParams eqp;
+  BcTable bcs;
+  double dtfac;  // 2/3 * cfl * dtscale
+  double rmin;
+};
+
+enum StageMode : int { MODE_RHS = 0, MODE_STAGE = 1, MODE_FINAL = 2 };
+
+struct StageArgs {
+  const double* x;   // right-hand-side input
+  const double* u0;  // step start state (MODE_FINAL)
+  double* out;
+  int mode;
+  int time_from_state;  // 1: t = st->t + st->dt * frac; 0: t = t_arg
+  double frac;
+  double t_arg;
+  double dt_arg;        // dt used when time_from_state == 0
+  int reset_lambda;     // volume kernel zeroes st->lam_bits first
+};
+
+template <int N> struct Sizes {
+  static constexpr int NP = (N + 1) * (N + 2) / 2;
+  static constexpr int NG = 2 * (N + 1);
+  static constexpr int NF = 3 * NG;
+  // cubature points for cubature order 3(N+1) (src/lib/wxcubature2d.cc:26-28)
+  static constexpr int NC = N == 1 ? 12 : N == 2 ? 19 : N == 3 ? 36 : N == 4 ? 54 : N == 5 ? 73 : N == 6 ? 93 : N == 7 ? 118 : 145;
+};
+
+// Host launchers (dg_fp64.cu).
+// ev (optional): 4 events recorded before/between/after the three kernels
+cudaError_t launch_rhs_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev = nullptr);
+cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStream_t s);
+cudaError_t launch_finalize(const DgDev& d, cudaStream_t s);
+cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wJ, cudaStream_t s);
+int fp64_supported(int eq, int N);
+
+}  // namespace apollo

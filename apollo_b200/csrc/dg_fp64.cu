@@ -1,0 +1,428 @@
+// Float64 nodal-DG right-hand side on sm_100a: one volume kernel, one face
+// kernel and one LIFT kernel with the SSP stage update fused in, per stage.
+//
+//  k_volume  : per element tile, q -> cubature values (V), physical flux at
+//              every cubature point, volume contraction with the weighted
+//              derivative operators (Dr, Ds) and the face traces (I q).
+//              Apollo: wxnodaldg2dmethod.cc:346-394 with
+//              wxcubature2d.cc:290-363.
+//  k_face    : per face Gauss point, both traces through the face map (the
+//              partner in reversed Gauss order), boundary hook, Lax-Friedrichs
+//              flux, times sJ and the Gauss weight, written to both sides, and
+//              the max wave speed.  Apollo: wxnodaldg2dmethod.cc:396-469.
+//  k_lift    : per element tile, surface contraction (L = VVT I^T), 1/J,
+//              combination with the volume term and the stage update.
+//              Apollo: wxcubature2d.cc:367-382, wxnodaldggeometry2d.cc:444-456,
+//              wxnodaldg2dmethod.cc:475-504; PETSc TSSSP RK_2 update.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dg_device.cuh"
+
+namespace apollo {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int N, int M> struct VolTile {
+  static constexpr int NP = Sizes<N>::NP, NC = Sizes<N>::NC, NF = Sizes<N>::NF;
+  static constexpr int E = 8;  // elements per tile
+  static constexpr int OPS = NC * NP + 2 * NP * NC + NF * NP;
+  static constexpr int QS = E * NP * M;
+  static constexpr int RS = E * NC * 2 * M;
+  static constexpr size_t BYTES = sizeof(double) * (OPS + QS + RS);
+};
+
+template <int EQ, int N>
+__global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
+  using P = Eq<EQ>;
+  constexpr int M = P::M;
+  using T = VolTile<N, M>;
+  constexpr int NP = T::NP, NC = T::NC, NF = T::NF, E = T::E;
+  extern __shared__ double smem[];
+  double* sV = smem;
+  double* sDr = sV + NC * NP;
+  double* sDs = sDr + NP * NC;
+  double* sI = sDs + NP * NC;
+  double* sq = sI + NF * NP;
+  double* srs = sq + T::QS;
+  const int tid = threadIdx.x;
+  if (a.reset_lambda && blockIdx.x == 0 && tid == 0) d.st->lam_bits = 0ull;
+  for (int i = tid; i < NC * NP; i += kThreads) sV[i] = d.V[i];
+  for (int i = tid; i < NP * NC; i += kThreads) { sDr[i] = d.Dr[i]; sDs[i] = d.Ds[i]; }
+  for (int i = tid; i < NF * NP; i += kThreads) sI[i] = d.I[i];
+  int err = 0;
+  const int ntiles = (d.K + E - 1) / E;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int k0 = tile * E;
+    const int ne = min(E, d.K - k0);
+    __syncthreads();
+    const double* src = a.x + (size_t)k0 * NP * M;
+    for (int i = tid; i < ne * NP * M; i += kThreads) sq[i] = src[i];
+    __syncthreads();
+    // cubature values and fluxes
+    for (int idx = tid; idx < ne * NC; idx += kThreads) {
+      const int e = idx / NC, c = idx - e * NC;
+      double qc[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) qc[f] = 0.0;
+      const double* vrow = sV + c * NP;
+      const double* qe = sq + e * NP * M;
+#pragma unroll 5
+      for (int j = 0; j < NP; ++j) {
+        const double v = vrow[j];
+#pragma unroll
+        for (int f = 0; f < M; ++f) qc[f] = fma(v, qe[j * M + f], qc[f]);
+      }
+      double F[M], G[M];
+      P::flux2(d.eqp, qc, F, G, &err);
+      const ElemGeo& g = d.geo[k0 + e];
+      double* rs = srs + (e * NC + c) * 2 * M;
+#pragma unroll
+      for (int f = 0; f < M; ++f) {
+        rs[f] = g.rx * F[f] + g.ry * G[f];
+        rs[M + f] = g.sx * F[f] + g.sy * G[f];
+      }
+    }
+    // face traces
+    for (int idx = tid; idx < ne * NF; idx += kThreads) {
+      const int e = idx / NF, gp = idx - e * NF;
+      double tq[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) tq[f] = 0.0;
+      const double* irow = sI + gp * NP;
+      const double* qe = sq + e * NP * M;
+#pragma unroll 5
+      for (int j = 0; j < NP; ++j) {
+        const double v = irow[j];
+#pragma unroll
+        for (int f = 0; f < M; ++f) tq[f] = fma(v, qe[j * M + f], tq[f]);
+      }
+      double* dst = d.trace + ((size_t)(k0 + e) * NF + gp) * M;
+#pragma unroll
+      for (int f = 0; f < M; ++f) dst[f] = tq[f];
+    }
+    __syncthreads();
+    // volume contraction
+    for (int idx = tid; idx < ne * NP; idx += kThreads) {
+      const int e = idx / NP, i = idx - e * NP;
+      double acc[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) acc[f] = 0.0;
+      const double* dr = sDr + i * NC;
+      const double* ds = sDs + i * NC;
+      const double* rs = srs + e * NC * 2 * M;
+#pragma unroll 2
+      for (int c = 0; c < NC; ++c) {
+        const double a1 = dr[c], a2 = ds[c];
+#pragma unroll
+        for (int f = 0; f < M; ++f) acc[f] = fma(a1, rs[c * 2 * M + f], fma(a2, rs[c * 2 * M + M + f], acc[f]));
+      }
+      double* dst = d.vol + ((size_t)(k0 + e) * NP + i) * M;
+#pragma unroll
+      for (int f = 0; f < M; ++f) dst[f] = acc[f];
+    }
+  }
+  if (err) atomicOr(&d.st->err, err);
+}
+
+template <int EQ, int N>
+__global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
+  using P = Eq<EQ>;
+  constexpr int M = P::M;
+  constexpr int NG = Sizes<N>::NG, NF = Sizes<N>::NF;
+  const double t = a.time_from_state ? d.st->t + d.st->dt * a.frac : a.t_arg;
+  int err = 0;
+  double lmax = 0.0;
+  const int total = d.nfaces * NG;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int fi = idx / NG, gq = idx - fi * NG;
+    const FaceRec fr = d.faces[fi];
+    const ElemGeo& g = d.geo[fr.k1];
+    const double nx = g.nx[fr.f1], ny = g.ny[fr.f1], sJ = g.sJ[fr.f1];
+    double qM[M], qP[M], nf[M];
+    const double* tm = d.trace + ((size_t)fr.k1 * NF + fr.f1 * NG + gq) * M;
+#pragma unroll
+    for (int f = 0; f < M; ++f) qM[f] = tm[f];
+    if (fr.k2 >= 0) {
+      const double* tp = d.trace + ((size_t)fr.k2 * NF + fr.f2 * NG + (NG - 1 - gq)) * M;
+#pragma unroll
+      for (int f = 0; f < M; ++f) qP[f] = tp[f];
+    } else {
+      // Gauss point coordinates on face f1: the affine map of the face
+      // parametrisation (wxcubature2d.cc:118-124)
+      const double z = d.gz[gq];
+      double r, s;
+      if (fr.f1 == 0) { r = z; s = -1.0; }
+      else if (fr.f1 == 1) { r = -z; s = z; }
+      else { r = -1.0; s = -z; }
+      const double x = 0.5 * (-g.vx[0] * (r + s) + g.vx[1] * (1. + r) + g.vx[2] * (1. + s));
+      const double y = 0.5 * (-g.vy[0] * (r + s) + g.vy[1] * (1. + r) + g.vy[2] * (1. + s));
+      apply_bc<EQ, double>(d.bcs, -fr.k2, t, x, y, nx, ny, qM, qP);
+    }
+    double lam = P::numflux(d.eqp, nx, ny, qM, qP, nf, &err);
+    lam = fabs(lam);
+    lmax = lam > lmax ? lam : lmax;
+    const double w = d.gw[gq] * sJ;
+    double* om = d.flux + ((size_t)fr.k1 * NF + fr.f1 * NG + gq) * M;
+#pragma unroll
+    for (int f = 0; f < M; ++f) om[f] = nf[f] * w;
+    if (fr.k2 >= 0) {
+      double* op = d.flux + ((size_t)fr.k2 * NF + fr.f2 * NG + (NG - 1 - gq)) * M;
+#pragma unroll
+      for (int f = 0; f < M; ++f) op[f] = -(nf[f] * w);
+    }
+  }
+  // block max of the wave speed, one atomic per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double v = __shfl_xor_sync(0xffffffffu, lmax, o);
+    lmax = v > lmax ? v : lmax;
+  }
+  if ((threadIdx.x & 31) == 0 && lmax > 0.0) atomic_max_nonneg(&d.st->lam_bits, lmax);
+  if (err) atomicOr(&d.st->err, err);
+}
+
+template <int N, int M> struct LiftTile {
+  static constexpr int NP = Sizes<N>::NP, NF = Sizes<N>::NF;
+  static constexpr int E = 8;
+  static constexpr size_t BYTES = sizeof(double) * (NP * NF + E * NF * M);
+};
+
+template <int EQ, int N>
+__global__ void __launch_bounds__(kThreads) k_lift(DgDev d, StageArgs a) {
+  constexpr int M = Eq<EQ>::M;
+  using T = LiftTile<N, M>;
+  constexpr int NP = T::NP, NF = T::NF, E = T::E;
+  extern __shared__ double smem[];
+  double* sL = smem;
+  double* sf = sL + NP * NF;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < NP * NF; i += kThreads) sL[i] = d.L[i];
+  const double dt = a.time_from_state ? d.st->dt : a.dt_arg;
+  const double c_stage = dt / 4.0;  // dt/(s-1), s = 5
+  const double c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
+  int err = 0;
+  const int ntiles = (d.K + E - 1) / E;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int k0 = tile * E;
+    const int ne = min(E, d.K - k0);
+    __syncthreads();
+    const double* src = d.flux + (size_t)k0 * NF * M;
+    for (int i = tid; i < ne * NF * M; i += kThreads) sf[i] = src[i];
+    __syncthreads();
+    for (int idx = tid; idx < ne * NP; idx += kThreads) {
+      const int e = idx / NP, i = idx - e * NP;
+      const int k = k0 + e;
+      double acc[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) acc[f] = 0.0;
+      const double* lrow = sL + i * NF;
+      const double* fe = sf + e * NF * M;
+#pragma unroll 4
+      for (int gp = 0; gp < NF; ++gp) {
+        const double l = lrow[gp];
+#pragma unroll
+        for (int f = 0; f < M; ++f) acc[f] = fma(l, fe[gp * M + f], acc[f]);
+      }
+      const double invJ = d.geo[k].invJ;
+      const size_t off = ((size_t)k * NP + i) * M;
+#pragma unroll
+      for (int f = 0; f < M; ++f) {
+        const double r = d.vol[off + f] - invJ * acc[f];
+        if (r != r) err |= ERRB_NAN;
+        double o;
+        if (a.mode == MODE_RHS) o = r;
+        else if (a.mode == MODE_STAGE) o = a.x[off + f] + c_stage * r;
+        else o = c_al * a.x[off + f] + c_be * r + c_ga * a.u0[off + f];
+        a.out[off + f] = o;
+      }
+    }
+  }
+  if (err) atomicOr(&d.st->err, err);
+}
+
+template <int EQ>
+__global__ void k_init_speed(DgDev d, const double* u, int nnodes) {
+  constexpr int M = Eq<EQ>::M;
+  double lmax = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnodes; i += gridDim.x * blockDim.x) {
+    double q[M];
+#pragma unroll
+    for (int f = 0; f < M; ++f) q[f] = u[(size_t)i * M + f];
+    double s2 = Eq<EQ>::speed2(d.eqp, q);
+    double lam = sqrt(s2 > 0.0 ? s2 : 0.0);
+    lmax = lam > lmax ? lam : lmax;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double v = __shfl_xor_sync(0xffffffffu, lmax, o);
+    lmax = v > lmax ? v : lmax;
+  }
+  if ((threadIdx.x & 31) == 0 && lmax > 0.0) atomic_max_nonneg(&d.st->lam_bits, lmax);
+}
+
+// After a step: t += dt; dt = min(dt, suggestion of the last stage), clipped
+// to the end time (ApSolver::ComputeRHSforTS + MonitorVTK,
+// src/solvers/apsolver.cc:421-480).
+__global__ void k_finalize(DgDev d) {
+  DevState* st = d.st;
+  const double lam = __longlong_as_double((long long)st->lam_bits);
+  const double sugg = d.dtfac * (d.rmin / lam);
+  st->last_sugg = sugg;
+  const double dt = st->dt;
+  const double t = st->t + dt;
+  double nd = fmin(sugg, dt);
+  if (st->tend > 0.0 && fabs(st->tend - t) < nd) nd = fabs(st->tend - t);
+  st->t = t;
+  st->dt = nd;
+  st->steps += 1;
+}
+
+template <int EQ>
+__global__ void k_integrals(DgDev d, const double* u, const double* wmass, int NP) {
+  constexpr int M = Eq<EQ>::M;
+  double acc[M];
+#pragma unroll
+  for (int f = 0; f < M; ++f) acc[f] = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < d.K; k += gridDim.x * blockDim.x) {
+    const double J = d.geo[k].J;
+    for (int j = 0; j < NP; ++j) {
+      const double w = wmass[j] * J;
+#pragma unroll
+      for (int f = 0; f < M; ++f) acc[f] += w * u[((size_t)k * NP + j) * M + f];
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < M; ++f) {
+    double v = acc[f];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&d.st->sums[f], v);
+  }
+}
+
+int g_num_sms = 0;
+int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+template <int EQ, int N>
+cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+  constexpr int M = Eq<EQ>::M;
+  using VT = VolTile<N, M>;
+  using LT = LiftTile<N, M>;
+  static unsigned configured = 0;  // bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured & (1u << (dev & 31)))) {
+    cudaError_t e = cudaFuncSetAttribute(k_volume<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VT::BYTES);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_lift<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LT::BYTES);
+    if (e != cudaSuccess) return e;
+    configured |= 1u << (dev & 31);
+  }
+  const int sms = num_sms();
+  const int vt = (d.K + VT::E - 1) / VT::E;
+  int per_sm = (int)((200 * 1024) / VT::BYTES);
+  if (per_sm < 1) per_sm = 1;
+  if (per_sm > 8) per_sm = 8;
+  int gv = sms * per_sm;
+  if (gv > vt) gv = vt;
+  if (ev) cudaEventRecord(ev[0], s);
+  k_volume<EQ, N><<<gv, kThreads, VT::BYTES, s>>>(d, a);
+  if (ev) cudaEventRecord(ev[1], s);
+  const int fthreads = d.nfaces * Sizes<N>::NG;
+  int gf = (fthreads + kThreads - 1) / kThreads;
+  if (gf > sms * 8) gf = sms * 8;
+  if (gf < 1) gf = 1;
+  k_face<EQ, N><<<gf, kThreads, 0, s>>>(d, a);
+  if (ev) cudaEventRecord(ev[2], s);
+  const int lt = (d.K + LT::E - 1) / LT::E;
+  int lper = (int)((200 * 1024) / LT::BYTES);
+  if (lper < 1) lper = 1;
+  if (lper > 8) lper = 8;
+  int gl = sms * lper;
+  if (gl > lt) gl = lt;
+  k_lift<EQ, N><<<gl, kThreads, LT::BYTES, s>>>(d, a);
+  if (ev) cudaEventRecord(ev[3], s);
+  return cudaGetLastError();
+}
+
+template <int EQ>
+cudaError_t dispatch_n(const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+  switch (d.N) {
+    case 2: return launch_rhs_t<EQ, 2>(d, a, s, ev);
+    case 3: return launch_rhs_t<EQ, 3>(d, a, s, ev);
+    case 4: return launch_rhs_t<EQ, 4>(d, a, s, ev);
+    case 5: return launch_rhs_t<EQ, 5>(d, a, s, ev);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+int fp64_supported(int eq, int N) { return eq >= 0 && eq <= 4 && N >= 2 && N <= 5; }
+
+cudaError_t launch_rhs_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+  switch (eq) {
+    case EQ_ADVECTION: return dispatch_n<EQ_ADVECTION>(d, a, s, ev);
+    case EQ_EULER: return dispatch_n<EQ_EULER>(d, a, s, ev);
+    case EQ_MAXWELL: return dispatch_n<EQ_MAXWELL>(d, a, s, ev);
+    case EQ_EULER2D: return dispatch_n<EQ_EULER2D>(d, a, s, ev);
+    case EQ_MAXWELL_TM: return dispatch_n<EQ_MAXWELL_TM>(d, a, s, ev);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStream_t s) {
+  const int np = (d.N + 1) * (d.N + 2) / 2;
+  const int nn = d.K * np;
+  int g = (nn + 255) / 256;
+  if (g > num_sms() * 8) g = num_sms() * 8;
+  if (g < 1) g = 1;
+  switch (eq) {
+    case EQ_ADVECTION: k_init_speed<EQ_ADVECTION><<<g, 256, 0, s>>>(d, u, nn); break;
+    case EQ_EULER: k_init_speed<EQ_EULER><<<g, 256, 0, s>>>(d, u, nn); break;
+    case EQ_MAXWELL: k_init_speed<EQ_MAXWELL><<<g, 256, 0, s>>>(d, u, nn); break;
+    case EQ_EULER2D: k_init_speed<EQ_EULER2D><<<g, 256, 0, s>>>(d, u, nn); break;
+    case EQ_MAXWELL_TM: k_init_speed<EQ_MAXWELL_TM><<<g, 256, 0, s>>>(d, u, nn); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const DgDev& d, cudaStream_t s) {
+  k_finalize<<<1, 1, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wmass, cudaStream_t s) {
+  const int np = (d.N + 1) * (d.N + 2) / 2;
+  int g = (d.K + 255) / 256;
+  if (g > num_sms() * 4) g = num_sms() * 4;
+  if (g < 1) g = 1;
+  switch (eq) {
+    case EQ_ADVECTION: k_integrals<EQ_ADVECTION><<<g, 256, 0, s>>>(d, u, wmass, np); break;
+    case EQ_EULER: k_integrals<EQ_EULER><<<g, 256, 0, s>>>(d, u, wmass, np); break;
+    case EQ_MAXWELL: k_integrals<EQ_MAXWELL><<<g, 256, 0, s>>>(d, u, wmass, np); break;
+    case EQ_EULER2D: k_integrals<EQ_EULER2D><<<g, 256, 0, s>>>(d, u, wmass, np); break;
+    case EQ_MAXWELL_TM: k_integrals<EQ_MAXWELL_TM><<<g, 256, 0, s>>>(d, u, wmass, np); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace apollo

@@ -1,0 +1,601 @@
+// C ABI of the nodal-DG solver: setup (operators, geometry, face map), device
+// buffers, the right-hand side and the SSPRK(5,2) stepper with Apollo's dt
+// policy.  See include/apollo_dg.h for the contract of each entry point.
+#include "apollo_dg.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "dg_device.cuh"
+#include "dg_mixed.h"
+#include "dg_operators.h"
+
+using namespace apollo;
+
+struct apollo_dg {
+  apollo_dg_config cfg{};
+  std::string err;
+  int eq = -1;
+  EqParams eqp{};
+  BcTable bcs{};
+  RefOps ops;
+  int K = 0, M = 0;
+  double dtscale = 0.0;
+  std::vector<ElemGeo> geo_h;
+  std::vector<FaceRec> faces_h;
+  std::vector<double> xn, yn;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // device memory
+  ElemGeo* geo_d = nullptr;
+  FaceRec* faces_d = nullptr;
+  double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
+         *gw_d = nullptr, *wmass_d = nullptr;
+  double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
+  double *vol_d = nullptr, *trace_d = nullptr, *flux_d = nullptr;
+  DevState* st_d = nullptr;
+  DevState* st_h = nullptr;  // pinned
+  bool have_state = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  MixedPlan* mixed = nullptr;
+};
+
+namespace {
+
+apollo_status fail(apollo_dg* h, apollo_status code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+apollo_status cuda_fail(apollo_dg* h, cudaError_t e, const char* where) {
+  return fail(h, APOLLO_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, where)                          \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
+  } while (0)
+
+int fields_of(int eq) {
+  switch (eq) {
+    case EQ_ADVECTION: return 1;
+    case EQ_EULER: return 5;
+    case EQ_MAXWELL: return 8;
+    case EQ_EULER2D: return 4;
+    case EQ_MAXWELL_TM: return 3;
+  }
+  return 0;
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void free_mesh(apollo_dg* h) {
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  dfree(h->geo_d); dfree(h->faces_d);
+  dfree(h->V_d); dfree(h->Dr_d); dfree(h->Ds_d); dfree(h->I_d); dfree(h->L_d); dfree(h->gz_d); dfree(h->gw_d);
+  dfree(h->wmass_d);
+  dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
+  dfree(h->vol_d); dfree(h->trace_d); dfree(h->flux_d);
+  if (h->mixed) { mixed_destroy(h->mixed); h->mixed = nullptr; }
+  h->have_state = false;
+}
+
+template <class T>
+cudaError_t upload(T** dst, const T* src, size_t n) {
+  cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+DgDev make_dev(const apollo_dg* h) {
+  DgDev d{};
+  d.K = h->K;
+  d.nfaces = (int)h->faces_h.size();
+  d.N = h->ops.N;
+  d.geo = h->geo_d;
+  d.faces = h->faces_d;
+  d.V = h->V_d; d.Dr = h->Dr_d; d.Ds = h->Ds_d; d.I = h->I_d; d.L = h->L_d; d.gz = h->gz_d; d.gw = h->gw_d;
+  d.vol = h->vol_d; d.trace = h->trace_d; d.flux = h->flux_d;
+  d.st = h->st_d;
+  d.eqp = h->eqp;
+  d.bcs = h->bcs;
+  d.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
+  d.rmin = h->ops.rmin;
+  return d;
+}
+
+apollo_status check_ready(apollo_dg* h) {
+  if (!h) return APOLLO_ERR_ARG;
+  if (h->eq < 0) return fail(h, APOLLO_ERR_STATE, "no equation set");
+  if (h->K == 0) return fail(h, APOLLO_ERR_STATE, "no mesh set");
+  return APOLLO_OK;
+}
+
+apollo_status read_errors(apollo_dg* h) {
+  if (h->st_h->err & ERRB_NONPHYS) return fail(h, APOLLO_ERR_NONPHYSICAL, "negative density or pressure in the Euler flux");
+  if (h->st_h->err & ERRB_NAN) return fail(h, APOLLO_ERR_NAN, "NaN in the right-hand side");
+  if (h->st_h->err & ERRB_TIMEOUT) return fail(h, APOLLO_ERR_TIMEOUT, "device wait timed out");
+  return APOLLO_OK;
+}
+
+// One right-hand side or stage into the handle's stream.
+apollo_status enqueue_stage(apollo_dg* h, const StageArgs& a, apollo_precision prec, cudaEvent_t* ev = nullptr) {
+  DgDev d = make_dev(h);
+  cudaError_t e;
+  if (prec == APOLLO_PREC_MIXED) {
+    if (!h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision is not available for this equation/order");
+    e = mixed_launch_rhs(h->mixed, h->eq, d, a, h->stream, ev);
+  } else {
+    e = launch_rhs_fp64(h->eq, d, a, h->stream, ev);
+  }
+  if (e != cudaSuccess) return cuda_fail(h, e, "rhs launch");
+  return APOLLO_OK;
+}
+
+apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
+  const int s = 5;
+  for (int i = 0; i < s; ++i) {
+    StageArgs a{};
+    a.time_from_state = 1;
+    a.reset_lambda = 1;
+    if (i < s - 1) {
+      a.x = i == 0 ? h->U_d : h->W_d;
+      a.out = h->W_d;
+      a.mode = MODE_STAGE;
+      a.frac = i / (s - 1.);
+    } else {
+      a.x = h->W_d;
+      a.u0 = h->U_d;
+      a.out = h->U_d;
+      a.mode = MODE_FINAL;
+      a.frac = 1.0;
+    }
+    apollo_status r = enqueue_stage(h, a, prec);
+    if (r != APOLLO_OK) return r;
+  }
+  DgDev d = make_dev(h);
+  cudaError_t e = launch_finalize(d, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "finalize launch");
+  return APOLLO_OK;
+}
+
+apollo_status step_graph(apollo_dg* h, apollo_precision prec, cudaGraphExec_t* out) {
+  int gi = prec == APOLLO_PREC_MIXED ? 1 : 0;
+  if (!h->graph[gi]) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    apollo_status r = enqueue_step(h, prec);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (r != APOLLO_OK) { if (g) cudaGraphDestroy(g); return r; }
+    if (e != cudaSuccess) return cuda_fail(h, e, "end capture");
+    e = cudaGraphInstantiate(&h->graph[gi], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "graph instantiate");
+  }
+  *out = h->graph[gi];
+  return APOLLO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+apollo_status apollo_dg_create(const apollo_dg_config* cfg, apollo_dg** out) {
+  if (!cfg || !out) return APOLLO_ERR_ARG;
+  *out = nullptr;
+  if (cfg->polynomial_order < 2 || cfg->polynomial_order > 5) return APOLLO_ERR_CONFIG;
+  if (!(cfg->cfl > 0.0)) return APOLLO_ERR_CONFIG;
+  apollo_dg* h = new apollo_dg();
+  h->cfg = *cfg;
+  if (cudaSetDevice(cfg->device) != cudaSuccess) { delete h; return APOLLO_ERR_CUDA; }
+  if (!build_ref_ops(cfg->polynomial_order, h->ops)) { delete h; return APOLLO_ERR_CONFIG; }
+  if (cfg->stream) {
+    h->stream = (cudaStream_t)cfg->stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return APOLLO_ERR_CUDA; }
+    h->own_stream = true;
+  }
+  if (cudaMalloc((void**)&h->st_d, sizeof(DevState)) != cudaSuccess ||
+      cudaMallocHost((void**)&h->st_h, sizeof(DevState)) != cudaSuccess) {
+    apollo_dg_destroy(h);
+    return APOLLO_ERR_ALLOC;
+  }
+  std::memset(h->st_h, 0, sizeof(DevState));
+  cudaMemcpy(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice);
+  *out = h;
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const double* params, int nparams) {
+  if (!h || !kind) return APOLLO_ERR_ARG;
+  if (h->K) return fail(h, APOLLO_ERR_STATE, "set the equation before the mesh");
+  std::string k(kind);
+  int eq = -1;
+  if (k == "advectionEqn") eq = EQ_ADVECTION;
+  else if (k == "eulerEqn") eq = EQ_EULER;
+  else if (k == "phMaxwellEqn") eq = EQ_MAXWELL;
+  else if (k == "eulerEqn2d") eq = EQ_EULER2D;
+  else if (k == "maxwellTM") eq = EQ_MAXWELL_TM;
+  else return fail(h, APOLLO_ERR_CONFIG, "unknown equation kind " + k);
+  if (nparams < 0 || nparams > 4 || (nparams > 0 && !params)) return fail(h, APOLLO_ERR_ARG, "bad parameter list");
+  EqParams p{};
+  for (int i = 0; i < nparams; ++i) p.p[i] = params[i];
+  if ((eq == EQ_EULER || eq == EQ_EULER2D) && !(p.p[0] > 1.0))
+    return fail(h, APOLLO_ERR_CONFIG, "eulerEqn needs gas_gamma > 1");
+  if ((eq == EQ_MAXWELL || eq == EQ_MAXWELL_TM) && !(p.p[0] > 0.0))
+    return fail(h, APOLLO_ERR_CONFIG, "Maxwell needs c0 > 0");
+  if (eq == EQ_MAXWELL_TM && (p.p[1] != 0.0 || p.p[2] != 0.0))
+    return fail(h, APOLLO_ERR_CONFIG, "maxwellTM requires gamma = chi = 0");
+  h->eq = eq;
+  h->eqp = p;
+  h->M = fields_of(eq);
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_add_bc(apollo_dg* h, const char* kind, const double* params, int nparams) {
+  if (!h || !kind) return APOLLO_ERR_ARG;
+  if (h->bcs.n >= kMaxBc) return fail(h, APOLLO_ERR_CONFIG, "too many boundary conditions");
+  if (nparams < 0 || nparams > 8 || (nparams > 0 && !params)) return fail(h, APOLLO_ERR_ARG, "bad parameter list");
+  std::string k(kind);
+  int b = -1;
+  if (k == "gridFixedBC") b = BC_FIXED;
+  else if (k == "isentropicVortexBC") b = BC_VORTEX;
+  else if (k == "maxwellTransverseMagneticBC") b = BC_TM;
+  else if (k == "phmConductingWallBC") b = BC_PEC;
+  else return fail(h, APOLLO_ERR_CONFIG, "unknown boundary condition kind " + k);
+  int i = h->bcs.n++;
+  h->bcs.kind[i] = b;
+  for (int j = 0; j < 8; ++j) h->bcs.p[i][j] = j < nparams ? params[j] : 0.0;
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, const double* vy, int K,
+                                 const int* etov, const int* face_tag, const int* vert_canon) {
+  if (!h || !vx || !vy || !etov || nverts < 3 || K < 1) return APOLLO_ERR_ARG;
+  if (h->eq < 0) return fail(h, APOLLO_ERR_STATE, "set the equation before the mesh");
+  CK(cudaSetDevice(h->cfg.device), "set device");
+  free_mesh(h);
+  const RefOps& o = h->ops;
+  const int Np = o.Np, M = h->M;
+  h->K = 0;
+  h->geo_h.assign(K, ElemGeo{});
+  h->xn.assign((size_t)K * Np, 0.0);
+  h->yn.assign((size_t)K * Np, 0.0);
+  double dtscale = 1.0e6;
+  for (int k = 0; k < K; ++k) {
+    int v[3] = {etov[3 * k], etov[3 * k + 1], etov[3 * k + 2]};
+    for (int j = 0; j < 3; ++j)
+      if (v[j] < 0 || v[j] >= nverts) return fail(h, APOLLO_ERR_MESH, "vertex index out of range");
+    const double p1x = vx[v[0]], p1y = vy[v[0]], p2x = vx[v[1]], p2y = vy[v[1]], p3x = vx[v[2]], p3y = vy[v[2]];
+    for (int n = 0; n < Np; ++n) {
+      const double r = o.r[n], s = o.s[n];
+      h->xn[(size_t)k * Np + n] = 0.5 * (-p1x * (r + s) + p2x * (1. + r) + p3x * (1. + s));
+      h->yn[(size_t)k * Np + n] = 0.5 * (-p1y * (r + s) + p2y * (1. + r) + p3y * (1. + s));
+    }
+    // inscribed radius, Apollo CalculateNodeCoordinates2d (wxnodaldggeometry2d.cc:220-227)
+    const double l1 = std::sqrt(std::pow(p1x - p2x, 2) + std::pow(p1y - p2y, 2));
+    const double l2 = std::sqrt(std::pow(p2x - p3x, 2) + std::pow(p2y - p3y, 2));
+    const double l3 = std::sqrt(std::pow(p3x - p1x, 2) + std::pow(p3y - p1y, 2));
+    const double sp = 0.5 * (l1 + l2 + l3);
+    const double area = std::sqrt(std::fabs(sp * (sp - l1) * (sp - l2) * (sp - l3)));
+    dtscale = std::min(dtscale, area / sp);
+    // GeometricFactors2d and Normals2d from the vertex nodes (:382-442)
+    const double x1 = h->xn[(size_t)k * Np + o.fmask[0]], y1 = h->yn[(size_t)k * Np + o.fmask[0]];
+    const double x2 = h->xn[(size_t)k * Np + o.fmask[o.N + 1]], y2 = h->yn[(size_t)k * Np + o.fmask[o.N + 1]];
+    const double x3 = h->xn[(size_t)k * Np + o.fmask[2 * (o.N + 1)]], y3 = h->yn[(size_t)k * Np + o.fmask[2 * (o.N + 1)]];
+    const double dxdr = (x2 - x1) / 2, dxds = (x3 - x1) / 2, dydr = (y2 - y1) / 2, dyds = (y3 - y1) / 2;
+    const double J = -dxds * dydr + dxdr * dyds;
+    if (!(J > 0)) return fail(h, APOLLO_ERR_MESH, "non-positive Jacobian in element " + std::to_string(k));
+    ElemGeo& g = h->geo_h[k];
+    g.rx = dyds / J; g.sx = -dydr / J; g.ry = -dxds / J; g.sy = dxdr / J;
+    g.J = J; g.invJ = 1.0 / J;
+    double nr[3][2] = {{(y2 - y1), -(x2 - x1)}, {(y3 - y2), -(x3 - x2)}, {(y1 - y3), -(x1 - x3)}};
+    for (int f = 0; f < 3; ++f) {
+      const double sJ = std::sqrt(nr[f][0] * nr[f][0] + nr[f][1] * nr[f][1]);
+      if (!(sJ > 0)) return fail(h, APOLLO_ERR_MESH, "zero edge length in element " + std::to_string(k));
+      g.nx[f] = nr[f][0] / sJ;
+      g.ny[f] = nr[f][1] / sJ;
+      g.sJ[f] = sJ / 2.;
+    }
+    g.vx[0] = p1x; g.vx[1] = p2x; g.vx[2] = p3x;
+    g.vy[0] = p1y; g.vy[1] = p2y; g.vy[2] = p3y;
+  }
+  h->dtscale = dtscale;
+  // face map: faces sharing both (canonical) vertices pair up
+  static const int vn[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+  std::unordered_map<unsigned long long, int> open;
+  open.reserve((size_t)K * 2);
+  std::vector<int> partner((size_t)K * 3, -1);
+  for (int k = 0; k < K; ++k)
+    for (int f = 0; f < 3; ++f) {
+      const int tag = face_tag ? face_tag[3 * k + f] : 0;
+      if (tag < 0) return fail(h, APOLLO_ERR_MESH, "negative face tag");
+      if (tag > 0) continue;
+      int a = etov[3 * k + vn[f][0]], b = etov[3 * k + vn[f][1]];
+      if (vert_canon) { a = vert_canon[a]; b = vert_canon[b]; }
+      if (a == b) return fail(h, APOLLO_ERR_MESH, "degenerate face");
+      const unsigned long long key = ((unsigned long long)(unsigned)std::min(a, b) << 32) | (unsigned)std::max(a, b);
+      auto it = open.find(key);
+      if (it == open.end()) {
+        open.emplace(key, 3 * k + f);
+      } else {
+        const int kf = it->second;
+        if (kf < 0) return fail(h, APOLLO_ERR_MESH, "face shared by more than two elements");
+        partner[3 * k + f] = kf;
+        partner[kf] = 3 * k + f;
+        it->second = -1;
+      }
+    }
+  h->faces_h.clear();
+  h->faces_h.reserve((size_t)K * 2);
+  for (int k = 0; k < K; ++k)
+    for (int f = 0; f < 3; ++f) {
+      const int tag = face_tag ? face_tag[3 * k + f] : 0;
+      const int p = partner[3 * k + f];
+      if (tag > 0 || p < 0) {
+        const int t = tag > 0 ? tag : 1;
+        if (t > std::max(1, h->bcs.n)) return fail(h, APOLLO_ERR_MESH, "face tag without a boundary condition");
+        if (h->bcs.n == 0) return fail(h, APOLLO_ERR_MESH, "boundary face but no boundary condition added");
+        h->faces_h.push_back(FaceRec{k, f, -t, -1});
+      } else if (p > 3 * k + f) {
+        h->faces_h.push_back(FaceRec{k, f, p / 3, p % 3});
+      }
+    }
+  // device buffers
+  const size_t nU = (size_t)K * Np * M, nT = (size_t)K * o.Nf * M;
+  CK(upload(&h->geo_d, h->geo_h.data(), h->geo_h.size()), "geometry upload");
+  CK(upload(&h->faces_d, h->faces_h.data(), h->faces_h.size()), "face map upload");
+  std::vector<double> DrW(o.DrW.a), DsW(o.DsW.a);
+  CK(upload(&h->V_d, o.Vc.a.data(), o.Vc.a.size()), "op upload");
+  CK(upload(&h->Dr_d, DrW.data(), DrW.size()), "op upload");
+  CK(upload(&h->Ds_d, DsW.data(), DsW.size()), "op upload");
+  CK(upload(&h->I_d, o.Interp.a.data(), o.Interp.a.size()), "op upload");
+  CK(upload(&h->L_d, o.Lift.a.data(), o.Lift.a.size()), "op upload");
+  CK(upload(&h->gz_d, o.gz.data(), o.gz.size()), "op upload");
+  CK(upload(&h->gw_d, o.gw.data(), o.gw.size()), "op upload");
+  CK(upload(&h->wmass_d, o.mass_colsum.data(), o.mass_colsum.size()), "op upload");
+  CK(cudaMalloc((void**)&h->U_d, nU * sizeof(double)), "state alloc");
+  CK(cudaMalloc((void**)&h->W_d, nU * sizeof(double)), "state alloc");
+  CK(cudaMalloc((void**)&h->in_d, nU * sizeof(double)), "state alloc");
+  CK(cudaMalloc((void**)&h->out_d, nU * sizeof(double)), "state alloc");
+  CK(cudaMalloc((void**)&h->vol_d, nU * sizeof(double)), "scratch alloc");
+  CK(cudaMalloc((void**)&h->trace_d, nT * sizeof(double)), "scratch alloc");
+  CK(cudaMalloc((void**)&h->flux_d, nT * sizeof(double)), "scratch alloc");
+  CK(cudaMemset(h->U_d, 0, nU * sizeof(double)), "state clear");
+  h->K = K;
+  h->mixed = mixed_create(h->eq, o, K, h->M);
+  return APOLLO_OK;
+}
+
+int apollo_dg_num_fields(const apollo_dg* h) { return h ? h->M : 0; }
+int apollo_dg_num_nodes(const apollo_dg* h) { return h ? h->ops.Np : 0; }
+int apollo_dg_num_elements(const apollo_dg* h) { return h ? h->K : 0; }
+int apollo_dg_num_cubature(const apollo_dg* h) { return h ? h->ops.Nc : 0; }
+int apollo_dg_num_gauss(const apollo_dg* h) { return h ? h->ops.Ng : 0; }
+
+apollo_status apollo_dg_node_coords(apollo_dg* h, double* x, double* y) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!x || !y) return APOLLO_ERR_ARG;
+  std::memcpy(x, h->xn.data(), h->xn.size() * sizeof(double));
+  std::memcpy(y, h->yn.data(), h->yn.size() * sizeof(double));
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_set_state(apollo_dg* h, const double* U, int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!U) return APOLLO_ERR_ARG;
+  const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
+  CK(cudaMemcpyAsync(h->U_d, U, n, where == APOLLO_DEVICE_PTR ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     h->stream), "set state");
+  CK(cudaStreamSynchronize(h->stream), "set state");
+  h->have_state = true;
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_get_state(apollo_dg* h, double* U, int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!U) return APOLLO_ERR_ARG;
+  const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
+  CK(cudaMemcpyAsync(U, h->U_d, n, where == APOLLO_DEVICE_PTR ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     h->stream), "get state");
+  CK(cudaStreamSynchronize(h->stream), "get state");
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_init_dt(apollo_dg* h, double* dt) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!dt) return APOLLO_ERR_ARG;
+  if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  CK(cudaMemsetAsync(&h->st_d->lam_bits, 0, sizeof(unsigned long long), h->stream), "init dt");
+  DgDev d = make_dev(h);
+  CK(launch_init_speed(h->eq, d, h->U_d, h->stream), "init dt");
+  CK(cudaMemcpyAsync(h->st_h, h->st_d, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream), "init dt");
+  CK(cudaStreamSynchronize(h->stream), "init dt");
+  double lam;
+  std::memcpy(&lam, &h->st_h->lam_bits, sizeof(double));
+  *dt = 2. / 3. * h->cfg.cfl * h->dtscale * (h->ops.rmin / lam);
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_rhs(apollo_dg* h, double t, double dt, const double* in, double* out, double* suggested_dt,
+                            int where, apollo_precision prec) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!in || !out) return APOLLO_ERR_ARG;
+  const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
+  const double* x = in;
+  double* o = out;
+  if (where != APOLLO_DEVICE_PTR) {
+    CK(cudaMemcpyAsync(h->in_d, in, n, cudaMemcpyHostToDevice, h->stream), "rhs input copy");
+    x = h->in_d;
+    o = h->out_d;
+  }
+  CK(cudaMemsetAsync(&h->st_d->err, 0, sizeof(int), h->stream), "rhs");
+  StageArgs a{};
+  a.x = x;
+  a.out = o;
+  a.mode = MODE_RHS;
+  a.time_from_state = 0;
+  a.t_arg = t;
+  a.dt_arg = dt;
+  a.reset_lambda = 1;
+  r = enqueue_stage(h, a, prec);
+  if (r) return r;
+  if (where != APOLLO_DEVICE_PTR) CK(cudaMemcpyAsync(out, h->out_d, n, cudaMemcpyDeviceToHost, h->stream), "rhs output copy");
+  CK(cudaMemcpyAsync(h->st_h, h->st_d, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream), "rhs");
+  CK(cudaStreamSynchronize(h->stream), "rhs");
+  if (suggested_dt) {
+    double lam;
+    std::memcpy(&lam, &h->st_h->lam_bits, sizeof(double));
+    *suggested_dt = 2. / 3. * h->cfg.cfl * h->dtscale * (h->ops.rmin / lam);
+  }
+  return read_errors(h);
+}
+
+apollo_status apollo_dg_step_async(apollo_dg* h, int nsteps, double t, double dt, apollo_precision prec) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (nsteps < 0) return APOLLO_ERR_ARG;
+  if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  DevState s{};
+  s.t = t;
+  s.dt = dt;
+  s.tend = 0.0;
+  std::memcpy(h->st_h, &s, sizeof(DevState));
+  CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
+  cudaGraphExec_t g = nullptr;
+  r = step_graph(h, prec, &g);
+  if (r) return r;
+  for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(g, h->stream), "graph launch");
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_synchronize(apollo_dg* h) {
+  if (!h) return APOLLO_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream), "synchronize");
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_get_time(apollo_dg* h, double* t, double* dt) {
+  if (!h || !t || !dt) return APOLLO_ERR_ARG;
+  CK(cudaMemcpyAsync(h->st_h, h->st_d, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream), "get time");
+  CK(cudaStreamSynchronize(h->stream), "get time");
+  *t = h->st_h->t;
+  *dt = h->st_h->dt;
+  return read_errors(h);
+}
+
+apollo_status apollo_dg_step(apollo_dg* h, int nsteps, double* t, double* dt, double tend, apollo_precision prec) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!t || !dt || nsteps < 0) return APOLLO_ERR_ARG;
+  if (tend <= 0.0) {
+    r = apollo_dg_step_async(h, nsteps, *t, *dt, prec);
+    if (r) return r;
+    return apollo_dg_get_time(h, t, dt);
+  }
+  // with an end time: clip before the first step, then one step at a time
+  double tt = *t, dd = *dt;
+  if (std::fabs(tend - tt) < dd) dd = std::fabs(tend - tt);
+  for (int i = 0; i < nsteps && tt < tend; ++i) {
+    DevState s{};
+    s.t = tt;
+    s.dt = dd;
+    s.tend = tend;
+    std::memcpy(h->st_h, &s, sizeof(DevState));
+    CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
+    cudaGraphExec_t g = nullptr;
+    r = step_graph(h, prec, &g);
+    if (r) return r;
+    CK(cudaGraphLaunch(g, h->stream), "graph launch");
+    r = apollo_dg_get_time(h, &tt, &dd);
+    if (r) return r;
+  }
+  *t = tt;
+  *dt = dd;
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_integrals(apollo_dg* h, const double* U, int where, double* sums) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!sums) return APOLLO_ERR_ARG;
+  const double* x = h->U_d;
+  if (U) {
+    if (where == APOLLO_DEVICE_PTR) {
+      x = U;
+    } else {
+      const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
+      CK(cudaMemcpyAsync(h->in_d, U, n, cudaMemcpyHostToDevice, h->stream), "integrals input");
+      x = h->in_d;
+    }
+  }
+  CK(cudaMemsetAsync(h->st_d->sums, 0, sizeof(h->st_d->sums), h->stream), "integrals");
+  DgDev d = make_dev(h);
+  CK(launch_integrals(h->eq, d, x, h->wmass_d, h->stream), "integrals");
+  CK(cudaMemcpyAsync(h->st_h, h->st_d, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream), "integrals");
+  CK(cudaStreamSynchronize(h->stream), "integrals");
+  for (int f = 0; f < h->M; ++f) sums[f] = h->st_h->sums[f];
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int iters, double* ms, int* nk) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!ms || !nk || iters < 1) return APOLLO_ERR_ARG;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) CK(cudaEventCreate(&e), "event");
+  double acc[3] = {0, 0, 0};
+  StageArgs a{};
+  a.x = h->U_d;
+  a.out = h->out_d;
+  a.mode = MODE_RHS;
+  a.reset_lambda = 1;
+  for (int i = 0; i < iters; ++i) {
+    r = enqueue_stage(h, a, prec, ev);
+    if (r) break;
+    CK(cudaEventSynchronize(ev[3]), "event sync");
+    for (int k = 0; k < 3; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (r) return r;
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / iters;
+  *nk = 3;
+  return APOLLO_OK;
+}
+
+const char* apollo_dg_last_error(const apollo_dg* h) { return h ? h->err.c_str() : "null handle"; }
+
+apollo_status apollo_dg_destroy(apollo_dg* h) {
+  if (!h) return APOLLO_ERR_ARG;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_mesh(h);
+  dfree(h->st_d);
+  if (h->st_h) cudaFreeHost(h->st_h);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return APOLLO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,218 @@
+"""Host-side mirror of Apollo's nodal-DG sub-solver over the C ABI (include/apollo_dg.h).
+
+``NodalDG2d`` keeps the call shape of ``WxNodalDG2dMethod`` (setup from an
+equation kind, boundary-condition kinds and a mesh; ``init`` for the first dt;
+``step(t, dt, in, out)`` returning ``(status, suggested_dt)``) and adds the
+resident-state stepper ``advance`` (PETSc TSSSP SSPRK(5,2) with Apollo's dt
+policy).  Arrays are float64 ``[K][Np][m]``, numpy (host) or torch CUDA tensors
+(device).  The CUDA library is required: import fails loudly without it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .mesh import Mesh
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libapollo_dg.so")
+
+APOLLO_HOST_PTR, APOLLO_DEVICE_PTR = 0, 1
+PREC = {"fp64": 0, "mixed": 1}
+
+STATUS = {
+    0: "APOLLO_OK", 1: "APOLLO_ERR_CONFIG", 2: "APOLLO_ERR_MESH", 3: "APOLLO_ERR_NONPHYSICAL",
+    4: "APOLLO_ERR_NAN", 5: "APOLLO_ERR_TIMEOUT", 6: "APOLLO_ERR_CUDA", 7: "APOLLO_ERR_STATE",
+    8: "APOLLO_ERR_ARG", 9: "APOLLO_ERR_ALLOC",
+}
+
+# Apollo equation kinds -> fields per node
+FIELDS = {"advectionEqn": 1, "eulerEqn": 5, "phMaxwellEqn": 8, "eulerEqn2d": 4, "maxwellTM": 3}
+
+
+class ApolloError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Config(C.Structure):
+    _fields_ = [("polynomial_order", C.c_int), ("cfl", C.c_double), ("device", C.c_int), ("stream", C.c_void_p)]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libapollo_dg.so and declare its entry points (raises if missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} not built: run __graft_entry__.build() or make -C apollo_b200/csrc")
+    lib = C.CDLL(path)
+    H = C.c_void_p
+    sig = {
+        "apollo_dg_create": (C.c_int, [C.POINTER(_Config), C.POINTER(H)]),
+        "apollo_dg_set_equation": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
+        "apollo_dg_add_bc": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
+        "apollo_dg_set_mesh": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip]),
+        "apollo_dg_num_fields": (C.c_int, [H]),
+        "apollo_dg_num_nodes": (C.c_int, [H]),
+        "apollo_dg_num_elements": (C.c_int, [H]),
+        "apollo_dg_num_cubature": (C.c_int, [H]),
+        "apollo_dg_num_gauss": (C.c_int, [H]),
+        "apollo_dg_node_coords": (C.c_int, [H, _dp, _dp]),
+        "apollo_dg_set_state": (C.c_int, [H, C.c_void_p, C.c_int]),
+        "apollo_dg_get_state": (C.c_int, [H, C.c_void_p, C.c_int]),
+        "apollo_dg_init_dt": (C.c_int, [H, _dp]),
+        "apollo_dg_rhs": (C.c_int, [H, C.c_double, C.c_double, C.c_void_p, C.c_void_p, _dp, C.c_int, C.c_int]),
+        "apollo_dg_step": (C.c_int, [H, C.c_int, _dp, _dp, C.c_double, C.c_int]),
+        "apollo_dg_step_async": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_int]),
+        "apollo_dg_get_time": (C.c_int, [H, _dp, _dp]),
+        "apollo_dg_synchronize": (C.c_int, [H]),
+        "apollo_dg_integrals": (C.c_int, [H, C.c_void_p, C.c_int, _dp]),
+        "apollo_dg_kernel_times": (C.c_int, [H, C.c_int, C.c_int, _dp, _ip]),
+        "apollo_dg_last_error": (C.c_char_p, [H]),
+        "apollo_dg_destroy": (C.c_int, [H]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    """(pointer, where) of a numpy array or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+        return C.c_void_p(a.ctypes.data), APOLLO_HOST_PTR
+    # torch tensor
+    assert a.dtype.__repr__().endswith("float64") and a.is_contiguous()
+    return C.c_void_p(a.data_ptr()), APOLLO_DEVICE_PTR if a.is_cuda else APOLLO_HOST_PTR
+
+
+class NodalDG2d:
+    """One nodal-DG discretisation on the GPU (Apollo ``Kind = nodalDG2d``)."""
+
+    def __init__(self, N: int, cfl: float, equation: str, eq_params, mesh: Mesh, bcs=(), device: int = 0,
+                 stream: int | None = None):
+        self.lib = load_library()
+        cfg = _Config(N, cfl, device, C.c_void_p(stream) if stream else None)
+        h = C.c_void_p()
+        self._check(self.lib.apollo_dg_create(C.byref(cfg), C.byref(h)), h=None)
+        self.h = h
+        p = np.asarray(list(eq_params), dtype=np.float64)
+        self._check(self.lib.apollo_dg_set_equation(h, equation.encode(), p.ctypes.data_as(_dp), len(p)))
+        for kind, params in bcs:
+            bp = np.asarray(list(params), dtype=np.float64)
+            self._check(self.lib.apollo_dg_add_bc(h, kind.encode(), bp.ctypes.data_as(_dp), len(bp)))
+        self.mesh = mesh
+        self._check(self.lib.apollo_dg_set_mesh(
+            h, mesh.nverts, mesh.vx.ctypes.data_as(_dp), mesh.vy.ctypes.data_as(_dp), mesh.K,
+            mesh.etov.ctypes.data_as(_ip), mesh.face_tag.ctypes.data_as(_ip), mesh.vert_canon.ctypes.data_as(_ip)))
+        self.N = N
+        self.equation = equation
+        self.K = self.lib.apollo_dg_num_elements(h)
+        self.Np = self.lib.apollo_dg_num_nodes(h)
+        self.m = self.lib.apollo_dg_num_fields(h)
+        self.Nc = self.lib.apollo_dg_num_cubature(h)
+        self.Ng = self.lib.apollo_dg_num_gauss(h)
+
+    def _check(self, code, h=0):
+        if code != 0:
+            hh = self.h if h == 0 else h
+            msg = self.lib.apollo_dg_last_error(hh).decode() if hh else ""
+            raise ApolloError(code, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.apollo_dg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.K, self.Np, self.m)
+
+    @property
+    def dofs(self) -> int:
+        return self.K * self.Np * self.m
+
+    def node_coords(self):
+        x = np.empty((self.K, self.Np))
+        y = np.empty((self.K, self.Np))
+        self._check(self.lib.apollo_dg_node_coords(self.h, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp)))
+        return x, y
+
+    def set_state(self, U):
+        p, where = _ptr(U)
+        self._check(self.lib.apollo_dg_set_state(self.h, p, where))
+
+    def get_state(self, out=None):
+        if out is None:
+            out = np.empty(self.shape)
+        p, where = _ptr(out)
+        self._check(self.lib.apollo_dg_get_state(self.h, p, where))
+        return out
+
+    def init_dt(self) -> float:
+        dt = C.c_double()
+        self._check(self.lib.apollo_dg_init_dt(self.h, C.byref(dt)))
+        return dt.value
+
+    def step(self, t: float, dt: float, u, out=None, precision: str = "fp64"):
+        """One RHS evaluation out = L(u) (WxNodalDG2dMethod::step); returns (out, suggested dt)."""
+        if out is None:
+            out = np.empty(self.shape) if isinstance(u, np.ndarray) else u.new_empty(u.shape)
+        pi, wi = _ptr(u)
+        po, wo = _ptr(out)
+        assert wi == wo
+        s = C.c_double()
+        self._check(self.lib.apollo_dg_rhs(self.h, t, dt, pi, po, C.byref(s), wi, PREC[precision]))
+        return out, s.value
+
+    def advance(self, nsteps: int, t: float, dt: float, tend: float = -1.0, precision: str = "fp64"):
+        """Advance the resident state; returns (t, dt for the next step)."""
+        tt, dd = C.c_double(t), C.c_double(dt)
+        self._check(self.lib.apollo_dg_step(self.h, nsteps, C.byref(tt), C.byref(dd), tend, PREC[precision]))
+        return tt.value, dd.value
+
+    def advance_async(self, nsteps: int, t: float, dt: float, precision: str = "fp64"):
+        self._check(self.lib.apollo_dg_step_async(self.h, nsteps, t, dt, PREC[precision]))
+
+    def synchronize(self):
+        self._check(self.lib.apollo_dg_synchronize(self.h))
+
+    def time(self):
+        tt, dd = C.c_double(), C.c_double()
+        self._check(self.lib.apollo_dg_get_time(self.h, C.byref(tt), C.byref(dd)))
+        return tt.value, dd.value
+
+    def kernel_times(self, iters: int = 10, precision: str = "fp64"):
+        """Average ms per kernel of one RHS on the resident state."""
+        ms = np.zeros(8)
+        nk = C.c_int()
+        self._check(self.lib.apollo_dg_kernel_times(self.h, PREC[precision], iters, ms.ctypes.data_as(_dp),
+                                                    C.byref(nk)))
+        return ms[:nk.value]
+
+    def integrals(self, U=None):
+        sums = np.zeros(self.m)
+        if U is None:
+            self._check(self.lib.apollo_dg_integrals(self.h, None, 0, sums.ctypes.data_as(_dp)))
+        else:
+            p, where = _ptr(U)
+            self._check(self.lib.apollo_dg_integrals(self.h, p, where, sums.ctypes.data_as(_dp)))
+        return sums

@@ -1,0 +1,350 @@
+"""Benchmark: DOF-updates/s of the nodal-DG SSPRK(5,2) stepper on B200.
+
+Workload (one "step" = one SSPRK(5,2) time step, 5 right-hand sides, over the
+whole mesh): 2D compressible Euler isentropic vortex (gamma 1.4, strength 5,
+centre (5,5)) on the periodic [0,10]^2, 256 x 256 jittered vertex grid
+(K = 130,050 triangles), order N = 4 (Np = 15), Lax-Friedrichs (Rusanov) flux,
+CFL 0.5, 4 conserved fields.  DOF = K * Np * 4; one DOF-update = one DOF
+advanced by one full step.  Synthetic seeded mesh and closed-form initial state.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed|auto]
+    python bench.py --impl reference ...   # the CPU reference arm
+
+Multi-GPU (torchrun): every rank advances its own instance (weak scaling, no
+data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-updates/s"
+WORKLOAD = "euler_vortex_N4_K130050"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=256, help="vertex grid size (256: K = 130,050)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# --------------------------------------------------------------- CPU arm ----
+def cpu_sample(n_sample: int = 128, steps: int = 2, threads: int | None = None):
+    """Time the CPU oracle (all host threads) on a bounded sample of the workload."""
+    from apollo_b200 import problems
+    from oracle import oracle as orc
+    threads = threads or os.cpu_count() or 1
+    p = problems.euler_vortex(n=n_sample, fields=5)
+    o = orc.Oracle(p.mesh, p.N, orc.EQ_EULER, p.eq_params, cfl=p.cfl)
+    o.set_threads(threads)
+    x, y = o.node_coords()
+    U = np.ascontiguousarray(p.ic(x, y))
+    dt = o.init_dt(U)
+    o.rhs(U)  # warm caches
+    t0 = time.perf_counter()
+    n, t, dt = o.run(U, steps, 0.0, dt)
+    el = time.perf_counter() - t0
+    dofs = p.mesh.K * o.Np * 4
+    return {
+        "value": dofs * n / el, "unit": METRIC, "cores": threads, "kind": "port",
+        "sample": f"{n} SSPRK(5,2) steps of the same vortex problem on a {n_sample}x{n_sample} vertex grid "
+                  f"(K={p.mesh.K}), CPU oracle (C++ restatement of Apollo's RHS loop, float64, 5 Euler fields "
+                  f"as Apollo carries them), {threads} threads",
+        "seconds": el,
+    }
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+    orc.build(with_ref=False)
+    from apollo_b200 import problems
+    threads = os.cpu_count() or 1
+    p = problems.euler_vortex(n=128, fields=5)
+    o = orc.Oracle(p.mesh, p.N, orc.EQ_EULER, p.eq_params, cfl=p.cfl)
+    o.set_threads(threads)
+    x, y = o.node_coords()
+    U = np.ascontiguousarray(p.ic(x, y))
+    t, dt = 0.0, o.init_dt(U)
+    for _ in range(args.warmup):
+        _, t, dt = o.run(U, 1, t, dt)
+    t0 = time.perf_counter()
+    _, t, dt = o.run(U, args.steps, t, dt)
+    el = time.perf_counter() - t0
+    dofs = p.mesh.K * o.Np * 4
+    value = dofs * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_K": p.mesh.K, "N": 4, "fields": 4, "flux": "LF"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"each step: one SSPRK(5,2) step of the vortex on a 128x128 vertex grid "
+                                   f"(K={p.mesh.K}); Apollo's RHS algorithm restated in C++ (oracle), "
+                                   f"{threads} threads"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU arm ----
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"apollo_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        try:
+            self.f.close()
+        except Exception:
+            pass
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i]:
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the dominant kernels from the committed ncu summary."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    except Exception:
+        return {}
+
+
+def ours_arm(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = dist_mod
+    from apollo_b200 import NodalDG2d, problems
+
+    p = problems.euler_vortex(n=args.n, fields=4)
+    stream = torch.cuda.Stream()
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=local, stream=stream.cuda_stream)
+    x, y = s.node_coords()
+    U0 = np.ascontiguousarray(p.ic(x, y))
+    s.set_state(U0)
+    dt0 = s.init_dt()
+
+    prec = args.precision
+    if prec == "auto":
+        prec = "fp64"
+        try:
+            s.step(0.0, 0.0, U0[:0] if False else U0, precision="mixed")
+            prec = "mixed"
+        except Exception:
+            prec = "fp64"
+    dofs = s.K * s.Np * s.m
+
+    def timed(precision, steps, warmup):
+        s.set_state(U0)
+        s.advance_async(warmup, 0.0, dt0, precision=precision)
+        t_w, dt_w = s.time()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            s.advance_async(steps, t_w, dt_w, precision=precision)
+            e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            tt = torch.tensor([ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms
+
+    with ClockSampler(local) as clk:
+        ms = timed(prec, args.steps, args.warmup)
+    clocks = clk.summary()
+    ms_step = ms / args.steps
+    value = dofs * world * args.steps / (ms / 1000.0)
+    t_end, _ = s.time()
+    U_end = s.get_state()
+    l2_exact = float(np.linalg.norm(U_end - p.exact(x, y, t_end)) / np.linalg.norm(p.exact(x, y, t_end)))
+
+    extra = {}
+    if prec == "mixed":
+        ms64 = timed("fp64", args.steps, args.warmup)
+        extra["fp64"] = {"value": dofs * world * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps}
+        extra["speedup_vs_fp64"] = ms64 / ms
+
+    # per-kernel device time and the roofline of the dominant kernel
+    s.set_state(U0)
+    kt = s.kernel_times(10, precision=prec)
+    names = ["volume", "face", "lift_update"]
+    peaks, peak_src = measured_peaks()
+    N, K, M = p.N, s.K, s.m
+    Np, Nc, Ng = s.Np, s.Nc, s.Ng
+    Nf = 3 * Ng
+    nfaces = 3 * K // 2
+    alg_bytes = {  # compulsory bytes per launch (float64)
+        "volume": K * (8 * Np * M + 8 * Np * M + 8 * Nf * M + 32),
+        "face": nfaces * 2 * (8 * Ng * M) * 2 + nfaces * 16,
+        "lift_update": K * (8 * Np * M * 3 + 8 * Nf * M + 8),
+    }
+    alg_flops = {
+        "volume": K * 2 * M * (Nc * Np + 2 * Nc * Np + Nf * Np),
+        "face": nfaces * Ng * 60,
+        "lift_update": K * 2 * M * Nf * Np,
+    }
+    dom = int(np.argmax(kt))
+    dname = names[dom]
+    achieved = alg_bytes[dname] / (kt[dom] / 1000.0) / 1e9
+    traffic = profile_traffic().get(f"{prec}:{dname}:{WORKLOAD}")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": dname,
+                "peak_source": f"{peak_src} hbm_gbs",
+                "kernel_ms": dict(zip(names, [float(v) for v in kt])),
+                "fp64_tflops": alg_flops[dname] / (kt[dom] / 1000.0) / 1e12,
+                "note": "float64 kernels are bounded by the FP64 pipe (B200 nominal 37 TFLOP/s), not HBM"}
+    if prec == "mixed":
+        roofline["note"] = "mixed kernels: tensor-core contractions, HBM-bound"
+
+    e2e = None
+    if not args.no_e2e:
+        # end to end through the public API: per step, the state from pinned host
+        # memory to the device, one SSPRK step, the state back to pinned host memory
+        hU = torch.empty(s.shape, dtype=torch.float64, pin_memory=True)
+        hU.numpy()[...] = U0
+        hO = torch.empty(s.shape, dtype=torch.float64, pin_memory=True)
+        t, dt = 0.0, dt0
+        ne = max(3, min(args.steps, 20))
+        for _ in range(2):
+            s.set_state(hU.numpy())
+            t, dt = s.advance(1, t, dt, precision=prec)
+            s.get_state(hO.numpy())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            s.set_state(hU.numpy())
+            t, dt = s.advance(1, t, dt, precision=prec)
+            s.get_state(hO.numpy())
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if dist:
+            tt = torch.tensor([el], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el = float(tt.item())
+        nb = s.K * s.Np * s.m * 8
+        e2e = {"value": dofs * world * ne / el, "unit": METRIC, "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
+               "steps": ne, "how": "wall clock; per step apollo_dg_set_state (pinned H2D) + apollo_dg_step (1 step) "
+                                   "+ apollo_dg_get_state (pinned D2H)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_sample()
+        except Exception as exc:  # the CPU arm never hides a GPU result
+            cpu = {"value": None, "error": str(exc)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "mixed(bf16x3 tensor, fp32 acc, f64 state)",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "K": s.K, "N": N, "Np": Np, "fields": M, "flux": "LF", "cfl": p.cfl,
+                       "precision": prec, "l2_flush": "inputs larger than L2 (state + stage + scratch "
+                       f"{(dofs * 8 * 4 + 2 * K * Nf * M * 8) / 2**20:.0f} MiB > 126 MiB)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "l2_vs_exact_vortex": l2_exact, "t_end": t_end,
+            "gpu_launches": args.steps * 16, "clocks": clocks, "roofline": roofline, "e2e": e2e,
+            "cpu_baseline": cpu, **extra,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,160 @@
+/*
+ * apollo_dg.h — C ABI of the B200 nodal-DG right-hand side and SSP Runge–Kutta
+ * stepper.  Plain pointers and sizes only; the library owns every device buffer
+ * it allocates and the caller frees nothing of it.
+ *
+ * State layout at this boundary is Apollo's: per element, node-major then field,
+ * U[k][node][field] in float64 (src/subsolvers/wxnodaldg2dmethod.cc:199,330-332).
+ *
+ * Reference interfaces each entry point stands in for (paths inside Apollo):
+ *   apollo_dg_create / set_equation / add_bc / set_mesh
+ *        WxNodalDG2dMethod<REAL>::setup(wxc, DM)  src/subsolvers/wxnodaldg2dmethod.cc:50-152
+ *        with WxHyperbolicEqnSet::setup            src/hyper/wxhyperboliceqnset.cc:43-89
+ *        and the geometry/cubature constructors    src/lib/wxnodaldggeometry2d.cc:10-107,
+ *                                                   src/lib/wxcubature2d.cc:10-169
+ *   apollo_dg_init_dt
+ *        WxNodalDG2dMethod<REAL>::init(dt, Vec)     src/subsolvers/wxnodaldg2dmethod.cc:154-233
+ *   apollo_dg_rhs
+ *        WxNodalDG2dMethod<REAL>::step(t, dt, in, out) -> WxStepperStatus{status, suggestedDt}
+ *                                                   src/subsolvers/wxnodaldg2dmethod.cc:235-542
+ *   apollo_dg_step
+ *        WxPetscTimeSteppingSolver::solve (TSSSP)  src/subsolvers/wxpetsctimestepping.h:69-101
+ *        with ApSolver::ComputeRHSforTS/MonitorVTK src/solvers/apsolver.cc:421-480
+ *   apollo_dg_destroy
+ *        WxNodalDG2dMethod<REAL>::~WxNodalDG2dMethod src/subsolvers/wxnodaldg2dmethod.cc:18-45
+ */
+#ifndef APOLLO_DG_H
+#define APOLLO_DG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct apollo_dg apollo_dg;
+
+/* Return codes.  The reference calls exit(1) where these are returned. */
+typedef enum {
+  APOLLO_OK = 0,
+  APOLLO_ERR_CONFIG = 1,      /* unknown kind, bad parameter, unsupported order */
+  APOLLO_ERR_MESH = 2,        /* non-positive Jacobian or edge length, bad connectivity */
+  APOLLO_ERR_NONPHYSICAL = 3, /* rho <= 0 or p <= 0 in the Euler flux with no floor set */
+  APOLLO_ERR_NAN = 4,         /* NaN in a right-hand side */
+  APOLLO_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+  APOLLO_ERR_CUDA = 6,        /* a CUDA runtime call failed */
+  APOLLO_ERR_STATE = 7,       /* call out of order (no mesh, no equation, no state) */
+  APOLLO_ERR_ARG = 8,         /* null pointer or size out of range */
+  APOLLO_ERR_ALLOC = 9        /* device allocation failed */
+} apollo_status;
+
+/* Arithmetic of the right-hand side.  The state, the stage accumulation, the
+ * dt reduction and the conserved sums stay float64 in every form. */
+typedef enum {
+  APOLLO_PREC_FP64 = 0,  /* plain float64 path */
+  APOLLO_PREC_MIXED = 1  /* tensor-core contractions with split operands, fp32 accumulation */
+} apollo_precision;
+
+/* Pointer location flags for apollo_dg_rhs / set_state / get_state. */
+#define APOLLO_HOST_PTR 0
+#define APOLLO_DEVICE_PTR 1
+
+typedef struct {
+  int polynomial_order; /* N; kernels exist for N = 2..5 ("polynomialOrder") */
+  double cfl;           /* "cfl" */
+  int device;           /* CUDA device ordinal */
+  void* stream;         /* cudaStream_t to run on; NULL = a stream owned by the handle */
+} apollo_dg_config;
+
+/* Setup -------------------------------------------------------------------- */
+apollo_status apollo_dg_create(const apollo_dg_config* cfg, apollo_dg** out);
+
+/* Equation plugin by Apollo kind name, parameters in the order listed:
+ *   "advectionEqn"  ux, uy, uz                     (1 field)
+ *   "eulerEqn"      gas_gamma, minPressure, minDensity   (5 fields: rho, rhou, rhov, rhow, E)
+ *   "phMaxwellEqn"  c0, gamma, chi                 (8 fields: Ex, Ey, Ez, Bx, By, Bz, phi, psi)
+ * and two planar forms of the same equations (an extension; identical
+ * arithmetic when the dropped fields are zero):
+ *   "eulerEqn2d"    gas_gamma, minPressure, minDensity   (4 fields: rho, rhou, rhov, E)
+ *   "maxwellTM"     c0                             (3 fields: Ez, Bx, By)
+ * Numerical flux: Lax-Friedrichs ("Numerical_Flux = LF"). */
+apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const double* params, int nparams);
+
+/* Boundary-condition plugin, appended to the list; a face tagged t uses the
+ * t-th condition added (Apollo's boundaryConditions[t-1]).  Kinds and params:
+ *   "gridFixedBC"                   value
+ *   "isentropicVortexBC"            u0, v0, x0, y0, gas_gamma, beta
+ *   "maxwellTransverseMagneticBC"   (none)
+ *   "phmConductingWallBC"           (none)                                      */
+apollo_status apollo_dg_add_bc(apollo_dg* h, const char* kind, const double* params, int nparams);
+
+/* Mesh: vertices (vx, vy), counter-clockwise triangles etov[K][3] (vertex 0 ->
+ * reference (-1,-1), 1 -> (1,-1), 2 -> (-1,1)); face_tag[K][3]: 0 = pair with
+ * the face sharing both vertices (or, if none, boundary condition 1), t > 0 =
+ * boundary condition t; vert_canon[nverts]: canonical vertex id used for
+ * pairing (periodic identification), may be NULL.  Builds geometry, face map
+ * and operators on the device. */
+apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, const double* vy, int K,
+                                 const int* etov, const int* face_tag, const int* vert_canon);
+
+/* Sizes: fields per node, nodes per element, elements, cubature points, Gauss
+ * points per face. */
+int apollo_dg_num_fields(const apollo_dg* h);
+int apollo_dg_num_nodes(const apollo_dg* h);
+int apollo_dg_num_elements(const apollo_dg* h);
+int apollo_dg_num_cubature(const apollo_dg* h);
+int apollo_dg_num_gauss(const apollo_dg* h);
+
+/* Physical node coordinates x, y [K][Np] into host memory. */
+apollo_status apollo_dg_node_coords(apollo_dg* h, double* x, double* y);
+
+/* Resident state U [K][Np][m]: copy in / out (host or device pointer). */
+apollo_status apollo_dg_set_state(apollo_dg* h, const double* U, int where);
+apollo_status apollo_dg_get_state(apollo_dg* h, double* U, int where);
+
+/* Initial dt from the resident state: 2/3 cfl dtscale rmin / max wave speed,
+ * wave speeds from the Riemann solver at every node. */
+apollo_status apollo_dg_init_dt(apollo_dg* h, double* dt);
+
+/* One right-hand-side evaluation out = L(in) at time t (dt is passed to the
+ * boundary hooks as Apollo does).  in/out are [K][Np][m], host or device
+ * pointers per `where`; suggested_dt (may be NULL) receives
+ * 2/3 cfl dtscale rmin / max numerical-flux speed. */
+apollo_status apollo_dg_rhs(apollo_dg* h, double t, double dt, const double* in, double* out,
+                            double* suggested_dt, int where, apollo_precision prec);
+
+/* Advance the resident state by up to nsteps SSPRK(5,2) steps (PETSc TSSSP
+ * default), starting at *t with step *dt.  After each step the next dt is
+ * min(dt, suggestion of the last stage), clipped so t does not pass tend
+ * (tend <= 0: no end time).  On return *t and *dt hold the time reached and
+ * the dt for the next step.  With tend <= 0 the steps are queued without host
+ * synchronisation (one CUDA graph per step); the call returns after the last
+ * step completes. */
+apollo_status apollo_dg_step(apollo_dg* h, int nsteps, double* t, double* dt, double tend, apollo_precision prec);
+
+/* Same as apollo_dg_step but returns as soon as the work is queued on the
+ * handle's stream; *t and *dt are not updated (read them with
+ * apollo_dg_get_time after apollo_dg_synchronize). */
+apollo_status apollo_dg_step_async(apollo_dg* h, int nsteps, double t, double dt, apollo_precision prec);
+apollo_status apollo_dg_get_time(apollo_dg* h, double* t, double* dt);
+apollo_status apollo_dg_synchronize(apollo_dg* h);
+
+/* Per-field sums of the element integrals of U (M J U summed), float64. */
+apollo_status apollo_dg_integrals(apollo_dg* h, const double* U, int where, double* sums);
+
+/* Diagnostics: average device time in milliseconds of each kernel of one
+ * right-hand side, over `iters` evaluations of the resident state (CUDA events
+ * on the handle's stream).  ms[0..2] = volume, face, LIFT + update.  *nk
+ * receives the number of kernels timed. */
+apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int iters, double* ms, int* nk);
+
+/* Error text of the last failing call on this handle. */
+const char* apollo_dg_last_error(const apollo_dg* h);
+
+apollo_status apollo_dg_destroy(apollo_dg* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* APOLLO_DG_H */

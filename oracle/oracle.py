@@ -1,0 +1,231 @@
+"""ORACLE — test infrastructure only.  ctypes bindings for the CPU checkers.
+
+* ``Oracle``      — the C++ restatement of Apollo's nodal-DG RHS and SSPRK(5,2)
+                    stepper (dg_oracle.cpp, built to _build/liboracle.so).
+* ``RefPlugins``  — Apollo's own equation plugins and exprFunc compiled
+                    unmodified (ref_adapter.cpp, built to _ref/libapollo_ref.so
+                    where the Apollo source tree exists).
+
+Only tests, ``__graft_entry__.smoke`` and the CPU-baseline leg of ``bench.py``
+import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libapollo_ref.so")
+
+EQ_ADVECTION, EQ_EULER, EQ_MAXWELL = 0, 1, 2
+BC_FIXED, BC_VORTEX, BC_TM, BC_PEC = 0, 1, 2, 3
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def build(with_ref: bool = True) -> None:
+    """Compile the oracle (and the reference plugins where the source exists)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    src = os.environ.get("APOLLO_SRC", "/root/reference/src")
+    if with_ref and os.path.isdir(src):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"APOLLO_SRC={src}"], check=True)
+
+
+def _lib():
+    if not os.path.exists(LIB_PATH):
+        build(with_ref=False)
+    lib = C.CDLL(LIB_PATH)
+    lib.orc_create.restype = C.c_void_p
+    lib.orc_create.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, C.c_int, _ip,
+                               _dp, C.c_double]
+    for name in ("orc_destroy",):
+        getattr(lib, name).argtypes = [C.c_void_p]
+    for name in ("orc_meqn", "orc_np", "orc_nc", "orc_ng", "orc_error"):
+        getattr(lib, name).argtypes = [C.c_void_p]
+        getattr(lib, name).restype = C.c_int
+    for name in ("orc_dtscale", "orc_rmin"):
+        getattr(lib, name).argtypes = [C.c_void_p]
+        getattr(lib, name).restype = C.c_double
+    lib.orc_set_threads.argtypes = [C.c_void_p, C.c_int]
+    lib.orc_set_ref_plugins.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_node_coords.argtypes = [C.c_void_p, _dp, _dp]
+    lib.orc_connectivity.argtypes = [C.c_void_p, _ip]
+    lib.orc_operator.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.orc_rhs.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, _dp]
+    lib.orc_rhs.restype = C.c_double
+    lib.orc_init_dt.argtypes = [C.c_void_p, _dp]
+    lib.orc_init_dt.restype = C.c_double
+    lib.orc_ssp_step.argtypes = [C.c_void_p, _dp, C.c_double, C.c_double]
+    lib.orc_ssp_step.restype = C.c_double
+    lib.orc_run.argtypes = [C.c_void_p, _dp, C.c_int, _dp, _dp, C.c_double]
+    lib.orc_run.restype = C.c_int
+    return lib
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class Oracle:
+    """CPU oracle for one mesh, order and equation (fields in Apollo's count:
+    1 advection, 5 Euler, 8 Maxwell)."""
+
+    def __init__(self, mesh, N: int, eq: int, eqp, bcs=(), cfl: float = 0.5):
+        self.lib = _lib()
+        self.N = N
+        eqp = np.zeros(4) if eqp is None else np.asarray(list(eqp) + [0.0] * (4 - len(eqp)), dtype=np.float64)
+        kinds = np.asarray([b[0] for b in bcs] or [0], dtype=np.int32)
+        pars = np.zeros((max(1, len(bcs)), 8))
+        for i, b in enumerate(bcs):
+            pars[i, :len(b[1])] = b[1]
+        self._keep = [mesh, eqp, kinds, pars]
+        self.h = self.lib.orc_create(N, eq, _p(eqp), mesh.nverts, _p(mesh.vx), _p(mesh.vy), mesh.K,
+                                     _p(mesh.etov, _ip), _p(mesh.face_tag, _ip), _p(mesh.vert_canon, _ip),
+                                     max(1, len(bcs)), _p(kinds, _ip), _p(pars), cfl)
+        self.K = mesh.K
+        self.meqn = self.lib.orc_meqn(self.h)
+        self.Np = self.lib.orc_np(self.h)
+        self.Nc = self.lib.orc_nc(self.h)
+        self.Ng = self.lib.orc_ng(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    @property
+    def shape(self):
+        return (self.K, self.Np, self.meqn)
+
+    def set_threads(self, n: int) -> None:
+        self.lib.orc_set_threads(self.h, int(n))
+
+    def use_ref_plugins(self, ref: "RefPlugins", eqn_handle) -> None:
+        self._ref_keep = (ref, eqn_handle)
+        self.lib.orc_set_ref_plugins(self.h, C.cast(ref.lib.ref_flux, C.c_void_p),
+                                     C.cast(ref.lib.ref_numflux, C.c_void_p), eqn_handle)
+
+    def node_coords(self):
+        x = np.empty((self.K, self.Np))
+        y = np.empty((self.K, self.Np))
+        self.lib.orc_node_coords(self.h, _p(x), _p(y))
+        return x, y
+
+    def connectivity(self):
+        c = np.empty((self.K, 6), dtype=np.int32)
+        self.lib.orc_connectivity(self.h, _p(c, _ip))
+        return c
+
+    def operator(self, which: int):
+        shapes = {0: (self.Nc, self.Np), 1: (self.Nc, self.Np), 2: (self.Nc, self.Np), 3: (3 * self.Ng, self.Np),
+                  4: (self.Np, self.Np), 5: (self.Nc,), 6: (self.Ng,)}
+        out = np.empty(shapes[which])
+        self.lib.orc_operator(self.h, which, _p(out))
+        return out
+
+    @property
+    def error(self) -> int:
+        return self.lib.orc_error(self.h)
+
+    @property
+    def dtscale(self) -> float:
+        return self.lib.orc_dtscale(self.h)
+
+    @property
+    def rmin(self) -> float:
+        return self.lib.orc_rmin(self.h)
+
+    def rhs(self, u, t: float = 0.0, dt: float = 0.0):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.shape)
+        out = np.empty_like(u)
+        sugg = self.lib.orc_rhs(self.h, t, dt, _p(u), _p(out))
+        return out, sugg
+
+    def init_dt(self, u) -> float:
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.shape)
+        return self.lib.orc_init_dt(self.h, _p(u))
+
+    def ssp_step(self, u, t0: float, dt: float) -> float:
+        assert u.flags.c_contiguous and u.dtype == np.float64
+        return self.lib.orc_ssp_step(self.h, _p(u), t0, dt)
+
+    def run(self, u, nsteps: int, t: float, dt: float, tend: float = -1.0):
+        """Advance u in place; returns (steps taken, t, dt for the next step)."""
+        assert u.flags.c_contiguous and u.dtype == np.float64
+        tt = C.c_double(t)
+        dd = C.c_double(dt)
+        n = self.lib.orc_run(self.h, _p(u), nsteps, C.byref(tt), C.byref(dd), tend)
+        return n, tt.value, dd.value
+
+
+class RefPlugins:
+    """Apollo's own equation plugins and exprFunc (compiled unmodified)."""
+
+    def __init__(self):
+        if not os.path.exists(REF_PATH):
+            raise FileNotFoundError(REF_PATH)
+        lib = C.CDLL(REF_PATH)
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_eqn_create.restype = C.c_void_p
+        lib.ref_eqn_create.argtypes = [C.c_char_p]
+        lib.ref_eqn_destroy.argtypes = [C.c_void_p]
+        lib.ref_eqn_meqn.argtypes = [C.c_void_p]
+        lib.ref_eqn_meqn.restype = C.c_int
+        lib.ref_flux.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        lib.ref_numflux.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        lib.ref_speed2.argtypes = [C.c_void_p, _dp]
+        lib.ref_speed2.restype = C.c_double
+        lib.ref_exprfunc_create.restype = C.c_void_p
+        lib.ref_exprfunc_create.argtypes = [C.c_char_p]
+        lib.ref_exprfunc_size.argtypes = [C.c_void_p]
+        lib.ref_exprfunc_size.restype = C.c_int
+        lib.ref_exprfunc_eval.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _dp]
+        lib.ref_exprfunc_destroy.argtypes = [C.c_void_p]
+        self.lib = lib
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_PATH)
+
+    def equation(self, kind: str, **params):
+        body = "\n".join(f"  {k} = {v}" for k, v in params.items())
+        text = f"<top>\n Equations = [eq]\n <eq>\n  Kind = {kind}\n{body}\n </eq>\n</top>\n"
+        h = self.lib.ref_eqn_create(text.encode())
+        if not h:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return h
+
+    def flux(self, h, d: int, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        f = np.zeros_like(q)
+        self.lib.ref_flux(h, d, _p(q), _p(f))
+        return f
+
+    def numflux(self, h, n, qM, qP):
+        n = np.ascontiguousarray(n, dtype=np.float64)
+        qM = np.array(qM, dtype=np.float64)
+        qP = np.array(qP, dtype=np.float64)
+        f = np.zeros_like(qM)
+        lam = C.c_double(0.0)
+        self.lib.ref_numflux(h, _p(n), _p(qM), _p(qP), _p(f), C.byref(lam))
+        return f, lam.value
+
+    def speed2(self, h, q) -> float:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        return self.lib.ref_speed2(h, _p(q))
+
+    def exprfunc(self, text: str):
+        h = self.lib.ref_exprfunc_create(text.encode())
+        if not h:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return h
+
+    def exprfunc_eval(self, h, t: float, x: float, y: float):
+        out = np.zeros(self.lib.ref_exprfunc_size(h))
+        self.lib.ref_exprfunc_eval(h, t, x, y, _p(out))
+        return out

@@ -1,0 +1,75 @@
+"""Generate the golden fixtures under tests/golden/ (run in the development container).
+
+Each fixture is a small seeded case of one benchmark problem: the mesh arrays,
+the initial state, one right-hand side with its suggested dt, the initial dt,
+and the state after a few SSPRK(5,2) steps with Apollo's dt policy.  They are
+produced by the CPU oracle with Apollo's own equation plugins compiled
+unmodified (oracle/_ref/libapollo_ref.so, the per-point flux and numerical flux
+hooks are the reference code); initial states are cross-checked against
+Apollo's own exprFunc evaluating the example inputs' expressions.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from apollo_b200 import problems  # noqa: E402
+from oracle import oracle as orc  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CASES = [
+    # name, builder, kwargs, oracle eq, eq params, ref kind, ref params, bcs, steps
+    ("adv_N3", problems.advection, dict(n=8, N=3), orc.EQ_ADVECTION, (1.0, 0.5, 0.0), "advectionEqn",
+     dict(ux=1.0, uy=0.5), (), 4),
+    ("adv_N2", problems.advection, dict(n=7, N=2, seed=3), orc.EQ_ADVECTION, (1.0, 0.5, 0.0), "advectionEqn",
+     dict(ux=1.0, uy=0.5), (), 4),
+    ("euler_N4", problems.euler_vortex, dict(n=7, N=4, fields=5), orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn",
+     dict(gas_gamma=1.4), (), 3),
+    ("euler_N3", problems.euler_vortex, dict(n=8, N=3, fields=5, seed=5), orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn",
+     dict(gas_gamma=1.4), (), 3),
+    ("maxwell_N5", problems.maxwell_tm, dict(n=6, N=5, fields=8), orc.EQ_MAXWELL, (1.0, 0.0, 0.0), "phMaxwellEqn",
+     dict(c0=1.0), ((orc.BC_TM, ()),), 3),
+    ("maxwell_N2", problems.maxwell_tm, dict(n=7, N=2, fields=8, seed=2), orc.EQ_MAXWELL, (1.0, 0.0, 0.0),
+     "phMaxwellEqn", dict(c0=1.0), ((orc.BC_TM, ()),), 3),
+]
+
+
+def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref):
+    prob = builder(**kw)
+    mesh = prob.mesh
+    o = orc.Oracle(mesh, prob.N, eq, eqp, bcs=bcs, cfl=prob.cfl)
+    eh = ref.equation(ref_kind, **ref_params)
+    o.use_ref_plugins(ref, eh)
+    x, y = o.node_coords()
+    U0 = np.ascontiguousarray(prob.ic(x, y), dtype=np.float64)
+    rhs, sugg = o.rhs(U0, 0.0, 0.0)
+    dt0 = o.init_dt(U0)
+    U = U0.copy()
+    n, t, dt = o.run(U, steps, 0.0, dt0)
+    assert n == steps and o.error == 0
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        vx=mesh.vx, vy=mesh.vy, etov=mesh.etov, face_tag=mesh.face_tag, vert_canon=mesh.vert_canon,
+        N=prob.N, cfl=prob.cfl, eq=eq, eqp=np.asarray(eqp, dtype=np.float64), equation=ref_kind,
+        bc_kinds=np.asarray([b[0] for b in bcs], dtype=np.int32), x=x, y=y, U0=U0, rhs=rhs, sugg=sugg, dt0=dt0,
+        steps=steps, U_end=U, t_end=t, dt_end=dt)
+    return name, U0.shape, float(np.abs(rhs).max())
+
+
+def main():
+    orc.build(with_ref=True)
+    ref = orc.RefPlugins()
+    for case in CASES:
+        print(make_case(*case, ref=ref))
+
+
+if __name__ == "__main__":
+    main()

