@@ -30,104 +30,160 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// ---------------------------------------------------------------------------
+// Float64 tensor-core fragments: mma.sync m8n8k4 f64 (DMMA).  Fragment layout
+// (PTX ISA, mma.m8n8k4 .f64): A 8x4, lane holds A[lane/4][lane%4]; B 4x8, lane
+// holds B[lane%4][lane/4]; C 8x8, lane holds C[lane/4][2*(lane%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+constexpr int round_up(int x, int m) { return (x + m - 1) / m * m; }
+// leading dimension (in doubles) of a shared-memory tile read by fragments:
+// rows 4 apart must land 8 banks apart, i.e. ld = 4 (mod 16)
+constexpr int pad_ld(int x) { return x + ((4 - x % 16) + 16) % 16; }
+
+// Tile of elements for the float64 volume kernel.  Columns of every GEMM are
+// (element, field) pairs; rows are cubature points, Gauss points or nodes.
 template <int N, int M> struct VolTile {
   static constexpr int NP = Sizes<N>::NP, NC = Sizes<N>::NC, NF = Sizes<N>::NF;
-  static constexpr int E = 8;  // elements per tile
-  static constexpr int OPS = NC * NP + 2 * NP * NC + NF * NP;
-  static constexpr int QS = E * NP * M;
-  static constexpr int RS = E * NC * 2 * M;
-  static constexpr size_t BYTES = sizeof(double) * (OPS + QS + RS);
+  // 16 elements per tile (8 for 8 fields or N >= 5), 64 for scalar advection,
+  // keeping the tile near 110 KB of shared memory (two blocks per SM)
+  static constexpr int E = M == 1 ? 64 : ((M == 8 || N >= 5) ? 8 : 16);
+  static constexpr int COLS = round_up(E * M, 8);
+  static constexpr int LDB = pad_ld(COLS);
+  static constexpr int NPK = round_up(NP, 4);    // K of V*q and I*q
+  static constexpr int LDA1 = pad_ld(NPK);
+  static constexpr int NCR = round_up(NC, 8);    // rows of V*q
+  static constexpr int NFR = round_up(NF, 8);    // rows of I*q
+  static constexpr int NPR = round_up(NP, 8);    // rows of D*[R;S]
+  static constexpr int K2 = round_up(2 * NC, 4); // K of D*[R;S]
+  static constexpr int LDA2 = pad_ld(K2);
+  static constexpr int RSR = K2 > NCR ? K2 : NCR;
+  static constexpr int OFF_V = 0;
+  static constexpr int OFF_D = OFF_V + NCR * LDA1;
+  static constexpr int OFF_I = OFF_D + NPR * LDA2;
+  static constexpr int OFF_Q = OFF_I + NFR * LDA1;
+  static constexpr int OFF_RS = OFF_Q + NPK * LDB;
+  static constexpr int TOTAL = OFF_RS + RSR * LDB;
+  static constexpr size_t BYTES = sizeof(double) * TOTAL;
 };
+
+constexpr int tile_n(int cblocks, int rblocks, int warps) {
+  // widest column tile (4, 2, 1 blocks of 8) that still gives every warp work
+  return (cblocks % 4 == 0 && rblocks * (cblocks / 4) >= warps) ? 4
+         : (cblocks % 2 == 0 && rblocks * (cblocks / 2) >= warps) ? 2 : 1;
+}
+
+// C[ROWS x COLS] = A[ROWS x K] B[K x COLS] over the block's warps; A, B in
+// shared memory; the epilogue gets (row, col, value) per output.
+template <int ROWS, int COLS, int K, int LDA, int LDB, int NWARPS, class Epi>
+__device__ __forceinline__ void block_dgemm(const double* A, const double* B, Epi epi) {
+  constexpr int RB = ROWS / 8, CB = COLS / 8, KS = K / 4;
+  constexpr int TN = tile_n(CB, RB, NWARPS);
+  constexpr int NT = RB * (CB / TN);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lr = lane >> 2, lc = lane & 3;
+  for (int t = warp; t < NT; t += NWARPS) {
+    const int rb = t % RB, cg = t / RB;
+    double c[TN][2];
+#pragma unroll
+    for (int n = 0; n < TN; ++n) c[n][0] = c[n][1] = 0.0;
+    const double* ap = A + (rb * 8 + lr) * LDA + lc;
+    const double* bp = B + lc * LDB + cg * TN * 8 + lr;
+#pragma unroll 4
+    for (int k = 0; k < KS; ++k) {
+      const double a = ap[k * 4];
+#pragma unroll
+      for (int n = 0; n < TN; ++n) dmma_8x8x4(c[n], a, bp[k * 4 * LDB + n * 8]);
+    }
+#pragma unroll
+    for (int n = 0; n < TN; ++n) {
+      const int col = (cg * TN + n) * 8 + 2 * lc;
+      epi(rb * 8 + lr, col, c[n][0]);
+      epi(rb * 8 + lr, col + 1, c[n][1]);
+    }
+  }
+}
 
 template <int EQ, int N>
 __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
   using P = Eq<EQ>;
   constexpr int M = P::M;
   using T = VolTile<N, M>;
-  constexpr int NP = T::NP, NC = T::NC, NF = T::NF, E = T::E;
+  constexpr int NP = T::NP, NC = T::NC, NF = T::NF, E = T::E, LDB = T::LDB;
+  constexpr int NWARPS = kThreads / 32;
   extern __shared__ double smem[];
-  double* sV = smem;
-  double* sDr = sV + NC * NP;
-  double* sDs = sDr + NP * NC;
-  double* sI = sDs + NP * NC;
-  double* sq = sI + NF * NP;
-  double* srs = sq + T::QS;
+  double* sV = smem + T::OFF_V;
+  double* sD = smem + T::OFF_D;
+  double* sI = smem + T::OFF_I;
+  double* sQ = smem + T::OFF_Q;
+  double* sRS = smem + T::OFF_RS;
   const int tid = threadIdx.x;
   if (a.reset_lambda && blockIdx.x == 0 && tid == 0) d.st->lam_bits = 0ull;
-  for (int i = tid; i < NC * NP; i += kThreads) sV[i] = d.V[i];
-  for (int i = tid; i < NP * NC; i += kThreads) { sDr[i] = d.Dr[i]; sDs[i] = d.Ds[i]; }
-  for (int i = tid; i < NF * NP; i += kThreads) sI[i] = d.I[i];
+  // operators, zero-padded: V [NCR][NPK], D = [Dr | Ds] [NPR][K2], I [NFR][NPK]
+  for (int i = tid; i < T::NCR * T::LDA1; i += kThreads) {
+    const int r = i / T::LDA1, c = i % T::LDA1;
+    sV[i] = (r < NC && c < NP) ? d.V[r * NP + c] : 0.0;
+  }
+  for (int i = tid; i < T::NPR * T::LDA2; i += kThreads) {
+    const int r = i / T::LDA2, c = i % T::LDA2;
+    double v = 0.0;
+    if (r < NP && c < NC) v = d.Dr[r * NC + c];
+    else if (r < NP && c >= NC && c < 2 * NC) v = d.Ds[r * NC + c - NC];
+    sD[i] = v;
+  }
+  for (int i = tid; i < T::NFR * T::LDA1; i += kThreads) {
+    const int r = i / T::LDA1, c = i % T::LDA1;
+    sI[i] = (r < NF && c < NP) ? d.I[r * NP + c] : 0.0;
+  }
+  // padding rows of the right-hand operands stay zero
+  for (int i = tid; i < T::NPK * LDB; i += kThreads) sQ[i] = 0.0;
+  for (int i = tid; i < T::RSR * LDB; i += kThreads) sRS[i] = 0.0;
   int err = 0;
   const int ntiles = (d.K + E - 1) / E;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int k0 = tile * E;
     const int ne = min(E, d.K - k0);
     __syncthreads();
+    // q tile, [e][node][field] -> Q[node][e*M + field]
     const double* src = a.x + (size_t)k0 * NP * M;
-    for (int i = tid; i < ne * NP * M; i += kThreads) sq[i] = src[i];
+    for (int i = tid; i < ne * NP * M; i += kThreads) {
+      const int e = i / (NP * M), r = i - e * NP * M, j = r / M, f = r - j * M;
+      sQ[j * LDB + e * M + f] = src[i];
+    }
     __syncthreads();
-    // cubature values and fluxes
+    // cubature values Qc = V Q (into the R/S buffer) and face traces I Q (to HBM)
+    block_dgemm<T::NCR, T::COLS, T::NPK, T::LDA1, LDB, NWARPS>(
+        sV, sQ, [&](int r, int c, double v) { sRS[r * LDB + c] = v; });
+    block_dgemm<T::NFR, T::COLS, T::NPK, T::LDA1, LDB, NWARPS>(sI, sQ, [&](int r, int c, double v) {
+      const int e = c / M, f = c - e * M;
+      if (r < NF && e < ne) d.trace[((size_t)(k0 + e) * NF + r) * M + f] = v;
+    });
+    __syncthreads();
+    // physical flux at every cubature point; R = rx F + ry G into row c,
+    // S = sx F + sy G into row NC + c (row c is overwritten by its reader only)
     for (int idx = tid; idx < ne * NC; idx += kThreads) {
       const int e = idx / NC, c = idx - e * NC;
-      double qc[M];
+      double qc[M], F[M], G[M];
 #pragma unroll
-      for (int f = 0; f < M; ++f) qc[f] = 0.0;
-      const double* vrow = sV + c * NP;
-      const double* qe = sq + e * NP * M;
-#pragma unroll 5
-      for (int j = 0; j < NP; ++j) {
-        const double v = vrow[j];
-#pragma unroll
-        for (int f = 0; f < M; ++f) qc[f] = fma(v, qe[j * M + f], qc[f]);
-      }
-      double F[M], G[M];
+      for (int f = 0; f < M; ++f) qc[f] = sRS[c * LDB + e * M + f];
       P::flux2(d.eqp, qc, F, G, &err);
       const ElemGeo& g = d.geo[k0 + e];
-      double* rs = srs + (e * NC + c) * 2 * M;
 #pragma unroll
       for (int f = 0; f < M; ++f) {
-        rs[f] = g.rx * F[f] + g.ry * G[f];
-        rs[M + f] = g.sx * F[f] + g.sy * G[f];
+        sRS[c * LDB + e * M + f] = g.rx * F[f] + g.ry * G[f];
+        sRS[(NC + c) * LDB + e * M + f] = g.sx * F[f] + g.sy * G[f];
       }
-    }
-    // face traces
-    for (int idx = tid; idx < ne * NF; idx += kThreads) {
-      const int e = idx / NF, gp = idx - e * NF;
-      double tq[M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) tq[f] = 0.0;
-      const double* irow = sI + gp * NP;
-      const double* qe = sq + e * NP * M;
-#pragma unroll 5
-      for (int j = 0; j < NP; ++j) {
-        const double v = irow[j];
-#pragma unroll
-        for (int f = 0; f < M; ++f) tq[f] = fma(v, qe[j * M + f], tq[f]);
-      }
-      double* dst = d.trace + ((size_t)(k0 + e) * NF + gp) * M;
-#pragma unroll
-      for (int f = 0; f < M; ++f) dst[f] = tq[f];
     }
     __syncthreads();
-    // volume contraction
-    for (int idx = tid; idx < ne * NP; idx += kThreads) {
-      const int e = idx / NP, i = idx - e * NP;
-      double acc[M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) acc[f] = 0.0;
-      const double* dr = sDr + i * NC;
-      const double* ds = sDs + i * NC;
-      const double* rs = srs + e * NC * 2 * M;
-#pragma unroll 2
-      for (int c = 0; c < NC; ++c) {
-        const double a1 = dr[c], a2 = ds[c];
-#pragma unroll
-        for (int f = 0; f < M; ++f) acc[f] = fma(a1, rs[c * 2 * M + f], fma(a2, rs[c * 2 * M + M + f], acc[f]));
-      }
-      double* dst = d.vol + ((size_t)(k0 + e) * NP + i) * M;
-#pragma unroll
-      for (int f = 0; f < M; ++f) dst[f] = acc[f];
-    }
+    // volume term: [Dr | Ds] [R; S]
+    block_dgemm<T::NPR, T::COLS, T::K2, T::LDA2, LDB, NWARPS>(sD, sRS, [&](int r, int c, double v) {
+      const int e = c / M, f = c - e * M;
+      if (r < NP && e < ne) d.vol[((size_t)(k0 + e) * NP + r) * M + f] = v;
+    });
   }
   if (err) atomicOr(&d.st->err, err);
 }
@@ -191,20 +247,32 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
 
 template <int N, int M> struct LiftTile {
   static constexpr int NP = Sizes<N>::NP, NF = Sizes<N>::NF;
-  static constexpr int E = 8;
-  static constexpr size_t BYTES = sizeof(double) * (NP * NF + E * NF * M);
+  static constexpr int E = M == 1 ? 64 : (M == 8 ? 8 : 16);
+  static constexpr int COLS = round_up(E * M, 8);
+  static constexpr int LDB = pad_ld(COLS);
+  static constexpr int NFK = round_up(NF, 4);  // K: face Gauss points
+  static constexpr int LDA = pad_ld(NFK);
+  static constexpr int NPR = round_up(NP, 8);
+  static constexpr int OFF_L = 0;
+  static constexpr int OFF_F = NPR * LDA;
+  static constexpr size_t BYTES = sizeof(double) * (OFF_F + NFK * LDB);
 };
 
 template <int EQ, int N>
 __global__ void __launch_bounds__(kThreads) k_lift(DgDev d, StageArgs a) {
   constexpr int M = Eq<EQ>::M;
   using T = LiftTile<N, M>;
-  constexpr int NP = T::NP, NF = T::NF, E = T::E;
+  constexpr int NP = T::NP, NF = T::NF, E = T::E, LDB = T::LDB;
+  constexpr int NWARPS = kThreads / 32;
   extern __shared__ double smem[];
-  double* sL = smem;
-  double* sf = sL + NP * NF;
+  double* sL = smem + T::OFF_L;
+  double* sF = smem + T::OFF_F;
   const int tid = threadIdx.x;
-  for (int i = tid; i < NP * NF; i += kThreads) sL[i] = d.L[i];
+  for (int i = tid; i < T::NPR * T::LDA; i += kThreads) {
+    const int r = i / T::LDA, c = i % T::LDA;
+    sL[i] = (r < NP && c < NF) ? d.L[r * NF + c] : 0.0;
+  }
+  for (int i = tid; i < T::NFK * LDB; i += kThreads) sF[i] = 0.0;
   const double dt = a.time_from_state ? d.st->dt : a.dt_arg;
   const double c_stage = dt / 4.0;  // dt/(s-1), s = 5
   const double c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
@@ -214,36 +282,26 @@ __global__ void __launch_bounds__(kThreads) k_lift(DgDev d, StageArgs a) {
     const int k0 = tile * E;
     const int ne = min(E, d.K - k0);
     __syncthreads();
+    // numerical-flux tile, [e][gauss][field] -> F[gauss][e*M + field]
     const double* src = d.flux + (size_t)k0 * NF * M;
-    for (int i = tid; i < ne * NF * M; i += kThreads) sf[i] = src[i];
-    __syncthreads();
-    for (int idx = tid; idx < ne * NP; idx += kThreads) {
-      const int e = idx / NP, i = idx - e * NP;
-      const int k = k0 + e;
-      double acc[M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) acc[f] = 0.0;
-      const double* lrow = sL + i * NF;
-      const double* fe = sf + e * NF * M;
-#pragma unroll 4
-      for (int gp = 0; gp < NF; ++gp) {
-        const double l = lrow[gp];
-#pragma unroll
-        for (int f = 0; f < M; ++f) acc[f] = fma(l, fe[gp * M + f], acc[f]);
-      }
-      const double invJ = d.geo[k].invJ;
-      const size_t off = ((size_t)k * NP + i) * M;
-#pragma unroll
-      for (int f = 0; f < M; ++f) {
-        const double r = d.vol[off + f] - invJ * acc[f];
-        if (r != r) err |= ERRB_NAN;
-        double o;
-        if (a.mode == MODE_RHS) o = r;
-        else if (a.mode == MODE_STAGE) o = a.x[off + f] + c_stage * r;
-        else o = c_al * a.x[off + f] + c_be * r + c_ga * a.u0[off + f];
-        a.out[off + f] = o;
-      }
+    for (int i = tid; i < ne * NF * M; i += kThreads) {
+      const int e = i / (NF * M), r = i - e * NF * M, g = r / M, f = r - g * M;
+      sF[g * LDB + e * M + f] = src[i];
     }
+    __syncthreads();
+    block_dgemm<T::NPR, T::COLS, T::NFK, T::LDA, LDB, NWARPS>(sL, sF, [&](int i, int c, double v) {
+      const int e = c / M, f = c - e * M;
+      if (i >= NP || e >= ne) return;
+      const int k = k0 + e;
+      const size_t off = ((size_t)k * NP + i) * M + f;
+      const double r = d.vol[off] - d.geo[k].invJ * v;
+      if (r != r) err |= ERRB_NAN;
+      double o;
+      if (a.mode == MODE_RHS) o = r;
+      else if (a.mode == MODE_STAGE) o = a.x[off] + c_stage * r;
+      else o = c_al * a.x[off] + c_be * r + c_ga * a.u0[off];
+      a.out[off] = o;
+    });
   }
   if (err) atomicOr(&d.st->err, err);
 }

@@ -42,7 +42,28 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="vertex grid size (256: K = 130,050)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--rhs-only", type=int, default=0,
+                    help="profiling driver: set up the workload, run this many RHS evaluations, exit")
     return ap.parse_args()
+
+
+def rhs_only(args):
+    """Set up the benchmark workload and evaluate the RHS a few times (for ncu)."""
+    import torch
+    from apollo_b200 import NodalDG2d, problems
+    p = problems.euler_vortex(n=args.n, fields=4)
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=0)
+    x, y = s.node_coords()
+    u = torch.from_numpy(np.ascontiguousarray(p.ic(x, y))).cuda()
+    out = torch.empty_like(u)
+    prec = "fp64" if args.precision == "auto" else args.precision
+    for _ in range(args.rhs_only):
+        s.step(0.0, 0.0, u, out, precision=prec)
+    torch.cuda.synchronize()
+    print(json.dumps({"rhs_only": args.rhs_only, "K": s.K, "precision": prec,
+                      "checksum": float(out.abs().sum().item())}))
+    s.close()
+    return 0
 
 
 def dist_env():
@@ -341,6 +362,8 @@ def ours_arm(args):
 
 def main():
     args = parse()
+    if args.rhs_only:
+        return rhs_only(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

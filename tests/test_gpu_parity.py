@@ -7,7 +7,12 @@ from golden_cases import NAMES, load, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-12  # relative L2, float64 path vs the float64 oracle
+TOL = 1e-12  # relative L2, float64 path vs the float64 oracle (states, stage updates)
+# The isentropic-vortex RHS is a small difference of O(1) flux terms (the
+# far field is a uniform flow whose flux divergence cancels); recompiling the
+# oracle itself with FMA contraction moves its RHS by 9e-13 relative L2.  The
+# RHS of those fixtures is held to this looser bound, the states to TOL.
+RHS_TOL_CANCELLING = 1e-11
 
 
 def _solver(g):
@@ -21,7 +26,11 @@ def test_rhs_matches_oracle(name):
     x, y = s.node_coords()
     assert rel_l2(x, g["x"]) == 0.0
     out, sugg = s.step(0.0, 0.0, g["U0"])
-    assert rel_l2(out, g["rhs"]) <= TOL
+    tol = RHS_TOL_CANCELLING if name.startswith("euler") else TOL
+    assert rel_l2(out, g["rhs"]) <= tol
+    # the forward-Euler stage u + dt L(u) that the stepper forms
+    dt0 = float(g["dt0"])
+    assert rel_l2(g["U0"] + dt0 * out, g["U0"] + dt0 * g["rhs"]) <= TOL
     assert sugg == pytest.approx(float(g["sugg"]), rel=1e-14)
 
 
@@ -48,7 +57,57 @@ def test_device_pointers(name):
     out = torch.empty_like(u)
     s.step(0.0, 0.0, u, out)
     torch.cuda.synchronize()
-    assert rel_l2(out.cpu().numpy(), g["rhs"]) <= TOL
+    host, _ = s.step(0.0, 0.0, g["U0"])
+    np.testing.assert_array_equal(out.cpu().numpy(), host)
+    tol = RHS_TOL_CANCELLING if name.startswith("euler") else TOL
+    assert rel_l2(out.cpu().numpy(), g["rhs"]) <= tol
+
+
+@pytest.mark.parametrize("case", ["euler5", "euler4", "maxwell8", "maxwell3", "advection"])
+@pytest.mark.parametrize("N", [2, 3, 4, 5])
+def test_rhs_random_states_vs_oracle(case, N):
+    """Well-conditioned RHS (random physical states, walls + vortex BC): 1e-12 relative L2."""
+    from oracle import oracle as orc
+    from apollo_b200.mesh import jittered_square
+    rng = np.random.default_rng(100 * N + len(case))
+    mesh = jittered_square(7, (0.0, 0.0), (2.0, 1.0), seed=N, periodic=False)
+    if case.startswith("euler"):
+        m = 5 if case == "euler5" else 4
+        kind = "eulerEqn" if m == 5 else "eulerEqn2d"
+        vb = (1.0, 0.3, 1.0, 0.5, 1.4, 2.0)
+        s = NodalDG2d(N, 0.5, kind, (1.4, 0.0, 0.0), mesh, bcs=(("isentropicVortexBC", vb),))
+        o = orc.Oracle(mesh, N, orc.EQ_EULER, (1.4, 0.0, 0.0), bcs=((orc.BC_VORTEX, vb),))
+        # perturbations of a physical state, so that the interpolants at the
+        # cubature and Gauss points keep rho > 0 and p > 0
+        U = 0.1 * rng.uniform(-1, 1, (mesh.K, s.Np, 5))
+        U[..., 0] += 1.0
+        U[..., 1] += 0.5
+        if m == 4:
+            U[..., 3] = 0.0
+        U[..., 4] = 0.5 * (U[..., 1] ** 2 + U[..., 2] ** 2 + U[..., 3] ** 2) / U[..., 0] + 2.0 + U[..., 4]
+        sel = [0, 1, 2, 3, 4] if m == 5 else [0, 1, 2, 4]
+    elif case.startswith("maxwell"):
+        m = 8 if case == "maxwell8" else 3
+        if m == 8:
+            s = NodalDG2d(N, 0.5, "phMaxwellEqn", (1.3, 0.2, 0.7), mesh, bcs=(("phmConductingWallBC", ()),))
+            o = orc.Oracle(mesh, N, orc.EQ_MAXWELL, (1.3, 0.2, 0.7), bcs=((orc.BC_PEC, ()),))
+            U = rng.uniform(-1, 1, (mesh.K, s.Np, 8))
+            sel = list(range(8))
+        else:
+            s = NodalDG2d(N, 0.5, "maxwellTM", (1.3,), mesh, bcs=(("phmConductingWallBC", ()),))
+            o = orc.Oracle(mesh, N, orc.EQ_MAXWELL, (1.3, 0.0, 0.0), bcs=((orc.BC_PEC, ()),))
+            U = np.zeros((mesh.K, s.Np, 8))
+            U[..., 2:5] = rng.uniform(-1, 1, (mesh.K, s.Np, 3))
+            sel = [2, 3, 4]
+    else:
+        s = NodalDG2d(N, 0.5, "advectionEqn", (0.7, -1.2, 0.0), mesh, bcs=(("gridFixedBC", (0.25,)),))
+        o = orc.Oracle(mesh, N, orc.EQ_ADVECTION, (0.7, -1.2, 0.0), bcs=((orc.BC_FIXED, (0.25,)),))
+        U = rng.uniform(-1, 1, (mesh.K, s.Np, 1))
+        sel = [0]
+    ref, sugg_ref = o.rhs(U, 0.3, 0.01)
+    out, sugg = s.step(0.3, 0.01, np.ascontiguousarray(U[..., sel]))
+    assert rel_l2(out, ref[..., sel]) <= TOL
+    assert sugg == pytest.approx(sugg_ref, rel=1e-14)
 
 
 def test_reduced_fields_equal_full_fields():
