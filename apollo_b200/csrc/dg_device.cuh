@@ -48,6 +48,7 @@ struct DgDev {
   int K, nfaces, N;
   const ElemGeo* geo;
   const FaceRec* faces;
+  const int* conn;  // [K][6]: per face (neighbour element, its face) or (-tag, -1) on a boundary
   const double *V, *Dr, *Ds, *I, *L, *gz, *gw;
   double *vol, *trace, *flux;  // scratch: [K][NP][M], [K][NF][M], [K][NF][M]
   DevState* st;

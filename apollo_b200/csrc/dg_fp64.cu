@@ -341,6 +341,7 @@ __global__ void k_finalize(DgDev d) {
   st->t = t;
   st->dt = nd;
   st->steps += 1;
+  st->lam_bits = 0ull;  // the next step's last stage reduces into it afresh
 }
 
 template <int EQ>

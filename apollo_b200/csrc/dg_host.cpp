@@ -35,9 +35,11 @@ struct apollo_dg {
   // device memory
   ElemGeo* geo_d = nullptr;
   FaceRec* faces_d = nullptr;
+  int* conn_d = nullptr;
+  std::vector<int> conn_h;
   double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
          *gw_d = nullptr, *wmass_d = nullptr;
-  double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
+  double *U_d = nullptr, *W_d = nullptr, *W2_d = nullptr, *in_d = nullptr, *out_d = nullptr;
   double *vol_d = nullptr, *trace_d = nullptr, *flux_d = nullptr;
   DevState* st_d = nullptr;
   DevState* st_h = nullptr;  // pinned
@@ -83,10 +85,10 @@ void dfree(T*& p) {
 void free_mesh(apollo_dg* h) {
   for (auto& g : h->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-  dfree(h->geo_d); dfree(h->faces_d);
+  dfree(h->geo_d); dfree(h->faces_d); dfree(h->conn_d);
   dfree(h->V_d); dfree(h->Dr_d); dfree(h->Ds_d); dfree(h->I_d); dfree(h->L_d); dfree(h->gz_d); dfree(h->gw_d);
   dfree(h->wmass_d);
-  dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
+  dfree(h->U_d); dfree(h->W_d); dfree(h->W2_d); dfree(h->in_d); dfree(h->out_d);
   dfree(h->vol_d); dfree(h->trace_d); dfree(h->flux_d);
   if (h->mixed) { mixed_destroy(h->mixed); h->mixed = nullptr; }
   h->have_state = false;
@@ -106,6 +108,7 @@ DgDev make_dev(const apollo_dg* h) {
   d.N = h->ops.N;
   d.geo = h->geo_d;
   d.faces = h->faces_d;
+  d.conn = h->conn_d;
   d.V = h->V_d; d.Dr = h->Dr_d; d.Ds = h->Ds_d; d.I = h->I_d; d.L = h->L_d; d.gz = h->gz_d; d.gw = h->gw_d;
   d.vol = h->vol_d; d.trace = h->trace_d; d.flux = h->flux_d;
   d.st = h->st_d;
@@ -146,17 +149,24 @@ apollo_status enqueue_stage(apollo_dg* h, const StageArgs& a, apollo_precision p
 
 apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
   const int s = 5;
+  // The float64 kernels read neighbour data only in the volume/face kernels,
+  // before the LIFT kernel writes, so their stages update W in place.  The
+  // fused mixed kernel reads neighbour states while other CTAs write, so its
+  // stages alternate between W and W2.
+  const bool pingpong = prec == APOLLO_PREC_MIXED;
+  double* last = h->W_d;
   for (int i = 0; i < s; ++i) {
     StageArgs a{};
     a.time_from_state = 1;
     a.reset_lambda = 1;
     if (i < s - 1) {
-      a.x = i == 0 ? h->U_d : h->W_d;
-      a.out = h->W_d;
+      a.x = i == 0 ? h->U_d : last;
+      a.out = (pingpong && (i & 1)) ? h->W2_d : h->W_d;
+      last = a.out;
       a.mode = MODE_STAGE;
       a.frac = i / (s - 1.);
     } else {
-      a.x = h->W_d;
+      a.x = last;
       a.u0 = h->U_d;
       a.out = h->U_d;
       a.mode = MODE_FINAL;
@@ -340,6 +350,7 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
     }
   h->faces_h.clear();
   h->faces_h.reserve((size_t)K * 2);
+  h->conn_h.assign((size_t)K * 6, -1);
   for (int k = 0; k < K; ++k)
     for (int f = 0; f < 3; ++f) {
       const int tag = face_tag ? face_tag[3 * k + f] : 0;
@@ -349,14 +360,19 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
         if (t > std::max(1, h->bcs.n)) return fail(h, APOLLO_ERR_MESH, "face tag without a boundary condition");
         if (h->bcs.n == 0) return fail(h, APOLLO_ERR_MESH, "boundary face but no boundary condition added");
         h->faces_h.push_back(FaceRec{k, f, -t, -1});
-      } else if (p > 3 * k + f) {
-        h->faces_h.push_back(FaceRec{k, f, p / 3, p % 3});
+        h->conn_h[6 * k + 2 * f] = -t;
+        h->conn_h[6 * k + 2 * f + 1] = -1;
+      } else {
+        if (p > 3 * k + f) h->faces_h.push_back(FaceRec{k, f, p / 3, p % 3});
+        h->conn_h[6 * k + 2 * f] = p / 3;
+        h->conn_h[6 * k + 2 * f + 1] = p % 3;
       }
     }
   // device buffers
   const size_t nU = (size_t)K * Np * M, nT = (size_t)K * o.Nf * M;
   CK(upload(&h->geo_d, h->geo_h.data(), h->geo_h.size()), "geometry upload");
   CK(upload(&h->faces_d, h->faces_h.data(), h->faces_h.size()), "face map upload");
+  CK(upload(&h->conn_d, h->conn_h.data(), h->conn_h.size()), "connectivity upload");
   std::vector<double> DrW(o.DrW.a), DsW(o.DsW.a);
   CK(upload(&h->V_d, o.Vc.a.data(), o.Vc.a.size()), "op upload");
   CK(upload(&h->Dr_d, DrW.data(), DrW.size()), "op upload");
@@ -368,6 +384,7 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
   CK(upload(&h->wmass_d, o.mass_colsum.data(), o.mass_colsum.size()), "op upload");
   CK(cudaMalloc((void**)&h->U_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->W_d, nU * sizeof(double)), "state alloc");
+  CK(cudaMalloc((void**)&h->W2_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->in_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->out_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->vol_d, nU * sizeof(double)), "scratch alloc");
@@ -438,6 +455,8 @@ apollo_status apollo_dg_rhs(apollo_dg* h, double t, double dt, const double* in,
   apollo_status r = check_ready(h);
   if (r) return r;
   if (!in || !out) return APOLLO_ERR_ARG;
+  if (prec == APOLLO_PREC_MIXED && where == APOLLO_DEVICE_PTR && (const double*)out == in)
+    return fail(h, APOLLO_ERR_ARG, "the mixed-precision RHS needs distinct in and out buffers");
   const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
   const double* x = in;
   double* o = out;

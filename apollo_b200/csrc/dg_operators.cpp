@@ -221,6 +221,25 @@ bool build_ref_ops(int N, RefOps& o) {
   o.mass_colsum.assign(o.Np, 0.0);
   for (int j = 0; j < o.Np; ++j)
     for (int i = 0; i < o.Np; ++i) o.mass_colsum[j] += Mass(i, j);
+  // node permutations of the three rotations of the reference triangle
+  const double vr[3] = {-1.0, 1.0, -1.0}, vs[3] = {-1.0, -1.0, 1.0};
+  o.rot.assign(3 * o.Np, -1);
+  bool ok = true;
+  for (int k = 0; k < 3 && ok; ++k)
+    for (int j = 0; j < o.Np && ok; ++j) {
+      const double l1 = 0.5 * (1.0 + o.r[j]), l2 = 0.5 * (1.0 + o.s[j]), l0 = 1.0 - l1 - l2;
+      const double pr = l0 * vr[k] + l1 * vr[(k + 1) % 3] + l2 * vr[(k + 2) % 3];
+      const double ps = l0 * vs[k] + l1 * vs[(k + 1) % 3] + l2 * vs[(k + 2) % 3];
+      int best = -1;
+      double bd = 1e-9;
+      for (int m = 0; m < o.Np; ++m) {
+        const double dd = std::fabs(o.r[m] - pr) + std::fabs(o.s[m] - ps);
+        if (dd < bd) { bd = dd; best = m; }
+      }
+      if (best < 0) ok = false;
+      else o.rot[k * o.Np + j] = best;
+    }
+  if (!ok) o.rot.clear();
   return true;
 }
 

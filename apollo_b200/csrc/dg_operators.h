@@ -38,6 +38,10 @@ struct RefOps {
   Mat Lift;       // [Np][Nf] = VVT Interp^T
   std::vector<double> mass_colsum;  // [Np] integrals of the nodal basis on the reference element
   double rmin = 0.0;
+  // rot[k][j]: the node at which a field rotated so that face k becomes face 0
+  // takes its value (vertex i of the rotated triangle is vertex (i + k) % 3);
+  // empty if the node set is not rotation symmetric to 1e-9
+  std::vector<int> rot;  // [3][Np]
 };
 
 bool build_ref_ops(int N, RefOps& out);

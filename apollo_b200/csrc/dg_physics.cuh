@@ -69,6 +69,10 @@ template <> struct Eq<EQ_ADVECTION> {
   APOLLO_HD static double speed2(const EqParams& P, const double* q) {
     return dmax3(0.0, P.p[0] * P.p[0], P.p[1] * P.p[1]);
   }
+  // the Lax-Friedrichs speed of numflux, in float64
+  APOLLO_HD static double lf_lambda(const EqParams& P, const double* qM, const double* qP) {
+    return dmax2(fabs(P.p[0]), fabs(P.p[1]));
+  }
 };
 
 // ---------------------------------------------------------------- Euler ----
@@ -141,6 +145,16 @@ struct EulerBase {
       nf[c] = T(0.5) * (nx * (fM[c] + fP[c]) + ny * (gM[c] + gP[c]) + lambda * (qM[c] - qP[c]));
     return lambda;
   }
+  APOLLO_HD static double lf_lambda(const EqParams& P, const double* qM, const double* qP) {
+    double a[MF], b[MF], pM[5], pP[5];
+    for (int c = 0; c < MF; ++c) { a[c] = qM[c]; b[c] = qP[c]; }
+    prim(P, a, pM);
+    prim(P, b, pP);
+    const double gamma = P.p[0];
+    const double c0M = sqrt(pM[1] * pM[1] + pM[2] * pM[2] + pM[3] * pM[3]) + sqrt(gamma * pM[4] / pM[0]);
+    const double c0P = sqrt(pP[1] * pP[1] + pP[2] * pP[2] + pP[3] * pP[3]) + sqrt(gamma * pP[4] / pP[0]);
+    return c0M > c0P ? c0M : c0P;
+  }
   // max over the Roe solver's waves (ql = qr = q) of max(sx^2, sy^2)
   APOLLO_HD static double speed2(const EqParams& P, const double* q) {
     double g1 = P.p[0] - 1.0, lam = 0.0;
@@ -203,6 +217,9 @@ template <> struct Eq<EQ_MAXWELL> {
       nf[c] = T(0.5) * (nx * (fM[c] + fP[c]) + ny * (gM[c] + gP[c]) + lambda * (qM[c] - qP[c]));
     return lambda;
   }
+  APOLLO_HD static double lf_lambda(const EqParams& P, const double* qM, const double* qP) {
+    return dmax3(P.p[2] * P.p[0], P.p[1] * P.p[0], P.p[0]);
+  }
   APOLLO_HD static double speed2(const EqParams& P, const double* q) {
     double c0 = P.p[0], g = P.p[1], k = P.p[2];
     double s[6] = {c0, -c0, c0 * g, -c0 * g, c0 * k, -c0 * k};
@@ -236,6 +253,9 @@ template <> struct Eq<EQ_MAXWELL_TM> {
     for (int c = 0; c < 3; ++c)
       nf[c] = T(0.5) * (nx * (fM[c] + fP[c]) + ny * (gM[c] + gP[c]) + lambda * (qM[c] - qP[c]));
     return lambda;
+  }
+  APOLLO_HD static double lf_lambda(const EqParams& P, const double* qM, const double* qP) {
+    return dmax3(0.0 * P.p[0], 0.0 * P.p[0], P.p[0]);
   }
   APOLLO_HD static double speed2(const EqParams& P, const double* q) {
     double c0 = P.p[0];

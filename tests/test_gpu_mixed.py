@@ -1,0 +1,85 @@
+"""Mixed-precision (tcgen05, split tf32, deviation form) path vs the float64 path (B200)."""
+import numpy as np
+import pytest
+
+from apollo_b200 import ApolloError, NodalDG2d, problems
+from golden_cases import NAMES, load, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(g):
+    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_mixed_rhs_close_to_fp64(name):
+    g = load(name)
+    s = _solver(g)
+    r64, s64 = s.step(0.0, 0.0, g["U0"])
+    rmx, smx = s.step(0.0, 0.0, g["U0"], precision="mixed")
+    dt0 = float(g["dt0"])
+    # the stage update the stepper forms, and the RHS itself.  These fixtures
+    # are coarse (5-8 vertices a side), where an element's fluctuation is as
+    # large as its mean and the deviation form gains little; tf32 x3 products
+    # with fp32 flux leave ~1e-6 of the RHS scale.
+    e_stage = rel_l2(g["U0"] + dt0 * rmx, g["U0"] + dt0 * r64)
+    e_rhs = rel_l2(rmx, r64)
+    print(name, "stage", e_stage, "rhs", e_rhs)
+    assert e_stage <= 1e-6
+    assert e_rhs <= 1e-4
+    assert smx == pytest.approx(s64, rel=1e-6)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_mixed_steps_close_to_fp64(name):
+    g = load(name)
+    s = _solver(g)
+    s.set_state(g["U0"])
+    dt0 = s.init_dt()
+    t64, d64 = s.advance(int(g["steps"]), 0.0, dt0)
+    U64 = s.get_state()
+    s.set_state(g["U0"])
+    tmx, dmx = s.advance(int(g["steps"]), 0.0, dt0, precision="mixed")
+    Umx = s.get_state()
+    e = rel_l2(Umx, U64)
+    print(name, "steps", e)
+    assert e <= 1e-6
+    assert tmx == pytest.approx(t64, rel=1e-7)
+
+
+def test_mixed_vortex_l2_after_steps():
+    """Euler vortex (N = 4) on a 64 x 64 grid: mixed stays within 1e-6 relative L2 of float64."""
+    p = problems.euler_vortex(n=64, N=4, fields=4)
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh)
+    x, y = s.node_coords()
+    U0 = np.ascontiguousarray(p.ic(x, y))
+    s.set_state(U0)
+    dt0 = s.init_dt()
+    s.advance(100, 0.0, dt0)
+    U64 = s.get_state()
+    s.set_state(U0)
+    s.advance(100, 0.0, dt0, precision="mixed")
+    Umx = s.get_state()
+    e = rel_l2(Umx, U64)
+    print("vortex 64x64 100 steps mixed vs fp64", e)
+    assert e <= 1e-6
+
+
+def test_mixed_rejects_aliased_buffers():
+    torch = pytest.importorskip("torch")
+    g = load(NAMES[0])
+    s = _solver(g)
+    u = torch.from_numpy(g["U0"]).cuda()
+    with pytest.raises(ApolloError):
+        s.step(0.0, 0.0, u, u, precision="mixed")
+
+
+def test_mixed_nan_reports_error():
+    g = load(NAMES[0])
+    s = _solver(g)
+    U = g["U0"].copy()
+    U[5, 1, 0] = np.nan
+    with pytest.raises(ApolloError) as e:
+        s.step(0.0, 0.0, U, precision="mixed")
+    assert e.value.code == 4

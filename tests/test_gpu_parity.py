@@ -142,7 +142,8 @@ def test_conservation_full_size_periodic():
     dt0 = s.init_dt()
     s.advance(20, 0.0, dt0)
     after = s.integrals()
-    assert np.all(np.abs(after - before) <= 1e-11 * np.abs(before))
+    # relative to the largest integral: the y-momentum integral is ~0 by symmetry
+    assert np.all(np.abs(after - before) <= 1e-12 * np.abs(before).max())
 
 
 def test_nan_input_reports_error():
