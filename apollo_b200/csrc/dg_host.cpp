@@ -603,6 +603,30 @@ apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int it
   return APOLLO_OK;
 }
 
+}  // extern "C"
+
+namespace apollo {
+
+// Read-only view of a handle's discretisation for the no-allocation entry
+// point (dg_noalloc.cu); the scratch pointers are left for the caller to set.
+bool handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size_t* nU, size_t* nT) {
+  if (!h || h->eq < 0 || h->K == 0) return false;
+  *d = make_dev(h);
+  *eq = h->eq;
+  *device = h->cfg.device;
+  *nU = (size_t)h->K * h->ops.Np * h->M;
+  *nT = (size_t)h->K * h->ops.Nf * h->M;
+  return true;
+}
+
+void handle_set_error(apollo_dg* h, const char* msg) {
+  if (h) h->err = msg;
+}
+
+}  // namespace apollo
+
+extern "C" {
+
 const char* apollo_dg_last_error(const apollo_dg* h) { return h ? h->err.c_str() : "null handle"; }
 
 apollo_status apollo_dg_destroy(apollo_dg* h) {

@@ -77,6 +77,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_synchronize": (C.c_int, [H]),
         "apollo_dg_integrals": (C.c_int, [H, C.c_void_p, C.c_int, _dp]),
         "apollo_dg_kernel_times": (C.c_int, [H, C.c_int, C.c_int, _dp, _ip]),
+        "apollo_dg_rhs_noalloc": (C.c_int, [H, C.c_double, C.c_double, C.c_void_p, C.c_void_p, _dp, C.c_void_p]),
         "apollo_dg_last_error": (C.c_char_p, [H]),
         "apollo_dg_destroy": (C.c_int, [H]),
     }

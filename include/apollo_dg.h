@@ -149,6 +149,28 @@ apollo_status apollo_dg_integrals(apollo_dg* h, const double* U, int where, doub
  * receives the number of kernels timed. */
 apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int iters, double* ms, int* nk);
 
+/* The float64 right-hand side for callers that cannot allocate device memory
+ * when they evaluate it (a host framework that owns all device memory through
+ * its own allocator, code inside another library's stream capture, a loop that
+ * must not take the device-wide synchronisation of cudaMalloc).  No counterpart
+ * in Apollo.  Same result as apollo_dg_rhs with APOLLO_PREC_FP64 on device
+ * pointers; the kernels' scratch (volume term, face traces, face fluxes) lives
+ * in a 64 MiB static device array that every GPU loading this library holds
+ * until the process exits, so this call allocates nothing.  The handle itself
+ * was built (and allocated) by apollo_dg_create / apollo_dg_set_mesh.
+ *   in, out       device pointers [K][Np][m], distinct
+ *   suggested_dt  may be NULL; when given, the call waits for the stream and
+ *                 reports non-physical states and NaN like apollo_dg_rhs
+ *   stream        cudaStream_t to run on (NULL: the legacy default stream)
+ * Meshes whose scratch exceeds 64 MiB ((Np + 6 (N + 1) * 2) * m * 8 bytes per
+ * element, about 28,000 elements at N = 4 with 4 fields) are rejected with
+ * APOLLO_ERR_ARG.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU, on
+ * any handle or stream of the same device, race. */
+apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt, const double* in, double* out,
+                                    double* suggested_dt, void* stream);
+
 /* Error text of the last failing call on this handle. */
 const char* apollo_dg_last_error(const apollo_dg* h);
 
