@@ -68,7 +68,8 @@ template <int N, int M> struct MixCfg {
   static constexpr int SZ_A1 = 128 * K1 * 4;
   static constexpr int SZ_CH = 128 * KV * 4;
   static constexpr int SZ_U = max_c(8 * SZ_A1, NBUF * 2 * SZ_CH);
-  static constexpr int SZ_ST = max_c(NC16, 32) * 128 * 4;
+  static constexpr int SR = 48;  // cubature points staged at a time (a multiple of VPC)
+  static constexpr int SZ_ST = max_c(SR, 32) * 128 * 4;
   static constexpr int O_B1H = 0, O_B1L = O_B1H + SZ_B1;
   static constexpr int O_B2H = O_B1L + SZ_B1, O_B2L = O_B2H + SZ_B2;
   static constexpr int O_U = round_up_c(O_B2L + SZ_B2, 128);
@@ -76,11 +77,13 @@ template <int N, int M> struct MixCfg {
   static constexpr int O_G0 = O_ST + SZ_ST;                // g = 0 traces: [6][128] float
   static constexpr int O_GEO = O_G0 + 6 * 128 * 4;         // [E][16] float
   static constexpr int O_RS = O_GEO + E * 16 * 4;          // operator row sums [NP][5] double
-  static constexpr int O_RB = O_RS + NP * 5 * 8;           // R(0), S(0): [E][2M] float
-  static constexpr int O_FB = O_RB + E * 2 * M * 4;        // face reference: [E][3][M] float
-  static constexpr int O_CN = O_FB + E * 3 * M * 4;        // [E][6] int
-  static constexpr int O_QB = O_CN + E * 6 * 4;            // means: own [128], neighbours [3][128] float
-  static constexpr int O_ROT = O_QB + 4 * 128 * 4;         // [3][NP] int
+  static constexpr int O_RB = O_RS + NP * 5 * 8;           // R(0), S(0): [E][2M] double
+  static constexpr int O_FB = O_RB + E * 2 * M * 8;        // face references: [E][3][M] double
+  static constexpr int O_RBH = O_FB + E * 3 * M * 8;       // fp32 point-0 fluxes F, G, face f*: [E][5M]
+  static constexpr int O_CN = O_RBH + E * 5 * M * 4;       // [E][6] int
+  static constexpr int O_QB = O_CN + E * 6 * 4;            // means: own [128], neighbours [3][128] double
+  static constexpr int O_QF = O_QB + 4 * 128 * 8;          // the same means as float
+  static constexpr int O_ROT = O_QF + 4 * 128 * 4;         // [3][NP] int
   static constexpr int O_MB = round_up_c(O_ROT + 3 * NP * 4, 8);  // mbarriers: A, ring[NBUF]
   static constexpr int O_TS = O_MB + 8 * (1 + NBUF);       // TMEM base, abort flag
   static constexpr int BYTES = O_TS + 16;
@@ -88,11 +91,10 @@ template <int N, int M> struct MixCfg {
   static_assert(NG <= 16, "one 16-column chunk per face");
 };
 
-// tf32 split by truncation: hi keeps the top 10 mantissa bits, lo = x - hi is
-// exact in fp32 and itself loses < 2^-11 |lo| when the tensor core reads it.
+// tf32 split, both halves rounded to nearest: x = hi + lo + O(2^-22 |x|).
 __device__ __forceinline__ void split_trunc(float x, float& h, float& l) {
-  h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-  l = x - h;
+  h = umma::to_tf32(x);
+  l = umma::to_tf32(x - h);
 }
 
 template <int M>
@@ -113,7 +115,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   constexpr int M = P::M;
   using C = MixCfg<N, M>;
   constexpr int NP = C::NP, NC = C::NC, NG = C::NG, NF = C::NF, EPQ = C::EPQ, E = C::E, K1 = C::K1;
-  constexpr int VPC = C::VPC, KV = C::KV;
+  constexpr int VPC = C::VPC, KV = C::KV, SR = C::SR;
+  static_assert(SR % VPC == 0 && SR % 16 == 0, "staging waves hold whole chunks");
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* B1h = sm + C::O_B1H;
   unsigned char* B1l = sm + C::O_B1L;
@@ -124,10 +127,12 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   float* G0 = (float*)(sm + C::O_G0);
   float* GEO = (float*)(sm + C::O_GEO);
   double* RSUM = (double*)(sm + C::O_RS);
-  float* Rb = (float*)(sm + C::O_RB);
-  float* Fb = (float*)(sm + C::O_FB);
+  double* Rb = (double*)(sm + C::O_RB);   // [E][2M]: R(0), S(0) in float64
+  double* Fb = (double*)(sm + C::O_FB);   // [E][3][M]: face references in float64
+  float* P0 = (float*)(sm + C::O_RBH);    // [E][5M]: fp32 F(0), G(0), f*_fc(0)
   int* CN = (int*)(sm + C::O_CN);
-  float* QB = (float*)(sm + C::O_QB);  // [0..127] own means, [128 (1 + fc) + r] neighbour means
+  double* QB = (double*)(sm + C::O_QB);  // [0..127] own means, [128 (1 + fc) + r] neighbour means
+  float* QF = (float*)(sm + C::O_QF);
   int* ROT = (int*)(sm + C::O_ROT);
   uint64_t* mbar = (uint64_t*)(sm + C::O_MB);
   uint32_t* tslot = (uint32_t*)(sm + C::O_TS);
@@ -147,6 +152,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     *(float*)(B1h + umma::kmajor_offset(r, k, K1)) = h;
     *(float*)(B1l + umma::kmajor_offset(r, k, K1)) = l;
   }
+  // B2: volume chunks (Dr, Ds at cubature points, weights folded in), then per
+  // face the LIFT columns times the Gauss weights
   for (int i = tid; i < C::NPN * C::KB2; i += kMixThreads) {
     const int r = i / C::KB2, k = i % C::KB2;
     double v = 0.0;
@@ -156,7 +163,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         if (c < NC) v = (k & 1) ? d.Ds[r * NC + c] : d.Dr[r * NC + c];
       } else {
         const int kk = k - C::NV * KV, fc = kk / 16, g = kk % 16;
-        if (g < NG) v = d.L[r * NF + fc * NG + g];
+        if (g < NG) v = d.L[r * NF + fc * NG + g] * d.gw[g];
       }
     }
     const float h = umma::to_tf32((float)v);
@@ -192,7 +199,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   const double dt = a.time_from_state ? d.st->dt : a.dt_arg;
   const bool want_lambda = a.mode != MODE_STAGE;
   int err = 0;
-  float lmax = 0.f;
+  double lmax = 0.0;
   uint32_t phA = 0, ring_uses[C::NBUF];
 #pragma unroll
   for (int b = 0; b < C::NBUF; ++b) ring_uses[b] = 0;
@@ -202,6 +209,34 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   const int rr = tid & 127, rq = rr >> 5, rln = rr & 31;
   const int rel = rln / M, rf = rln - rel * M, re = rq * EPQ + rel;
   auto rowb_of = [](int e) { return (e / EPQ) * 32 + (e % EPQ) * M; };
+
+  // fp32 pointwise physics, identical wherever it is evaluated
+  auto flux32 = [&](const float* qc, float* F, float* G) { P::flux2(d.eqp, qc, F, G, &err); };
+  auto bc_coords = [&](int e, int fc, int g, double& x, double& y) {
+    const ElemGeo& geo = d.geo[e];
+    const double z = d.gz[g];
+    double r, s;
+    if (fc == 0) { r = z; s = -1.0; }
+    else if (fc == 1) { r = -z; s = z; }
+    else { r = -1.0; s = -z; }
+    x = 0.5 * (-geo.vx[0] * (r + s) + geo.vx[1] * (1. + r) + geo.vx[2] * (1. + s));
+    y = 0.5 * (-geo.vy[0] * (r + s) + geo.vy[1] * (1. + r) + geo.vy[2] * (1. + s));
+  };
+  // Lax-Friedrichs flux on face fc at Gauss point g, fp32, float normals
+  auto numflux32 = [&](int e, int k, int fc, int g, const float* qM, float* qP, float* nf) {
+    const float* G = GEO + e * 16;
+    const float nx = G[5 + fc], ny = G[8 + fc];
+    const int nb = CN[e * 6 + 2 * fc];
+    if (nb < 0) {
+      double x, y;
+      bc_coords(k, fc, g, x, y);
+      apply_bc<EQ, float>(d.bcs, -nb, tstage, x, y, nx, ny, qM, qP);
+    }
+    float qMc[M];
+#pragma unroll
+    for (int f = 0; f < M; ++f) qMc[f] = qM[f];
+    return P::numflux(d.eqp, nx, ny, qMc, qP, nf, &err);
+  };
 
   const int ntiles = (d.K + E - 1) / E;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -250,7 +285,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         *(float4*)(Ah + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
         *(float4*)(Al + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
       }
-      QB[128 * kind + r] = (float)qbar;
+      QB[128 * kind + r] = qbar;
+      QF[128 * kind + r] = (float)qbar;
       if (kind == 0 && valid && f == 0) {
         const int k = k0 + e;
 #pragma unroll
@@ -299,23 +335,28 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     if (!umma::mbar_wait_bounded(umma::smem_u32(mbar), phA & 1)) *abort_flag = 1;
     phA++;
     umma::fence_after_sync();
-    // ---- cubature values ST[c][row]; g = 0 traces G0 (own faces, then partners)
-    if (tid < 128) {
-      const float qb = QB[rr];
+    // ---- staged cubature values (first wave) and the g = 0 traces, as
+    // deviations; the means are added in the precision of use
+    auto stage_wave = [&](int c_begin) {
+      if (tid < 128) {
 #pragma unroll 1
-      for (int c0 = 0; c0 < C::NC16; c0 += 16) {
-        float v[16];
-        umma::tmem_ld16(tlane + C::T_D1 + c0, v);
-        umma::tmem_wait_ld();
+        for (int c0 = 0; c0 < SR && c_begin + c0 < NC; c0 += 16) {
+          float v[16];
+          umma::tmem_ld16(tlane + C::T_D1 + c_begin + c0, v);
+          umma::tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) ST[(c0 + j) * 128 + rr] = qb + v[j];
+          for (int j = 0; j < 16; ++j) ST[(c0 + j) * 128 + rr] = v[j];
+        }
       }
+    };
+    stage_wave(0);
+    if (tid < 128) {
 #pragma unroll 1
       for (int fc = 0; fc < 3; ++fc) {
         float v[16];
         umma::tmem_ld16(tlane + C::T_D1 + C::NC8 + fc * NG, v);
         umma::tmem_wait_ld();
-        G0[fc * 128 + rr] = qb + v[0];
+        G0[fc * 128 + rr] = v[0];
       }
     } else if (tid < 256) {
       // the partner's g = 0 is its last Gauss point (reversed order)
@@ -324,64 +365,51 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         float v[16];
         umma::tmem_ld16(tlane + C::T_D3 + fc * C::N3, v);
         umma::tmem_wait_ld();
-        G0[(3 + fc) * 128 + rr] = QB[128 * (1 + fc) + rr] + v[NG - 1];
+        G0[(3 + fc) * 128 + rr] = v[NG - 1];
       }
     }
     __syncthreads();
     if (*abort_flag) break;
-    // ---- pointwise physics -------------------------------------------------------
-    auto flux_RS = [&](int e, const float* qc, float* Rv, float* Sv) {
-      float F[M], G[M];
-      P::flux2(d.eqp, qc, F, G, &err);
-      const float4 g = *(const float4*)(GEO + e * 16);
-#pragma unroll
-      for (int f = 0; f < M; ++f) {
-        Rv[f] = g.x * F[f] + g.y * G[f];
-        Sv[f] = g.z * F[f] + g.w * G[f];
-      }
-    };
-    // surface value -(L f*) / J before the contraction: f* sJ / J times -w_g
-    auto face_val = [&](int e, int fc, int g, const float* qM, float* qP, float* val, bool lam) {
-      const float* G = GEO + e * 16;
-      const float nx = G[5 + fc], ny = G[8 + fc];
-      const int nb = CN[e * 6 + 2 * fc];
-      if (nb < 0) {
-        const ElemGeo& geo = d.geo[k0 + e];
-        const double z = d.gz[g];
-        double r, s;
-        if (fc == 0) { r = z; s = -1.0; }
-        else if (fc == 1) { r = -z; s = z; }
-        else { r = -1.0; s = -z; }
-        const double x = 0.5 * (-geo.vx[0] * (r + s) + geo.vx[1] * (1. + r) + geo.vx[2] * (1. + s));
-        const double y = 0.5 * (-geo.vy[0] * (r + s) + geo.vy[1] * (1. + r) + geo.vy[2] * (1. + s));
-        apply_bc<EQ, float>(d.bcs, -nb, tstage, x, y, nx, ny, qM, qP);
-      }
-      float qMc[M], nf[M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) qMc[f] = qM[f];
-      const float l = P::numflux(d.eqp, nx, ny, qMc, qP, nf, &err);
-      if (lam) lmax = fabsf(l) > lmax ? fabsf(l) : lmax;
-      const float w = -(float)d.gw[g] * G[11 + fc];
-#pragma unroll
-      for (int f = 0; f < M; ++f) val[f] = nf[f] * w;
-    };
-    // reference values: R(0), S(0) and each face's value at its first Gauss point
+    // ---- point-0 references.  The fp32 values are what every other point's
+    // deviation is taken from (so a uniform state has zero deviations); the
+    // float64 constants multiply the operator row sums with float64 metrics
+    // and normals, which keeps a uniform flow exactly steady.
     for (int it = tid; it < ne * 4; it += kMixThreads) {
-      const int e = it >> 2, kind = it & 3, rowb = rowb_of(e);
+      const int e = it >> 2, kind = it & 3, rowb = rowb_of(e), k = k0 + e;
+      const ElemGeo& geo = d.geo[k];
+      float* p0 = P0 + e * 5 * M;
       if (kind == 0) {
-        float qc[M], Rv[M], Sv[M];
-        load_fields<M>(ST + rowb, qc);
-        flux_RS(e, qc, Rv, Sv);
+        float qc[M], F[M], G[M];
 #pragma unroll
-        for (int f = 0; f < M; ++f) { Rb[e * 2 * M + f] = Rv[f]; Rb[e * 2 * M + M + f] = Sv[f]; }
+        for (int f = 0; f < M; ++f) qc[f] = QF[rowb + f] + ST[rowb + f];
+        flux32(qc, F, G);
+#pragma unroll
+        for (int f = 0; f < M; ++f) {
+          p0[f] = F[f];
+          p0[M + f] = G[f];
+          Rb[e * 2 * M + f] = geo.rx * (double)F[f] + geo.ry * (double)G[f];
+          Rb[e * 2 * M + M + f] = geo.sx * (double)F[f] + geo.sy * (double)G[f];
+        }
       } else {
         const int fc = kind - 1;
-        float qM[M], qP[M], val[M];
+        float qM[M], qP[M], nf[M];
 #pragma unroll
-        for (int f = 0; f < M; ++f) { qM[f] = G0[fc * 128 + rowb + f]; qP[f] = G0[(3 + fc) * 128 + rowb + f]; }
-        face_val(e, fc, 0, qM, qP, val, false);
+        for (int f = 0; f < M; ++f) {
+          qM[f] = QF[rowb + f] + G0[fc * 128 + rowb + f];
+          qP[f] = QF[128 * (1 + fc) + rowb + f] + G0[(3 + fc) * 128 + rowb + f];
+        }
+        numflux32(e, k, fc, 0, qM, qP, nf);
+        // float64 flux of the same fp32 traces with float64 normals
+        double dM[M], dP[M], nf64[M];
 #pragma unroll
-        for (int f = 0; f < M; ++f) Fb[(e * 3 + fc) * M + f] = val[f];
+        for (int f = 0; f < M; ++f) { dM[f] = qM[f]; dP[f] = qP[f]; }
+        P::numflux(d.eqp, geo.nx[fc], geo.ny[fc], dM, dP, nf64, &err);
+        const double w = -geo.sJ[fc] * geo.invJ;
+#pragma unroll
+        for (int f = 0; f < M; ++f) {
+          p0[(2 + fc) * M + f] = nf[f];
+          Fb[(e * 3 + fc) * M + f] = nf64[f] * w;
+        }
       }
     }
     __syncthreads();
@@ -412,55 +440,42 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         umma::commit(umma::smem_u32(mbar + 1 + b));
       }
     };
-    {
-      // each thread keeps one (element, point-in-chunk) through the volume chunks
-      const int it = tid;
-      const bool act = it < ne * VPC;
-      const int e = act ? it / VPC : 0, cp = act ? it - e * VPC : 0, rowb = rowb_of(e);
-      float rb[M], sb[M];
-      if (act) {
+    // volume: deviation of the fp32 flux from its point-0 value, times the metric
+    auto vol_item = [&](int e, int cp, int c, unsigned char* bh, unsigned char* bl) {
+      const int rowb = rowb_of(e);
+      const float* p0 = P0 + e * 5 * M;
+      float qc[M], F[M], G[M];
+      load_fields<M>(ST + (c % SR) * 128 + rowb, qc);
 #pragma unroll
-        for (int f = 0; f < M; ++f) { rb[f] = Rb[e * 2 * M + f]; sb[f] = Rb[e * 2 * M + M + f]; }
+      for (int f = 0; f < M; ++f) qc[f] += QF[rowb + f];
+      flux32(qc, F, G);
+      const float4 g = *(const float4*)(GEO + e * 16);
+#pragma unroll
+      for (int f = 0; f < M; ++f) {
+        const float dF = F[f] - p0[f], dG = G[f] - p0[M + f];
+        float h0, l0, h1, l1;
+        split_trunc(g.x * dF + g.y * dG, h0, l0);
+        split_trunc(g.z * dF + g.w * dG, h1, l1);
+        const uint32_t off = umma::kmajor_offset(rowb + f, 2 * cp, KV);
+        *(float2*)(bh + off) = make_float2(h0, h1);
+        *(float2*)(bl + off) = make_float2(l0, l1);
       }
-      for (int ch = 0; ch < C::NV; ++ch) {
-        const int b = chunk_counter++ % C::NBUF;
-        claim(b);
-        unsigned char* bh = U + b * 2 * C::SZ_CH;
-        unsigned char* bl = bh + C::SZ_CH;
-        const int c = ch * VPC + cp;
-        if (act && c < NC) {
-          float qc[M], Rv[M], Sv[M];
-          load_fields<M>(ST + c * 128 + rowb, qc);
-          flux_RS(e, qc, Rv, Sv);
-#pragma unroll
-          for (int f = 0; f < M; ++f) {
-            float h0, l0, h1, l1;
-            split_trunc(Rv[f] - rb[f], h0, l0);
-            split_trunc(Sv[f] - sb[f], h1, l1);
-            const uint32_t off = umma::kmajor_offset(rowb + f, 2 * cp, KV);
-            *(float2*)(bh + off) = make_float2(h0, h1);
-            *(float2*)(bl + off) = make_float2(l0, l1);
-          }
-        }
-        // elements beyond one item per thread (more than 384 items per chunk)
-        for (int it2 = tid + kMixThreads; it2 < ne * VPC; it2 += kMixThreads) {
-          const int e2 = it2 / VPC, cp2 = it2 - e2 * VPC, c2 = ch * VPC + cp2, rowb2 = rowb_of(e2);
-          if (c2 >= NC) continue;
-          float qc[M], Rv[M], Sv[M];
-          load_fields<M>(ST + c2 * 128 + rowb2, qc);
-          flux_RS(e2, qc, Rv, Sv);
-#pragma unroll
-          for (int f = 0; f < M; ++f) {
-            float h0, l0, h1, l1;
-            split_trunc(Rv[f] - Rb[e2 * 2 * M + f], h0, l0);
-            split_trunc(Sv[f] - Rb[e2 * 2 * M + M + f], h1, l1);
-            const uint32_t off = umma::kmajor_offset(rowb2 + f, 2 * cp2, KV);
-            *(float2*)(bh + off) = make_float2(h0, h1);
-            *(float2*)(bl + off) = make_float2(l0, l1);
-          }
-        }
-        issue_chunk(b, ch * (KV / 4) * umma::kLBO, KV / 8, ch == 0);
+    };
+    for (int ch = 0; ch < C::NV; ++ch) {
+      if (ch > 0 && (ch * VPC) % SR == 0) {
+        // next staging wave (the previous chunk's items are done: issue barrier)
+        stage_wave(ch * VPC);
+        __syncthreads();
       }
+      const int b = chunk_counter++ % C::NBUF;
+      claim(b);
+      unsigned char* bh = U + b * 2 * C::SZ_CH;
+      unsigned char* bl = bh + C::SZ_CH;
+      for (int it = tid; it < ne * VPC; it += kMixThreads) {
+        const int e = it / VPC, cp = it - e * VPC, c = ch * VPC + cp;
+        if (c < NC) vol_item(e, cp, c, bh, bl);
+      }
+      issue_chunk(b, ch * (KV / 4) * umma::kLBO, KV / 8, ch == 0);
     }
     for (int fc = 0; fc < 3; ++fc) {
       // own (rows 0..NG-1) and partner (rows 16..16+NG-1) traces of this face
@@ -468,14 +483,14 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         float v[16];
         umma::tmem_ld16(tlane + C::T_D1 + C::NC8 + fc * NG, v);
         umma::tmem_wait_ld();
-        const float qb = QB[rr];
+        const float qb = QF[rr];
 #pragma unroll
         for (int j = 0; j < NG; ++j) ST[j * 128 + rr] = qb + v[j];
       } else if (tid < 256) {
         float v[16];
         umma::tmem_ld16(tlane + C::T_D3 + fc * C::N3, v);
         umma::tmem_wait_ld();
-        const float qbn = QB[128 * (1 + fc) + rr];
+        const float qbn = QF[128 * (1 + fc) + rr];
 #pragma unroll
         for (int j = 0; j < NG; ++j) ST[(16 + j) * 128 + rr] = qbn + v[NG - 1 - j];
       }
@@ -485,15 +500,21 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       unsigned char* bh = U + b * 2 * C::SZ_CH;
       unsigned char* bl = bh + C::SZ_CH;
       for (int it = tid; it < ne * NG; it += kMixThreads) {
-        const int e = it / NG, g = it - e * NG, rowb = rowb_of(e);
-        float qM[M], qP[M], val[M];
+        const int e = it / NG, g = it - e * NG, rowb = rowb_of(e), k = k0 + e;
+        float qM[M], qP[M], nf[M];
         load_fields<M>(ST + g * 128 + rowb, qM);
         load_fields<M>(ST + (16 + g) * 128 + rowb, qP);
-        face_val(e, fc, g, qM, qP, val, want_lambda);
+        const float lam = numflux32(e, k, fc, g, qM, qP, nf);
+        if (want_lambda) {
+          const double l = fabs((double)lam);
+          lmax = l > lmax ? l : lmax;
+        }
+        const float w = -GEO[e * 16 + 11 + fc];
+        const float* p0 = P0 + e * 5 * M + (2 + fc) * M;
 #pragma unroll
         for (int f = 0; f < M; ++f) {
           float h, l;
-          split_trunc(val[f] - Fb[(e * 3 + fc) * M + f], h, l);
+          split_trunc(w * (nf[f] - p0[f]), h, l);
           const uint32_t off = umma::kmajor_offset(rowb + f, g, KV);
           *(float*)(bh + off) = h;
           *(float*)(bl + off) = l;
@@ -545,11 +566,10 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   if (want_lambda) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      const float v = __shfl_xor_sync(0xffffffffu, lmax, o);
+      const double v = __shfl_xor_sync(0xffffffffu, lmax, o);
       lmax = v > lmax ? v : lmax;
     }
-    if (lane == 0 && lmax > 0.f)
-      atomicMax(&d.st->lam_bits, (unsigned long long)__double_as_longlong((double)lmax));
+    if (lane == 0 && lmax > 0.0) atomicMax(&d.st->lam_bits, (unsigned long long)__double_as_longlong(lmax));
   }
   if (err) atomicOr(&d.st->err, err);
   umma::fence_before_sync();
@@ -639,7 +659,7 @@ MixedPlan* mixed_create(int eq, const RefOps& o, int K, int M) {
       rs[i * 5 + 1] += o.DsW(i, c);
     }
     for (int fc = 0; fc < 3; ++fc)
-      for (int g = 0; g < o.Ng; ++g) rs[i * 5 + 2 + fc] += o.Lift(i, fc * o.Ng + g);
+      for (int g = 0; g < o.Ng; ++g) rs[i * 5 + 2 + fc] += o.Lift(i, fc * o.Ng + g) * o.gw[g];
   }
   if (o.rot.empty() || cudaMalloc((void**)&p->rowsum, rs.size() * sizeof(double)) != cudaSuccess ||
       cudaMalloc((void**)&p->rot, o.rot.size() * sizeof(int)) != cudaSuccess) {

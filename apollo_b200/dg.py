@@ -17,7 +17,8 @@ import numpy as np
 from .mesh import Mesh
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libapollo_dg.so")
+# APOLLO_DG_LIB selects another build of the library (e.g. an instrumented one)
+LIB_PATH = os.environ.get("APOLLO_DG_LIB", os.path.join(_HERE, "lib", "libapollo_dg.so"))
 
 APOLLO_HOST_PTR, APOLLO_DEVICE_PTR = 0, 1
 PREC = {"fp64": 0, "mixed": 1}
