@@ -39,7 +39,10 @@ struct apollo_dg {
   std::vector<int> conn_h;
   double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
          *gw_d = nullptr, *wmass_d = nullptr;
-  double *U_d = nullptr, *W_d = nullptr, *W2_d = nullptr, *in_d = nullptr, *out_d = nullptr;
+  double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
+  // mixed precision: fp32 face traces of U (TU) and of the stage states (T0, T1)
+  float *TU_d = nullptr, *T0_d = nullptr, *T1_d = nullptr;
+  bool tu_valid = false;
   double *vol_d = nullptr, *trace_d = nullptr, *flux_d = nullptr;
   DevState* st_d = nullptr;
   DevState* st_h = nullptr;  // pinned
@@ -88,7 +91,9 @@ void free_mesh(apollo_dg* h) {
   dfree(h->geo_d); dfree(h->faces_d); dfree(h->conn_d);
   dfree(h->V_d); dfree(h->Dr_d); dfree(h->Ds_d); dfree(h->I_d); dfree(h->L_d); dfree(h->gz_d); dfree(h->gw_d);
   dfree(h->wmass_d);
-  dfree(h->U_d); dfree(h->W_d); dfree(h->W2_d); dfree(h->in_d); dfree(h->out_d);
+  dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
+  dfree(h->TU_d); dfree(h->T0_d); dfree(h->T1_d);
+  h->tu_valid = false;
   dfree(h->vol_d); dfree(h->trace_d); dfree(h->flux_d);
   if (h->mixed) { mixed_destroy(h->mixed); h->mixed = nullptr; }
   h->have_state = false;
@@ -139,7 +144,9 @@ apollo_status enqueue_stage(apollo_dg* h, const StageArgs& a, apollo_precision p
   cudaError_t e;
   if (prec == APOLLO_PREC_MIXED) {
     if (!h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision is not available for this equation/order");
-    e = mixed_launch_rhs(h->mixed, h->eq, d, a, h->stream, ev);
+    StageArgs am = a;
+    if (am.mode == MODE_RHS) am.tr_scratch = h->T0_d;
+    e = mixed_launch_rhs(h->mixed, h->eq, d, am, h->stream, ev);
   } else {
     e = launch_rhs_fp64(h->eq, d, a, h->stream, ev);
   }
@@ -149,29 +156,28 @@ apollo_status enqueue_stage(apollo_dg* h, const StageArgs& a, apollo_precision p
 
 apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
   const int s = 5;
-  // The float64 kernels read neighbour data only in the volume/face kernels,
-  // before the LIFT kernel writes, so their stages update W in place.  The
-  // fused mixed kernel reads neighbour states while other CTAs write, so its
-  // stages alternate between W and W2.
-  const bool pingpong = prec == APOLLO_PREC_MIXED;
-  double* last = h->W_d;
+  // Stages update W in place: the float64 kernels read neighbour data only in
+  // the volume/face kernels, before the LIFT kernel writes, and the mixed
+  // kernel reads only its own elements' state plus the face traces of the
+  // previous stage, which alternate between T0 and T1 (TU holds those of U).
   for (int i = 0; i < s; ++i) {
     StageArgs a{};
     a.time_from_state = 1;
     a.reset_lambda = 1;
     if (i < s - 1) {
-      a.x = i == 0 ? h->U_d : last;
-      a.out = (pingpong && (i & 1)) ? h->W2_d : h->W_d;
-      last = a.out;
+      a.x = i == 0 ? h->U_d : h->W_d;
+      a.out = h->W_d;
       a.mode = MODE_STAGE;
       a.frac = i / (s - 1.);
     } else {
-      a.x = last;
+      a.x = h->W_d;
       a.u0 = h->U_d;
       a.out = h->U_d;
       a.mode = MODE_FINAL;
       a.frac = 1.0;
     }
+    a.tr_in = i == 0 ? h->TU_d : (i & 1) ? h->T0_d : h->T1_d;
+    a.tr_out = i == s - 1 ? h->TU_d : (i & 1) ? h->T1_d : h->T0_d;
     apollo_status r = enqueue_stage(h, a, prec);
     if (r != APOLLO_OK) return r;
   }
@@ -183,6 +189,13 @@ apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
 
 apollo_status step_graph(apollo_dg* h, apollo_precision prec, cudaGraphExec_t* out) {
   int gi = prec == APOLLO_PREC_MIXED ? 1 : 0;
+  // the mixed step starts from the face traces of U; a float64 step leaves them stale
+  if (prec == APOLLO_PREC_MIXED && h->mixed && !h->tu_valid) {
+    DgDev d = make_dev(h);
+    CK(mixed_launch_traces(h->mixed, d, h->U_d, h->TU_d, h->stream), "trace launch");
+    h->tu_valid = true;
+  }
+  if (prec != APOLLO_PREC_MIXED) h->tu_valid = false;
   if (!h->graph[gi]) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -384,7 +397,6 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
   CK(upload(&h->wmass_d, o.mass_colsum.data(), o.mass_colsum.size()), "op upload");
   CK(cudaMalloc((void**)&h->U_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->W_d, nU * sizeof(double)), "state alloc");
-  CK(cudaMalloc((void**)&h->W2_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->in_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->out_d, nU * sizeof(double)), "state alloc");
   CK(cudaMalloc((void**)&h->vol_d, nU * sizeof(double)), "scratch alloc");
@@ -393,6 +405,12 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
   CK(cudaMemset(h->U_d, 0, nU * sizeof(double)), "state clear");
   h->K = K;
   h->mixed = mixed_create(h->eq, o, K, h->M);
+  if (h->mixed) {
+    const size_t nTr = (size_t)K * o.Nf * M;
+    CK(cudaMalloc((void**)&h->TU_d, nTr * sizeof(float)), "trace alloc");
+    CK(cudaMalloc((void**)&h->T0_d, nTr * sizeof(float)), "trace alloc");
+    CK(cudaMalloc((void**)&h->T1_d, nTr * sizeof(float)), "trace alloc");
+  }
   return APOLLO_OK;
 }
 
@@ -420,6 +438,7 @@ apollo_status apollo_dg_set_state(apollo_dg* h, const double* U, int where) {
                      h->stream), "set state");
   CK(cudaStreamSynchronize(h->stream), "set state");
   h->have_state = true;
+  h->tu_valid = false;
   return APOLLO_OK;
 }
 

@@ -5,20 +5,22 @@
 // (32 / M elements each, so an element never straddles two warps).  Every
 // contraction runs on the tensor cores as kind::tf32 with a three-term split
 // (hi*hi + hi*lo + lo*hi, fp32 accumulation in TMEM) and acts only on
-// deviations from a float64 reference value per element and field:
+// deviations from float64 reference values:
 //
-//   q  = qbar + dq          qbar = nodal mean            (float64)
-//   V q      = qbar + V dq                  (cubature values)
-//   I q      = qbar + I dq                  (own face traces)
-//   I q_nb   = qbar_nb + I dq_nb            (neighbour traces, recomputed from
-//                                            the neighbour's state in L2)
-//   Dr R     = (Dr 1) R(0) + Dr (R - R(0))  (R = rx F + ry G at cubature points)
-//   L f*     = sum_f (L_f 1) f*_f(0) + L (f* - f*_f(0))
+//   V q        = qbar + V (q - qbar)              (cubature values; qbar = nodal mean)
+//   Dr R + Ds S = (Dr 1) R(qbar) + (Ds 1) S(qbar)
+//               + Dr (R - R(qbar)) + Ds (S - S(qbar))   (R = rx F + ry G, S = sx F + sy G)
+//   L f*       = sum_f (L_f w 1) f*_f(qbar) + L w (f* - f*_f(qbar))
 //
-// so the low-precision products see only the element-local fluctuation.  The
-// pointwise flux and the Lax-Friedrichs face flux are fp32; the state, the
-// reference values, the operator row sums, the stage accumulation, the dt
-// reduction (float64 wave speed, last stage only) stay float64.
+// The reference fluxes are evaluated from the same fp32 mean as the pointwise
+// fluxes, so a uniform state has exactly zero deviations, and their float64
+// counterparts (float64 metrics and normals) multiply float64 operator row
+// sums.  Face traces are not recomputed from the neighbours' states: every
+// stage that produces a state also writes its fp32 face traces
+//   trace = float(mean) + I float(q - mean)            [K][3][NG][M]
+// (k_mixed_traces computes the same values from any state), and the next
+// stage reads its own and its partners' traces from that buffer.  A stage
+// therefore reads only its own elements' state, so it may update in place.
 //
 // Apollo: the RHS of wxnodaldg2dmethod.cc:235-542 (volume :346-380, traces and
 // partner gather :389-440, numerical flux :442-469, surface integral and M^-1/J
@@ -32,69 +34,81 @@ namespace apollo {
 
 struct MixedPlan {
   int eq = 0, N = 0, M = 0;
-  double* rowsum = nullptr;  // [NP][5]: Dr 1, Ds 1, L_0 1, L_1 1, L_2 1 (float64)
-  int* rot = nullptr;        // [3][NP] node permutations rotating face k onto face 0
+  double* rowsum = nullptr;  // [NP][5]: Dr 1, Ds 1, L_0 w 1, L_1 w 1, L_2 w 1 (float64)
 };
 
 namespace {
 
 constexpr int kMixThreads = 384;
 constexpr int round_up_c(int x, int m) { return (x + m - 1) / m * m; }
-constexpr int max_c(int a, int b) { return a > b ? a : b; }
+constexpr int tmem_cols(int x) { return x <= 32 ? 32 : x <= 64 ? 64 : x <= 128 ? 128 : x <= 256 ? 256 : 512; }
 
 template <int N, int M> struct MixCfg {
   static constexpr int NP = Sizes<N>::NP, NC = Sizes<N>::NC, NG = Sizes<N>::NG, NF = Sizes<N>::NF;
   static constexpr int EPQ = 32 / M;  // elements per warp quadrant
   static constexpr int E = 4 * EPQ;   // elements per tile
   static constexpr int K1 = round_up_c(NP, 8);
-  static constexpr int VPC = 12;                      // cubature points per volume chunk
-  static constexpr int KV = 2 * VPC;                  // K columns per volume chunk (R, S)
+  static constexpr int KV = N >= 5 ? 16 : 32;         // K columns per chunk
+  static constexpr int VPC = KV / 2;                  // cubature points per volume chunk (R, S each)
   static constexpr int NV = (NC + VPC - 1) / VPC;     // volume chunks
-  static constexpr int NC8 = round_up_c(NC, 8);       // first Gauss-point row of B1
+  static constexpr int NFK = round_up_c(NF, 8);       // face columns (fc NG + g, packed)
+  static constexpr int NFC = (NFK + KV - 1) / KV;     // face chunks
+  static constexpr int NCH = NV + NFC;
   static constexpr int NC16 = round_up_c(NC, 16);
-  static constexpr int NI = round_up_c(NF, 16);
-  static constexpr int NA = round_up_c(NC8 + NI, 16);
-  static constexpr int N3 = 16;                       // neighbour traces: face 0 of the rotated data
   static constexpr int NPN = round_up_c(NP, 16);
-  static constexpr int KB2 = NV * KV + 3 * 16;        // then one 16-column chunk per face
-  static constexpr int NBUF = 3;
-  // TMEM columns
-  static constexpr int T_D1 = 0, T_D3 = NA, T_D2 = NA + 3 * N3;
-  static constexpr int TUSED = T_D2 + NPN;
-  static constexpr int TCOLS = TUSED <= 64 ? 64 : TUSED <= 128 ? 128 : TUSED <= 256 ? 256 : 512;
+  static constexpr int KB2 = NCH * KV;
+  static constexpr int NBUF = 2;
+  static constexpr int NWORK = kMixThreads - 32;      // worker threads; the last warp issues MMAs and copies
+  // TMEM columns: cubature values, then the right-hand side
+  static constexpr int T_D1 = 0, T_D2 = NC16;
+  static constexpr int TCOLS = tmem_cols(NC16 + NPN);
+  // K-major operand strides (bytes between 8-row groups)
+  static constexpr int SBO1 = K1 * 32;       // B1 = V and the A operand
+  static constexpr int SBO2 = KB2 * 32;      // B2 = [Dr Ds | L w]
+  static constexpr int SBOC = KV * 32 + 16;  // chunk operands, staggered across banks
   // shared memory, bytes (each operand as a tf32 hi half and lo half)
-  static constexpr int SZ_B1 = NA * K1 * 4;
-  static constexpr int SZ_B2 = NPN * KB2 * 4;
-  static constexpr int SZ_A1 = 128 * K1 * 4;
-  static constexpr int SZ_CH = 128 * KV * 4;
-  static constexpr int SZ_U = max_c(8 * SZ_A1, NBUF * 2 * SZ_CH);
-  static constexpr int SR = 48;  // cubature points staged at a time (a multiple of VPC)
-  static constexpr int SZ_ST = max_c(SR, 32) * 128 * 4;
+  static constexpr int SZ_B1 = (NC16 / 8) * SBO1;
+  static constexpr int SZ_B2 = (NPN / 8) * SBO2;
+  static constexpr int SZ_A = 16 * SBO1;
+  static constexpr int SZ_CH = 16 * SBOC;
+  static constexpr int SZ_ST = NC * 128 * 4;  // cubature deviations [NC][128] float
+  static constexpr int SZ_XD = NP * 128 * 4;  // result deviations [NP][128] float
+  static constexpr int XS_N = E * NP * M;     // one tile's state, doubles
+  // per-tile data, two slots (tile parity)
+  static constexpr int TD_GEO = 0;                         // [14][E] float: rx ry sx sy, nx[3] ny[3] -sJ/J[3] at 5..13
+  static constexpr int TD_CN = TD_GEO + 14 * E * 4;        // [E][6] int
+  static constexpr int TD_QF = TD_CN + E * 6 * 4;          // [M][E] float own means
+  static constexpr int TD_P0 = TD_QF + M * E * 4;          // [5M][E] float F, G, f*_fc at the mean
+  static constexpr int TD_RB = round_up_c(TD_P0 + 5 * M * E * 4, 8);  // [2M][E] double R, S at the mean
+  static constexpr int TD_FB = TD_RB + 2 * M * E * 8;      // [3M][E] double face references
+  static constexpr int SZ_TD = TD_FB + 3 * M * E * 8;
   static constexpr int O_B1H = 0, O_B1L = O_B1H + SZ_B1;
   static constexpr int O_B2H = O_B1L + SZ_B1, O_B2L = O_B2H + SZ_B2;
-  static constexpr int O_U = round_up_c(O_B2L + SZ_B2, 128);
-  static constexpr int O_ST = O_U + SZ_U;
-  static constexpr int O_G0 = O_ST + SZ_ST;                // g = 0 traces: [6][128] float
-  static constexpr int O_GEO = O_G0 + 6 * 128 * 4;         // [E][16] float
-  static constexpr int O_RS = O_GEO + E * 16 * 4;          // operator row sums [NP][5] double
-  static constexpr int O_RB = O_RS + NP * 5 * 8;           // R(0), S(0): [E][2M] double
-  static constexpr int O_FB = O_RB + E * 2 * M * 8;        // face references: [E][3][M] double
-  static constexpr int O_RBH = O_FB + E * 3 * M * 8;       // fp32 point-0 fluxes F, G, face f*: [E][5M]
-  static constexpr int O_CN = O_RBH + E * 5 * M * 4;       // [E][6] int
-  static constexpr int O_QB = O_CN + E * 6 * 4;            // means: own [128], neighbours [3][128] double
-  static constexpr int O_QF = O_QB + 4 * 128 * 8;          // the same means as float
-  static constexpr int O_ROT = O_QF + 4 * 128 * 4;         // [3][NP] int
-  static constexpr int O_MB = round_up_c(O_ROT + 3 * NP * 4, 8);  // mbarriers: A, ring[NBUF]
-  static constexpr int O_TS = O_MB + 8 * (1 + NBUF);       // TMEM base, abort flag
+  static constexpr int O_A = round_up_c(O_B2L + SZ_B2, 128);
+  static constexpr int O_RING = O_A + 2 * SZ_A;
+  static constexpr int O_ST = O_RING + NBUF * 2 * SZ_CH;
+  static constexpr int O_XD = O_ST + SZ_ST;
+  static constexpr int O_XS = round_up_c(O_XD + SZ_XD, 16);
+  static constexpr int O_IF = O_XS + XS_N * 8;                      // [NF][NP] float interpolation
+  static constexpr int O_RS = round_up_c(O_IF + NF * NP * 4, 8);    // [NP][5] double row sums
+  static constexpr int O_TD = O_RS + NP * 5 * 8;                    // 2 slots of per-tile data
+  static constexpr int O_XB = O_TD + 2 * SZ_TD;                     // [128] double means of the result
+  // mbarriers: state copy, A operand, GEMM-A done, tile RHS done, ring full[NBUF], ring empty[NBUF], drain
+  static constexpr int O_MB = O_XB + 128 * 8;
+  static constexpr int NMB = 5 + 2 * NBUF;
+  static constexpr int O_TS = O_MB + 8 * NMB;                       // TMEM base, abort flag
   static constexpr int BYTES = O_TS + 16;
   static constexpr bool FITS = BYTES <= 227 * 1024;
-  static_assert(NG <= 16, "one 16-column chunk per face");
+  static_assert(KV % 16 == 0 && SZ_TD % 8 == 0, "layout");
 };
 
-// tf32 split, both halves rounded to nearest: x = hi + lo + O(2^-22 |x|).
-__device__ __forceinline__ void split_trunc(float x, float& h, float& l) {
-  h = umma::to_tf32(x);
-  l = umma::to_tf32(x - h);
+// tf32 split of a per-point operand: hi keeps the top 19 bits of x, lo = x - hi
+// is exact in fp32 and the tensor core reads its top 19 bits, so
+// x = hi + lo + O(2^-21 |x|).  (The operators are split once per CTA with
+// rounding to nearest.)
+__device__ __forceinline__ void split_tf32(float x, float& h, float& l) {
+  h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+  l = x - h;
 }
 
 template <int M>
@@ -108,428 +122,478 @@ __device__ __forceinline__ void load_fields(const float* p, float* v) {
   }
 }
 
+// Face traces of one (element, field) row: for the NG Gauss points of face fc,
+// float(m) + sum_j I[fc NG + g][j] dv[j], fp32 fused multiply-adds in node
+// order.  Both the stage epilogue and k_mixed_traces call this, so the values
+// agree bit for bit for the same state.
+template <int NP, int NG>
+__device__ __forceinline__ void row_traces(const float* __restrict__ IF, const float* dv, int dstride, double m, int fc,
+                                           float* __restrict__ dst, int M) {
+  const float mf = (float)m;
+#pragma unroll 2
+  for (int g = 0; g < NG; ++g) {
+    const float* Ig = IF + (fc * NG + g) * NP;
+    float acc = 0.f;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) acc = fmaf(Ig[j], dv[j * dstride], acc);
+    dst[g * M] = mf + acc;
+  }
+}
+
+template <int NP>
+__device__ __forceinline__ double nodal_mean(const double* v) {
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < NP; ++j) s += v[j];
+  return s * (1.0 / NP);
+}
+
+// Worker-only barrier (named barrier 1; the control warp does not take part).
+template <int NW>
+__device__ __forceinline__ void workers_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(NW) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
+// Stage kernel.  Warps 0..10 are workers, warp 11 is the control warp: its
+// lane 0 issues every tcgen05 MMA and bulk copy.  Per tile the workers build
+// the A operand (state deviations), stage GEMM-A's cubature values, produce
+// the chunk operands of GEMM-B into a two-buffer ring (full/empty mbarriers),
+// and finish with the float64 epilogue and the result's face traces.  The
+// next tile's operand build and GEMM-A overlap this tile's epilogue; per-tile
+// data live in two slots by tile parity.
 template <int EQ, int N>
 __global__ void __launch_bounds__(kMixThreads, 1)
-    k_mixed_stage(DgDev d, StageArgs a, const double* __restrict__ rowsum, const int* __restrict__ rot) {
+    k_mixed_stage(DgDev d, StageArgs a, const double* __restrict__ rowsum, int flags) {
   using P = Eq<EQ>;
   constexpr int M = P::M;
   using C = MixCfg<N, M>;
   constexpr int NP = C::NP, NC = C::NC, NG = C::NG, NF = C::NF, EPQ = C::EPQ, E = C::E, K1 = C::K1;
-  constexpr int VPC = C::VPC, KV = C::KV, SR = C::SR;
-  static_assert(SR % VPC == 0 && SR % 16 == 0, "staging waves hold whole chunks");
+  constexpr int KV = C::KV, VPC = C::VPC, NV = C::NV, NW = C::NWORK, NBUF = C::NBUF;
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* B1h = sm + C::O_B1H;
   unsigned char* B1l = sm + C::O_B1L;
   unsigned char* B2h = sm + C::O_B2H;
   unsigned char* B2l = sm + C::O_B2L;
-  unsigned char* U = sm + C::O_U;
+  unsigned char* AOP = sm + C::O_A;
+  unsigned char* RING = sm + C::O_RING;
   float* ST = (float*)(sm + C::O_ST);
-  float* G0 = (float*)(sm + C::O_G0);
-  float* GEO = (float*)(sm + C::O_GEO);
+  float* XD = (float*)(sm + C::O_XD);
+  const double* XS = (const double*)(sm + C::O_XS);
+  float* IF = (float*)(sm + C::O_IF);
   double* RSUM = (double*)(sm + C::O_RS);
-  double* Rb = (double*)(sm + C::O_RB);   // [E][2M]: R(0), S(0) in float64
-  double* Fb = (double*)(sm + C::O_FB);   // [E][3][M]: face references in float64
-  float* P0 = (float*)(sm + C::O_RBH);    // [E][5M]: fp32 F(0), G(0), f*_fc(0)
-  int* CN = (int*)(sm + C::O_CN);
-  double* QB = (double*)(sm + C::O_QB);  // [0..127] own means, [128 (1 + fc) + r] neighbour means
-  float* QF = (float*)(sm + C::O_QF);
-  int* ROT = (int*)(sm + C::O_ROT);
+  double* XB = (double*)(sm + C::O_XB);
   uint64_t* mbar = (uint64_t*)(sm + C::O_MB);
   uint32_t* tslot = (uint32_t*)(sm + C::O_TS);
   volatile int* abort_flag = (volatile int*)(sm + C::O_TS + 4);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool x_bulk = flags & 1, u0_prefetch = flags & 2;
 
-  // ---- once per CTA: operators split into tf32 halves (K-major), zeroed A region
-  for (int i = tid; i < C::NA * K1; i += kMixThreads) {
+  // ---- once per CTA: operators split into tf32 halves (K-major)
+  for (int i = tid; i < C::NC16 * K1; i += kMixThreads) {
     const int r = i / K1, k = i % K1;
-    double v = 0.0;
-    if (k < NP) {
-      if (r < NC) v = d.V[r * NP + k];
-      else if (r >= C::NC8 && r < C::NC8 + NF) v = d.I[(r - C::NC8) * NP + k];
-    }
-    const float h = umma::to_tf32((float)v);
-    const float l = umma::to_tf32((float)(v - (double)h));
-    *(float*)(B1h + umma::kmajor_offset(r, k, K1)) = h;
-    *(float*)(B1l + umma::kmajor_offset(r, k, K1)) = l;
+    const double v = (r < NC && k < NP) ? d.V[r * NP + k] : 0.0;
+    const float h = umma::round_tf32((float)v);
+    const float l = umma::round_tf32((float)(v - (double)h));
+    *(float*)(B1h + umma::kmajor_offset_sbo(r, k, C::SBO1)) = h;
+    *(float*)(B1l + umma::kmajor_offset_sbo(r, k, C::SBO1)) = l;
   }
-  // B2: volume chunks (Dr, Ds at cubature points, weights folded in), then per
-  // face the LIFT columns times the Gauss weights
+  // B2: volume chunks (Dr, Ds at cubature points, weights folded in), then the
+  // face chunks: column fc NG + g is LIFT times the Gauss weight
   for (int i = tid; i < C::NPN * C::KB2; i += kMixThreads) {
     const int r = i / C::KB2, k = i % C::KB2;
     double v = 0.0;
     if (r < NP) {
-      if (k < C::NV * KV) {
+      if (k < NV * KV) {
         const int c = VPC * (k / KV) + (k % KV) / 2;
         if (c < NC) v = (k & 1) ? d.Ds[r * NC + c] : d.Dr[r * NC + c];
       } else {
-        const int kk = k - C::NV * KV, fc = kk / 16, g = kk % 16;
-        if (g < NG) v = d.L[r * NF + fc * NG + g] * d.gw[g];
+        const int col = k - NV * KV;
+        if (col < NF) v = d.L[r * NF + col] * d.gw[col % NG];
       }
     }
-    const float h = umma::to_tf32((float)v);
-    const float l = umma::to_tf32((float)(v - (double)h));
-    *(float*)(B2h + umma::kmajor_offset(r, k, C::KB2)) = h;
-    *(float*)(B2l + umma::kmajor_offset(r, k, C::KB2)) = l;
+    const float h = umma::round_tf32((float)v);
+    const float l = umma::round_tf32((float)(v - (double)h));
+    *(float*)(B2h + umma::kmajor_offset_sbo(r, k, C::SBO2)) = h;
+    *(float*)(B2l + umma::kmajor_offset_sbo(r, k, C::SBO2)) = l;
   }
-  for (int i = tid; i < C::SZ_U / 16; i += kMixThreads) ((float4*)U)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = tid; i < (2 * C::SZ_A + NBUF * 2 * C::SZ_CH) / 16; i += kMixThreads)
+    ((float4*)AOP)[i] = make_float4(0.f, 0.f, 0.f, 0.f);  // A operand and ring: finite padding
+  for (int i = tid; i < NF * NP; i += kMixThreads) IF[i] = (float)d.I[i];
   for (int i = tid; i < NP * 5; i += kMixThreads) RSUM[i] = rowsum[i];
-  for (int i = tid; i < 3 * NP; i += kMixThreads) ROT[i] = rot[i];
+  // mbarriers: 0 state copy, 1 A operand (all workers), 2 GEMM-A done, 3 RHS
+  // done, 4 + b ring buffer b full (all workers), 4 + NBUF + b ring buffer b empty
+  const uint32_t mbX = umma::smem_u32(mbar + 0), mbA = umma::smem_u32(mbar + 1);
+  const uint32_t mbD1 = umma::smem_u32(mbar + 2), mbD2 = umma::smem_u32(mbar + 3);
+  auto mb_full = [&](int b) { return umma::smem_u32(mbar + 4 + b); };
+  auto mb_empty = [&](int b) { return umma::smem_u32(mbar + 4 + NBUF + b); };
+  const uint32_t mbDrain = umma::smem_u32(mbar + 4 + 2 * NBUF);
   if (tid == 0) {
-    for (int b = 0; b < 1 + C::NBUF; ++b) umma::mbar_init(umma::smem_u32(mbar + b), 1);
+    umma::mbar_init(mbDrain, 1);
+    umma::mbar_init(mbX, 1);
+    umma::mbar_init(mbA, NW);
+    umma::mbar_init(mbD1, 1);
+    umma::mbar_init(mbD2, 1);
+    for (int b = 0; b < NBUF; ++b) {
+      umma::mbar_init(mb_full(b), NW);
+      umma::mbar_init(mb_empty(b), 1);
+    }
     *abort_flag = 0;
   }
   if (warp == 0) umma::tmem_alloc(umma::smem_u32(tslot), C::TCOLS);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   umma::fence_proxy_async();
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tb = *tslot;
-  const uint32_t tlane = tb + ((uint32_t)(32 * (warp & 3)) << 16);
-
-  const uint32_t id_A = umma::idesc_tf32(128, C::NA);
-  const uint32_t id_3 = umma::idesc_tf32(128, C::N3);
-  const uint32_t id_B = umma::idesc_tf32(128, C::NPN);
-  const uint32_t sB1h = umma::smem_u32(B1h), sB1l = umma::smem_u32(B1l);
-  const uint32_t sB2h = umma::smem_u32(B2h), sB2l = umma::smem_u32(B2l);
-  const uint32_t sU = umma::smem_u32(U);
-  const uint32_t sbo1 = K1 * 32, sboB2 = C::KB2 * 32, sboCH = KV * 32;
-  const uint32_t b3_off = (C::NC8 / 8) * sbo1;  // B1 from its face-0 Gauss-point rows on
-
-  const double tstage = a.time_from_state ? d.st->t + d.st->dt * a.frac : a.t_arg;
-  const double dt = a.time_from_state ? d.st->dt : a.dt_arg;
-  const bool want_lambda = a.mode != MODE_STAGE;
-  int err = 0;
-  double lmax = 0.0;
-  uint32_t phA = 0, ring_uses[C::NBUF];
-#pragma unroll
-  for (int b = 0; b < C::NBUF; ++b) ring_uses[b] = 0;
-  uint32_t chunk_counter = 0;
-
-  // row (element, field) of a tile row index
-  const int rr = tid & 127, rq = rr >> 5, rln = rr & 31;
-  const int rel = rln / M, rf = rln - rel * M, re = rq * EPQ + rel;
-  auto rowb_of = [](int e) { return (e / EPQ) * 32 + (e % EPQ) * M; };
-
-  // fp32 pointwise physics, identical wherever it is evaluated
-  auto flux32 = [&](const float* qc, float* F, float* G) { P::flux2(d.eqp, qc, F, G, &err); };
-  auto bc_coords = [&](int e, int fc, int g, double& x, double& y) {
-    const ElemGeo& geo = d.geo[e];
-    const double z = d.gz[g];
-    double r, s;
-    if (fc == 0) { r = z; s = -1.0; }
-    else if (fc == 1) { r = -z; s = z; }
-    else { r = -1.0; s = -z; }
-    x = 0.5 * (-geo.vx[0] * (r + s) + geo.vx[1] * (1. + r) + geo.vx[2] * (1. + s));
-    y = 0.5 * (-geo.vy[0] * (r + s) + geo.vy[1] * (1. + r) + geo.vy[2] * (1. + s));
-  };
-  // Lax-Friedrichs flux on face fc at Gauss point g, fp32, float normals
-  auto numflux32 = [&](int e, int k, int fc, int g, const float* qM, float* qP, float* nf) {
-    const float* G = GEO + e * 16;
-    const float nx = G[5 + fc], ny = G[8 + fc];
-    const int nb = CN[e * 6 + 2 * fc];
-    if (nb < 0) {
-      double x, y;
-      bc_coords(k, fc, g, x, y);
-      apply_bc<EQ, float>(d.bcs, -nb, tstage, x, y, nx, ny, qM, qP);
-    }
-    float qMc[M];
-#pragma unroll
-    for (int f = 0; f < M; ++f) qMc[f] = qM[f];
-    return P::numflux(d.eqp, nx, ny, qMc, qP, nf, &err);
-  };
 
   const int ntiles = (d.K + E - 1) / E;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int k0 = tile * E;
-    const int ne = min(E, d.K - k0);
-    const bool rvalid = rel < EPQ && re < ne;
-    // ---- operands: own deviations (A1) and, per face, the neighbour's deviations
-    // rotated so that the shared face is its face 0 (A3); 4 x 128 row tasks
-    for (int task = tid; task < 4 * 128; task += kMixThreads) {
-      const int kind = task >> 7, r = task & 127;  // kind 0: own, 1..3: face kind - 1
-      const int q = r >> 5, ln = r & 31, el = ln / M, f = ln - el * M, e = q * EPQ + el;
-      const bool valid = el < EPQ && e < ne;
-      int src = -1, f2 = 0;
-      if (valid) {
-        if (kind == 0) {
-          src = k0 + e;
-        } else {
-          src = d.conn[(size_t)(k0 + e) * 6 + 2 * (kind - 1)];
-          f2 = d.conn[(size_t)(k0 + e) * 6 + 2 * (kind - 1) + 1];
+  const int my_tiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto tile_of = [&](int i) { return (int)blockIdx.x + i * (int)gridDim.x; };
+  auto x_copy_doubles = [&](int tile) {
+    const int ne = min(E, d.K - tile * E);
+    return ((ne * NP * M * 8) & ~15) / 8;
+  };
+  int err = 0;
+  int x_issued = 0;  // state copies issued (control warp)
+
+  if (warp == kMixThreads / 32 - 1) {
+    // ======================= control warp =======================
+    const uint32_t id_A = umma::idesc_tf32(128, C::NC16);
+    const uint32_t id_B = umma::idesc_tf32(128, C::NPN);
+    const uint32_t sB1h = umma::smem_u32(B1h), sB1l = umma::smem_u32(B1l);
+    const uint32_t sB2h = umma::smem_u32(B2h), sB2l = umma::smem_u32(B2l);
+    const uint32_t sA = umma::smem_u32(AOP), sRing = umma::smem_u32(RING);
+    auto issue_x = [&](int tile) {
+      const uint32_t bytes = (uint32_t)x_copy_doubles(tile) * 8u;
+      umma::mbar_expect_tx(mbX, bytes);
+      umma::bulk_g2s(umma::smem_u32(XS), a.x + (size_t)tile * E * NP * M, bytes, mbX);
+    };
+    if (x_bulk && my_tiles > 0 && lane == 0) issue_x(tile_of(0));
+    if (x_bulk && my_tiles > 0) x_issued = 1;
+    uint32_t cc = 0;  // chunk counter
+    bool ok = true;
+    for (int i = 0; i < my_tiles && ok; ++i) {
+      const int tile = tile_of(i);
+      // GEMM-A once the workers have written the A operand
+      ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mbA, i & 1));  // warp-uniform
+      if (!ok) break;
+      umma::fence_after_sync();
+      if (lane == 0) {
+#pragma unroll
+        for (int s = 0; s < K1 / 8; ++s) {
+          const uint32_t off = s * 2 * umma::kLBO;
+          const uint64_t ah = umma::make_desc(sA + off, umma::kLBO, C::SBO1);
+          const uint64_t al = umma::make_desc(sA + C::SZ_A + off, umma::kLBO, C::SBO1);
+          const uint64_t bh = umma::make_desc(sB1h + off, umma::kLBO, C::SBO1);
+          const uint64_t bl = umma::make_desc(sB1l + off, umma::kLBO, C::SBO1);
+          umma::mma_tf32(tb + C::T_D1, ah, bh, id_A, s > 0);
+          umma::mma_tf32(tb + C::T_D1, ah, bl, id_A, 1);
+          umma::mma_tf32(tb + C::T_D1, al, bh, id_A, 1);
+        }
+        umma::commit(mbD1);
+        // the state tile is consumed: fetch the next one; warm L2 with u0
+        if (x_bulk && i + 1 < my_tiles) issue_x(tile_of(i + 1));
+        if (u0_prefetch) {
+          const int ne = min(E, d.K - tile * E);
+          bulk_prefetch_l2(a.u0 + (size_t)tile * E * NP * M, (uint32_t)((ne * NP * M * 8) & ~15));
         }
       }
-      double qv[NP], qbar = 0.0;
-      if (src >= 0) {
-        const int* pr = ROT + f2 * NP;
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-          const int jj = kind == 0 ? j : pr[j];
-          qv[j] = a.x[((size_t)src * NP + jj) * M + f];
-          qbar += qv[j];
+      if (x_bulk && i + 1 < my_tiles) x_issued++;
+      // GEMM-B, chunk by chunk as the workers fill the ring
+      for (int ch = 0; ch < C::NCH && ok; ++ch, ++cc) {
+        const int b = cc % NBUF;
+        ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mb_full(b), (cc / NBUF) & 1));
+        if (!ok) break;
+        umma::fence_after_sync();
+        if (lane == 0) {
+          const uint32_t ah0 = sRing + b * 2 * C::SZ_CH, al0 = ah0 + C::SZ_CH;
+          const uint32_t b2 = ch * (KV / 4) * umma::kLBO;
+          const int ncols = ch < NV ? 2 * min(VPC, NC - ch * VPC) : min(KV, C::NFK - (ch - NV) * KV);
+          const int ns = (ncols + 7) / 8;
+          for (int s = 0; s < ns; ++s) {
+            const uint32_t off = s * 2 * umma::kLBO;
+            const uint64_t ah = umma::make_desc(ah0 + off, umma::kLBO, C::SBOC);
+            const uint64_t al = umma::make_desc(al0 + off, umma::kLBO, C::SBOC);
+            const uint64_t bh = umma::make_desc(sB2h + b2 + off, umma::kLBO, C::SBO2);
+            const uint64_t bl = umma::make_desc(sB2l + b2 + off, umma::kLBO, C::SBO2);
+            umma::mma_tf32(tb + C::T_D2, ah, bh, id_B, (ch == 0 && s == 0) ? 0u : 1u);
+            umma::mma_tf32(tb + C::T_D2, ah, bl, id_B, 1);
+            umma::mma_tf32(tb + C::T_D2, al, bh, id_B, 1);
+          }
+          umma::commit(mb_empty(b));
+          if (ch == C::NCH - 1) umma::commit(mbD2);
         }
-        qbar *= 1.0 / NP;
+        __syncwarp();
       }
-      unsigned char* Ah = U + 2 * kind * C::SZ_A1;
-      unsigned char* Al = Ah + C::SZ_A1;
-#pragma unroll
-      for (int j4 = 0; j4 < K1; j4 += 4) {
-        float hv[4], lv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int j = j4 + u;
-          float x = 0.f;
-          if (src >= 0 && j < NP) x = (float)(qv[j] - qbar);
-          split_trunc(x, hv[u], lv[u]);
+    }
+    if (!ok) *abort_flag = 1;
+  } else {
+    // ======================= workers =======================
+    const int wtid = tid;  // 0 .. NW-1
+    const uint32_t tlane = tb + ((uint32_t)(32 * (warp & 3)) << 16);
+    const double tstage = a.time_from_state ? d.st->t + d.st->dt * a.frac : a.t_arg;
+    const double dt = a.time_from_state ? d.st->dt : a.dt_arg;
+    const bool want_lambda = a.mode != MODE_STAGE;
+    const bool write_traces = a.tr_out != nullptr && a.mode != MODE_RHS;
+    double lmax = 0.0;
+    // this thread's tile row (element, field)
+    const int rr = tid & 127, rq = rr >> 5, rln = rr & 31;
+    const int rel = rln / M, rf = rln - rel * M, re = rq * EPQ + rel;
+    auto rowb_of = [](int e) { return (e / EPQ) * 32 + (e % EPQ) * M; };
+    auto bc_coords = [&](int k, int fc, int g, double& x, double& y) {
+      const ElemGeo& geo = d.geo[k];
+      const double z = d.gz[g];
+      double r, s;
+      if (fc == 0) { r = z; s = -1.0; }
+      else if (fc == 1) { r = -z; s = z; }
+      else { r = -1.0; s = -z; }
+      x = 0.5 * (-geo.vx[0] * (r + s) + geo.vx[1] * (1. + r) + geo.vx[2] * (1. + s));
+      y = 0.5 * (-geo.vy[0] * (r + s) + geo.vy[1] * (1. + r) + geo.vy[2] * (1. + s));
+    };
+    auto slot = [&](int i) { return sm + C::O_TD + (i & 1) * C::SZ_TD; };
+    bool ok = true;
+
+    // operand build of tile i: state deviations (A operand), means, geometry
+    auto build_a = [&](int i) {
+      const int tile = tile_of(i), k0 = tile * E, ne = min(E, d.K - k0);
+      unsigned char* td = slot(i);
+      float* GEO = (float*)(td + C::TD_GEO);
+      int* CN = (int*)(td + C::TD_CN);
+      float* QF = (float*)(td + C::TD_QF);
+      const double* xg = a.x + (size_t)k0 * NP * M;
+      int nx = 0;
+      if (x_bulk) {
+        if (!umma::mbar_wait_bounded(mbX, i & 1)) {
+          *abort_flag = 1;  // no arrival: the control warp's wait times out as well
+          return;
         }
-        const uint32_t off = umma::kmajor_offset(r, j4, K1);
-        *(float4*)(Ah + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
-        *(float4*)(Al + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+        nx = x_copy_doubles(tile);
       }
-      QB[128 * kind + r] = qbar;
-      QF[128 * kind + r] = (float)qbar;
-      if (kind == 0 && valid && f == 0) {
+      for (int task = wtid; task < 128 * (K1 / 4); task += NW) {
+        const int r = task & 127, grp = task >> 7;
+        const int q = r >> 5, ln = r & 31, el = ln / M, f = ln - el * M, e = q * EPQ + el;
+        float hv[4] = {0.f, 0.f, 0.f, 0.f}, lv[4] = {0.f, 0.f, 0.f, 0.f};
+        if (el < EPQ && e < ne) {
+          double v[NP];
+#pragma unroll
+          for (int j = 0; j < NP; ++j) {
+            const int idx = (e * NP + j) * M + f;
+            v[j] = idx < nx ? XS[idx] : xg[idx];
+          }
+          const double qbar = nodal_mean<NP>(v);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int j = grp * 4 + u;
+            if (j < NP) {
+              const int idx = (e * NP + j) * M + f;
+              const double xj = idx < nx ? XS[idx] : xg[idx];
+              split_tf32((float)(xj - qbar), hv[u], lv[u]);
+            }
+          }
+          if (grp == 0) QF[f * E + e] = (float)qbar;
+        }
+        const uint32_t off = umma::kmajor_offset_sbo(r, grp * 4, C::SBO1);
+        *(float4*)(AOP + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+        *(float4*)(AOP + C::SZ_A + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+      }
+      for (int e = NW - 1 - wtid; e < ne; e += NW) {
         const int k = k0 + e;
 #pragma unroll
-        for (int i = 0; i < 6; ++i) CN[e * 6 + i] = d.conn[(size_t)k * 6 + i];
+        for (int j = 0; j < 6; ++j) CN[e * 6 + j] = d.conn[(size_t)k * 6 + j];
         const ElemGeo& g = d.geo[k];
-        float* G = GEO + e * 16;
-        G[0] = (float)g.rx; G[1] = (float)g.ry; G[2] = (float)g.sx; G[3] = (float)g.sy; G[4] = (float)g.invJ;
+        GEO[0 * E + e] = (float)g.rx; GEO[1 * E + e] = (float)g.ry;
+        GEO[2 * E + e] = (float)g.sx; GEO[3 * E + e] = (float)g.sy;
 #pragma unroll
         for (int fc = 0; fc < 3; ++fc) {
-          G[5 + fc] = (float)g.nx[fc];
-          G[8 + fc] = (float)g.ny[fc];
-          G[11 + fc] = (float)(g.sJ[fc] * g.invJ);
+          GEO[(4 + fc) * E + e] = (float)g.nx[fc];
+          GEO[(7 + fc) * E + e] = (float)g.ny[fc];
+          GEO[(10 + fc) * E + e] = (float)(-g.sJ[fc] * g.invJ);
         }
       }
-    }
-    umma::fence_proxy_async();
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (tid == 0) {
-#pragma unroll
-      for (int s = 0; s < K1 / 8; ++s) {
-        const uint32_t off = s * 2 * umma::kLBO;
-        const uint64_t a1h = umma::make_desc(sU + off, umma::kLBO, sbo1);
-        const uint64_t a1l = umma::make_desc(sU + C::SZ_A1 + off, umma::kLBO, sbo1);
-        const uint64_t b1h = umma::make_desc(sB1h + off, umma::kLBO, sbo1);
-        const uint64_t b1l = umma::make_desc(sB1l + off, umma::kLBO, sbo1);
-        umma::mma_tf32(tb + C::T_D1, a1h, b1h, id_A, s > 0);
-        umma::mma_tf32(tb + C::T_D1, a1h, b1l, id_A, 1);
-        umma::mma_tf32(tb + C::T_D1, a1l, b1h, id_A, 1);
-        const uint64_t b3h = umma::make_desc(sB1h + b3_off + off, umma::kLBO, sbo1);
-        const uint64_t b3l = umma::make_desc(sB1l + b3_off + off, umma::kLBO, sbo1);
-#pragma unroll
-        for (int fc = 0; fc < 3; ++fc) {
-          const uint32_t base = sU + 2 * (1 + fc) * C::SZ_A1;
-          const uint64_t a3h = umma::make_desc(base + off, umma::kLBO, sbo1);
-          const uint64_t a3l = umma::make_desc(base + C::SZ_A1 + off, umma::kLBO, sbo1);
-          const uint32_t td = tb + C::T_D3 + fc * C::N3;
-          umma::mma_tf32(td, a3h, b3h, id_3, s > 0);
-          umma::mma_tf32(td, a3h, b3l, id_3, 1);
-          umma::mma_tf32(td, a3l, b3h, id_3, 1);
-        }
-      }
-      umma::commit(umma::smem_u32(mbar));
-    }
-    if (!umma::mbar_wait_bounded(umma::smem_u32(mbar), phA & 1)) *abort_flag = 1;
-    phA++;
-    umma::fence_after_sync();
-    // ---- staged cubature values (first wave) and the g = 0 traces, as
-    // deviations; the means are added in the precision of use
-    auto stage_wave = [&](int c_begin) {
-      if (tid < 128) {
-#pragma unroll 1
-        for (int c0 = 0; c0 < SR && c_begin + c0 < NC; c0 += 16) {
-          float v[16];
-          umma::tmem_ld16(tlane + C::T_D1 + c_begin + c0, v);
-          umma::tmem_wait_ld();
-#pragma unroll
-          for (int j = 0; j < 16; ++j) ST[(c0 + j) * 128 + rr] = v[j];
-        }
-      }
-    };
-    stage_wave(0);
-    if (tid < 128) {
-#pragma unroll 1
-      for (int fc = 0; fc < 3; ++fc) {
-        float v[16];
-        umma::tmem_ld16(tlane + C::T_D1 + C::NC8 + fc * NG, v);
-        umma::tmem_wait_ld();
-        G0[fc * 128 + rr] = v[0];
-      }
-    } else if (tid < 256) {
-      // the partner's g = 0 is its last Gauss point (reversed order)
-#pragma unroll 1
-      for (int fc = 0; fc < 3; ++fc) {
-        float v[16];
-        umma::tmem_ld16(tlane + C::T_D3 + fc * C::N3, v);
-        umma::tmem_wait_ld();
-        G0[(3 + fc) * 128 + rr] = v[NG - 1];
-      }
-    }
-    __syncthreads();
-    if (*abort_flag) break;
-    // ---- point-0 references.  The fp32 values are what every other point's
-    // deviation is taken from (so a uniform state has zero deviations); the
-    // float64 constants multiply the operator row sums with float64 metrics
-    // and normals, which keeps a uniform flow exactly steady.
-    for (int it = tid; it < ne * 4; it += kMixThreads) {
-      const int e = it >> 2, kind = it & 3, rowb = rowb_of(e), k = k0 + e;
-      const ElemGeo& geo = d.geo[k];
-      float* p0 = P0 + e * 5 * M;
-      if (kind == 0) {
-        float qc[M], F[M], G[M];
-#pragma unroll
-        for (int f = 0; f < M; ++f) qc[f] = QF[rowb + f] + ST[rowb + f];
-        flux32(qc, F, G);
-#pragma unroll
-        for (int f = 0; f < M; ++f) {
-          p0[f] = F[f];
-          p0[M + f] = G[f];
-          Rb[e * 2 * M + f] = geo.rx * (double)F[f] + geo.ry * (double)G[f];
-          Rb[e * 2 * M + M + f] = geo.sx * (double)F[f] + geo.sy * (double)G[f];
-        }
-      } else {
-        const int fc = kind - 1;
-        float qM[M], qP[M], nf[M];
-#pragma unroll
-        for (int f = 0; f < M; ++f) {
-          qM[f] = QF[rowb + f] + G0[fc * 128 + rowb + f];
-          qP[f] = QF[128 * (1 + fc) + rowb + f] + G0[(3 + fc) * 128 + rowb + f];
-        }
-        numflux32(e, k, fc, 0, qM, qP, nf);
-        // float64 flux of the same fp32 traces with float64 normals
-        double dM[M], dP[M], nf64[M];
-#pragma unroll
-        for (int f = 0; f < M; ++f) { dM[f] = qM[f]; dP[f] = qP[f]; }
-        P::numflux(d.eqp, geo.nx[fc], geo.ny[fc], dM, dP, nf64, &err);
-        const double w = -geo.sJ[fc] * geo.invJ;
-#pragma unroll
-        for (int f = 0; f < M; ++f) {
-          p0[(2 + fc) * M + f] = nf[f];
-          Fb[(e * 3 + fc) * M + f] = nf64[f] * w;
-        }
-      }
-    }
-    __syncthreads();
-    // ---- contraction with the weighted derivative and LIFT operators, by chunks
-    auto claim = [&](int b) {
-      if (ring_uses[b] > 0 &&
-          !umma::mbar_wait_bounded(umma::smem_u32(mbar + 1 + b), (ring_uses[b] - 1) & 1))
-        *abort_flag = 1;
-      ring_uses[b]++;
-    };
-    auto issue_chunk = [&](int b, uint32_t b2off, int ksteps, bool first) {
       umma::fence_proxy_async();
-      umma::fence_before_sync();
-      __syncthreads();
+      mbar_arrive(mbA);
+    };
+    // reference fluxes at the fp32 mean of tile i (tasks: volume + 3 faces per element)
+    auto refs = [&](int i, int t0, int nt) {
+      const int tile = tile_of(i), k0 = tile * E, ne = min(E, d.K - k0);
+      unsigned char* td = slot(i);
+      const float* GEO = (const float*)(td + C::TD_GEO);
+      const float* QF = (const float*)(td + C::TD_QF);
+      float* P0 = (float*)(td + C::TD_P0);
+      double* Rb = (double*)(td + C::TD_RB);
+      double* Fb = (double*)(td + C::TD_FB);
+      for (int task = t0; task < 4 * E; task += nt) {
+        const int kind = task / E, e = task - kind * E;
+        if (e >= ne) continue;
+        const ElemGeo& geo = d.geo[k0 + e];
+        float qc[M];
+#pragma unroll
+        for (int f = 0; f < M; ++f) qc[f] = QF[f * E + e];
+        // the fp32 flux of the mean; every float64 constant uses these same
+        // values, so the volume and face constants cancel for a uniform state
+        float F[M], G[M];
+        P::flux2(d.eqp, qc, F, G, &err);
+        if (kind == 0) {
+#pragma unroll
+          for (int f = 0; f < M; ++f) {
+            P0[f * E + e] = F[f];
+            P0[(M + f) * E + e] = G[f];
+            Rb[f * E + e] = geo.rx * (double)F[f] + geo.ry * (double)G[f];
+            Rb[(M + f) * E + e] = geo.sx * (double)F[f] + geo.sy * (double)G[f];
+          }
+        } else {
+          // face reference: the fp32 Lax-Friedrichs flux with both states at the
+          // mean (what a uniform state gives at every Gauss point); its float64
+          // constant is the normal flux nx F + ny G of the same F, G (the wave-speed
+          // term vanishes for equal states) with float64 normals
+          const int fc = kind - 1;
+          float qM[M], qP[M], nf[M];
+#pragma unroll
+          for (int f = 0; f < M; ++f) { qM[f] = qc[f]; qP[f] = qc[f]; }
+          P::numflux(d.eqp, GEO[(4 + fc) * E + e], GEO[(7 + fc) * E + e], qM, qP, nf, &err);
+          const double w = -geo.sJ[fc] * geo.invJ, nx = geo.nx[fc], ny = geo.ny[fc];
+#pragma unroll
+          for (int f = 0; f < M; ++f) {
+            P0[((2 + fc) * M + f) * E + e] = nf[f];
+            Fb[(fc * M + f) * E + e] = w * (nx * (double)F[f] + ny * (double)G[f]);
+          }
+        }
+      }
+    };
+    // cubature deviations of tile i from TMEM to ST (warps by lane quadrant)
+    auto stage = [&](int i) {
+      if (!umma::mbar_wait_bounded(mbD1, i & 1)) *abort_flag = 1;
       umma::fence_after_sync();
-      if (tid == 0) {
-        const uint32_t ah0 = sU + b * 2 * C::SZ_CH, al0 = ah0 + C::SZ_CH;
-        for (int s = 0; s < ksteps; ++s) {
-          const uint32_t off = s * 2 * umma::kLBO;
-          const uint64_t ah = umma::make_desc(ah0 + off, umma::kLBO, sboCH);
-          const uint64_t al = umma::make_desc(al0 + off, umma::kLBO, sboCH);
-          const uint64_t bh = umma::make_desc(sB2h + b2off + off, umma::kLBO, sboB2);
-          const uint64_t bl = umma::make_desc(sB2l + b2off + off, umma::kLBO, sboB2);
-          umma::mma_tf32(tb + C::T_D2, ah, bh, id_B, (first && s == 0) ? 0u : 1u);
-          umma::mma_tf32(tb + C::T_D2, ah, bl, id_B, 1);
-          umma::mma_tf32(tb + C::T_D2, al, bh, id_B, 1);
+      const int q = warp & 3, nwq = q < 3 ? 3 : 2;  // workers 0..10: three warps per quadrant, two for the last
+#pragma unroll 1
+      for (int blk = warp >> 2; blk < C::NC16 / 16; blk += nwq) {
+        float v[16];
+        umma::tmem_ld16(tlane + C::T_D1 + 16 * blk, v);
+        umma::tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (16 * blk + j < NC) ST[(16 * blk + j) * 128 + rr] = v[j];
+      }
+      umma::fence_before_sync();
+    };
+    // chunk operands of tile i into the ring; cc counts chunks over all tiles
+    uint32_t cc = 0;
+    auto items = [&](int i) {
+      const int tile = tile_of(i), k0 = tile * E, ne = min(E, d.K - k0);
+      unsigned char* td = slot(i);
+      const float* GEO = (const float*)(td + C::TD_GEO);
+      const int* CN = (const int*)(td + C::TD_CN);
+      const float* QF = (const float*)(td + C::TD_QF);
+      const float* P0 = (const float*)(td + C::TD_P0);
+      for (int ch = 0; ch < C::NCH; ++ch, ++cc) {
+        const int b = cc % NBUF;
+        if (cc >= NBUF && !umma::mbar_wait_bounded(mb_empty(b), ((cc / NBUF) - 1) & 1)) *abort_flag = 1;
+        unsigned char* bh = RING + b * 2 * C::SZ_CH;
+        unsigned char* bl = bh + C::SZ_CH;
+        if (ch < NV) {
+          // volume: deviation of the fp32 flux from the flux of the mean, times the metric
+          const int npts = min(VPC, NC - ch * VPC);
+          const int nfill = 4 * ((npts + 3) / 4);
+          for (int it = wtid; it < nfill * E; it += NW) {
+            const int cp = it / E, e = it - cp * E;
+            if (e >= ne) continue;
+            const int rowb = rowb_of(e);
+            float R[M], S[M];
+            if (cp < npts) {
+              const int c = ch * VPC + cp;
+              float qc[M], F[M], G[M];
+              load_fields<M>(ST + c * 128 + rowb, qc);
+#pragma unroll
+              for (int f = 0; f < M; ++f) qc[f] += QF[f * E + e];
+              P::flux2(d.eqp, qc, F, G, &err);
+              const float rx = GEO[0 * E + e], ry = GEO[1 * E + e], sx = GEO[2 * E + e], sy = GEO[3 * E + e];
+#pragma unroll
+              for (int f = 0; f < M; ++f) {
+                const float dF = F[f] - P0[f * E + e], dG = G[f] - P0[(M + f) * E + e];
+                R[f] = rx * dF + ry * dG;
+                S[f] = sx * dF + sy * dG;
+              }
+            } else {
+#pragma unroll
+              for (int f = 0; f < M; ++f) { R[f] = 0.f; S[f] = 0.f; }
+            }
+#pragma unroll
+            for (int f = 0; f < M; ++f) {
+              float h0, l0, h1, l1;
+              split_tf32(R[f], h0, l0);
+              split_tf32(S[f], h1, l1);
+              const uint32_t off = umma::kmajor_offset_sbo(rowb + f, 2 * cp, C::SBOC);
+              *(float2*)(bh + off) = make_float2(h0, h1);
+              *(float2*)(bl + off) = make_float2(l0, l1);
+            }
+          }
+        } else {
+          // faces: Lax-Friedrichs flux of the stored traces, deviation from the
+          // reference flux, times -sJ/J; column fc NG + g
+          const int col0 = (ch - NV) * KV;
+          const int ncol = min(KV, C::NFK - col0);
+          for (int it = wtid; it < ncol * E; it += NW) {
+            const int e = it % E, cl = it / E, col = col0 + cl;
+            if (e >= ne) continue;
+            const int rowb = rowb_of(e), k = k0 + e;
+            float dev[M];
+            if (col < NF) {
+              const int fc = col / NG, g = col - fc * NG;
+              float qM[M], qP[M], nf[M];
+              const int nb = CN[e * 6 + 2 * fc];
+              load_fields<M>(a.tr_in + ((size_t)(k * 3 + fc) * NG + g) * M, qM);
+              if (nb >= 0) {
+                const int f2 = CN[e * 6 + 2 * fc + 1];
+                load_fields<M>(a.tr_in + ((size_t)(nb * 3 + f2) * NG + (NG - 1 - g)) * M, qP);
+              }
+              const float nx = GEO[(4 + fc) * E + e], ny = GEO[(7 + fc) * E + e];
+              if (nb < 0) {
+                double x, y;
+                bc_coords(k, fc, g, x, y);
+                apply_bc<EQ, float>(d.bcs, -nb, tstage, x, y, nx, ny, qM, qP);
+              }
+              const float lam = P::numflux(d.eqp, nx, ny, qM, qP, nf, &err);
+              if (want_lambda) {
+                const double l = fabs((double)lam);
+                lmax = l > lmax ? l : lmax;
+              }
+              const float w = GEO[(10 + fc) * E + e];
+#pragma unroll
+              for (int f = 0; f < M; ++f) dev[f] = w * (nf[f] - P0[((2 + fc) * M + f) * E + e]);
+            } else {
+#pragma unroll
+              for (int f = 0; f < M; ++f) dev[f] = 0.f;
+            }
+#pragma unroll
+            for (int f = 0; f < M; ++f) {
+              float h, l;
+              split_tf32(dev[f], h, l);
+              const uint32_t off = umma::kmajor_offset_sbo(rowb + f, cl, C::SBOC);
+              *(float*)(bh + off) = h;
+              *(float*)(bl + off) = l;
+            }
+          }
         }
-        umma::commit(umma::smem_u32(mbar + 1 + b));
+        umma::fence_proxy_async();
+        mbar_arrive(mb_full(b));
       }
     };
-    // volume: deviation of the fp32 flux from its point-0 value, times the metric
-    auto vol_item = [&](int e, int cp, int c, unsigned char* bh, unsigned char* bl) {
-      const int rowb = rowb_of(e);
-      const float* p0 = P0 + e * 5 * M;
-      float qc[M], F[M], G[M];
-      load_fields<M>(ST + (c % SR) * 128 + rowb, qc);
-#pragma unroll
-      for (int f = 0; f < M; ++f) qc[f] += QF[rowb + f];
-      flux32(qc, F, G);
-      const float4 g = *(const float4*)(GEO + e * 16);
-#pragma unroll
-      for (int f = 0; f < M; ++f) {
-        const float dF = F[f] - p0[f], dG = G[f] - p0[M + f];
-        float h0, l0, h1, l1;
-        split_trunc(g.x * dF + g.y * dG, h0, l0);
-        split_trunc(g.z * dF + g.w * dG, h1, l1);
-        const uint32_t off = umma::kmajor_offset(rowb + f, 2 * cp, KV);
-        *(float2*)(bh + off) = make_float2(h0, h1);
-        *(float2*)(bl + off) = make_float2(l0, l1);
-      }
-    };
-    for (int ch = 0; ch < C::NV; ++ch) {
-      if (ch > 0 && (ch * VPC) % SR == 0) {
-        // next staging wave (the previous chunk's items are done: issue barrier)
-        stage_wave(ch * VPC);
-        __syncthreads();
-      }
-      const int b = chunk_counter++ % C::NBUF;
-      claim(b);
-      unsigned char* bh = U + b * 2 * C::SZ_CH;
-      unsigned char* bl = bh + C::SZ_CH;
-      for (int it = tid; it < ne * VPC; it += kMixThreads) {
-        const int e = it / VPC, cp = it - e * VPC, c = ch * VPC + cp;
-        if (c < NC) vol_item(e, cp, c, bh, bl);
-      }
-      issue_chunk(b, ch * (KV / 4) * umma::kLBO, KV / 8, ch == 0);
-    }
-    for (int fc = 0; fc < 3; ++fc) {
-      // own (rows 0..NG-1) and partner (rows 16..16+NG-1) traces of this face
-      if (tid < 128) {
-        float v[16];
-        umma::tmem_ld16(tlane + C::T_D1 + C::NC8 + fc * NG, v);
-        umma::tmem_wait_ld();
-        const float qb = QF[rr];
-#pragma unroll
-        for (int j = 0; j < NG; ++j) ST[j * 128 + rr] = qb + v[j];
-      } else if (tid < 256) {
-        float v[16];
-        umma::tmem_ld16(tlane + C::T_D3 + fc * C::N3, v);
-        umma::tmem_wait_ld();
-        const float qbn = QF[128 * (1 + fc) + rr];
-#pragma unroll
-        for (int j = 0; j < NG; ++j) ST[(16 + j) * 128 + rr] = qbn + v[NG - 1 - j];
-      }
-      const int b = chunk_counter++ % C::NBUF;
-      claim(b);
-      __syncthreads();
-      unsigned char* bh = U + b * 2 * C::SZ_CH;
-      unsigned char* bl = bh + C::SZ_CH;
-      for (int it = tid; it < ne * NG; it += kMixThreads) {
-        const int e = it / NG, g = it - e * NG, rowb = rowb_of(e), k = k0 + e;
-        float qM[M], qP[M], nf[M];
-        load_fields<M>(ST + g * 128 + rowb, qM);
-        load_fields<M>(ST + (16 + g) * 128 + rowb, qP);
-        const float lam = numflux32(e, k, fc, g, qM, qP, nf);
-        if (want_lambda) {
-          const double l = fabs((double)lam);
-          lmax = l > lmax ? l : lmax;
-        }
-        const float w = -GEO[e * 16 + 11 + fc];
-        const float* p0 = P0 + e * 5 * M + (2 + fc) * M;
-#pragma unroll
-        for (int f = 0; f < M; ++f) {
-          float h, l;
-          split_trunc(w * (nf[f] - p0[f]), h, l);
-          const uint32_t off = umma::kmajor_offset(rowb + f, g, KV);
-          *(float*)(bh + off) = h;
-          *(float*)(bl + off) = l;
-        }
-      }
-      issue_chunk(b, (C::NV * KV + 16 * fc) / 4 * umma::kLBO, 2, false);
-    }
-    // ---- wait for the last chunk, epilogue ----------------------------------------
-    {
-      const int blast = (chunk_counter - 1) % C::NBUF;
-      if (!umma::mbar_wait_bounded(umma::smem_u32(mbar + 1 + blast), (ring_uses[blast] - 1) & 1)) *abort_flag = 1;
-    }
-    __syncthreads();
-    umma::fence_after_sync();
-    if (tid < 128 && !*abort_flag) {
+    // float64 epilogue of tile i (threads 0..127: TMEM lane = tile row)
+    auto epilogue = [&](int i) {
+      const int tile = tile_of(i), k0 = tile * E, ne = min(E, d.K - k0);
+      const bool rvalid = rel < EPQ && re < ne;
+      const unsigned char* td = slot(i);
+      const double* Rb = (const double*)(td + C::TD_RB);
+      const double* Fb = (const double*)(td + C::TD_FB);
+      if (!umma::mbar_wait_bounded(mbD2, i & 1)) *abort_flag = 1;
+      umma::fence_after_sync();
       float dv[C::NPN];
 #pragma unroll
       for (int c0 = 0; c0 < C::NPN; c0 += 16) {
@@ -539,76 +603,195 @@ __global__ void __launch_bounds__(kMixThreads, 1)
 #pragma unroll
         for (int j = 0; j < 16; ++j) dv[c0 + j] = v[j];
       }
-      if (rvalid) {
-        const int k = k0 + re;
-        const double Rbar = Rb[re * 2 * M + rf], Sbar = Rb[re * 2 * M + M + rf];
-        const double F0 = Fb[(re * 3 + 0) * M + rf], F1 = Fb[(re * 3 + 1) * M + rf], F2 = Fb[(re * 3 + 2) * M + rf];
-        const double c_stage = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
+      umma::fence_before_sync();
+      if (!rvalid || *abort_flag) return;
+      const int k = k0 + re;
+      const double Rbar = Rb[rf * E + re], Sbar = Rb[(M + rf) * E + re];
+      const double F0 = Fb[(0 * M + rf) * E + re], F1 = Fb[(1 * M + rf) * E + re], F2 = Fb[(2 * M + rf) * E + re];
+      const double c_stage = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
+      const double* xrow = a.x + (size_t)k * NP * M + rf;
+      const double* urow = a.u0 + (size_t)k * NP * M + rf;
+      double* orow = a.out + (size_t)k * NP * M + rf;
+      double o[NP];
+      // out may alias x and u0 (same row, same thread): each batch of nodes is
+      // loaded in full before any of it is stored, so the loads overlap
+      constexpr int BT = 8;
 #pragma unroll
-        for (int i = 0; i < NP; ++i) {
-          const double* rs = RSUM + i * 5;
-          const double r = (double)dv[i] + rs[0] * Rbar + rs[1] * Sbar + rs[2] * F0 + rs[3] * F1 + rs[4] * F2;
-          if (r != r) err |= ERRB_NAN;
-          const size_t off = ((size_t)k * NP + i) * M + rf;
-          double o;
-          if (a.mode == MODE_RHS) o = r;
-          else if (a.mode == MODE_STAGE) o = a.x[off] + c_stage * r;
-          else o = c_al * a.x[off] + c_be * r + c_ga * a.u0[off];
-          a.out[off] = o;
+      for (int i0 = 0; i0 < NP; i0 += BT) {
+        double xr[BT], ur[BT];
+#pragma unroll
+        for (int u = 0; u < BT; ++u) {
+          const int n = i0 + u;
+          if (n < NP && a.mode != MODE_RHS) xr[u] = xrow[n * M];
+          if (n < NP && a.mode == MODE_FINAL) ur[u] = urow[n * M];
+        }
+#pragma unroll
+        for (int u = 0; u < BT; ++u) {
+          const int n = i0 + u;
+          if (n >= NP) break;
+          const double* rs = RSUM + n * 5;
+          const double r = (double)dv[n] + rs[0] * Rbar + rs[1] * Sbar + rs[2] * F0 + rs[3] * F1 + rs[4] * F2;
+          if (!isfinite(r)) err |= ERRB_NAN;
+          if (a.mode == MODE_RHS) o[n] = r;
+          else if (a.mode == MODE_STAGE) o[n] = xr[u] + c_stage * r;
+          else o[n] = c_al * xr[u] + c_be * r + c_ga * ur[u];
+        }
+#pragma unroll
+        for (int u = 0; u < BT; ++u) {
+          const int n = i0 + u;
+          if (n < NP) orow[n * M] = o[n];
         }
       }
-    }
-    umma::fence_before_sync();
-    __syncthreads();
-    if (*abort_flag) break;
-  }
-  if (*abort_flag && tid == 0) atomicOr(&d.st->err, ERRB_TIMEOUT);
-  if (want_lambda) {
+      if (write_traces) {
+        const double m = nodal_mean<NP>(o);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double v = __shfl_xor_sync(0xffffffffu, lmax, o);
-      lmax = v > lmax ? v : lmax;
+        for (int n = 0; n < NP; ++n) XD[n * 128 + rr] = (float)(o[n] - m);
+        XB[rr] = m;
+      }
+    };
+    // face traces of tile i's result: (face, row) tasks
+    auto traces = [&](int i) {
+      const int tile = tile_of(i), k0 = tile * E, ne = min(E, d.K - k0);
+      for (int task = wtid; task < 3 * 128; task += NW) {
+        const int fc = task >> 7, r = task & 127, q = r >> 5, ln = r & 31, el = ln / M, f = ln - el * M;
+        const int e = q * EPQ + el;
+        if (el >= EPQ || e >= ne) continue;
+        const int k = k0 + e;
+        row_traces<NP, NG>(IF, XD + r, 128, XB[r], fc, a.tr_out + ((size_t)(k * 3 + fc) * NG) * M + f, M);
+      }
+    };
+
+    if (my_tiles > 0) {
+      build_a(0);
+      workers_sync<NW>();
+      refs(0, wtid, NW);
+      stage(0);
+      workers_sync<NW>();
+      ok = !*abort_flag;
     }
-    if (lane == 0 && lmax > 0.0) atomicMax(&d.st->lam_bits, (unsigned long long)__double_as_longlong(lmax));
+    for (int i = 0; i < my_tiles && ok; ++i) {
+      const bool next = i + 1 < my_tiles;
+      items(i);
+      if (next) build_a(i + 1);
+      workers_sync<NW>();
+      if (*abort_flag) { ok = false; break; }
+      if (wtid < 128) epilogue(i);
+      else if (next) refs(i + 1, wtid - 128, NW - 128);
+      workers_sync<NW>();
+      if (write_traces && !*abort_flag) traces(i);
+      if (next) {
+        stage(i + 1);
+        workers_sync<NW>();
+        // read right after a worker barrier, so every worker leaves together
+        if (*abort_flag) ok = false;
+      }
+    }
+    if (want_lambda) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v = __shfl_xor_sync(0xffffffffu, lmax, o);
+        lmax = v > lmax ? v : lmax;
+      }
+      if (lane == 0 && lmax > 0.0) atomicMax(&d.st->lam_bits, (unsigned long long)__double_as_longlong(lmax));
+    }
   }
   if (err) atomicOr(&d.st->err, err);
   umma::fence_before_sync();
   __syncthreads();
+  umma::fence_after_sync();
+  if (*abort_flag) {
+    // after an abort: let every issued MMA complete (a fresh barrier, so its
+    // parity is unambiguous) and the state copy in flight, if any, land
+    if (warp == kMixThreads / 32 - 1) {
+      if (lane == 0) umma::commit(mbDrain);
+      __syncwarp();
+      umma::mbar_wait_bounded(mbDrain, 0);
+      if (x_issued > 0) umma::mbar_wait_bounded(mbX, (x_issued - 1) & 1);
+    }
+    if (tid == 0) atomicOr(&d.st->err, ERRB_TIMEOUT);
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+  }
   if (warp == 0) umma::tmem_dealloc(tb, C::TCOLS);
 }
 
+// Face traces [K][3][NG][M] of a state: one thread per (element, field, face).
+template <int N, int M>
+__global__ void __launch_bounds__(256) k_mixed_traces(int K, const double* __restrict__ x,
+                                                      const double* __restrict__ I, float* __restrict__ T) {
+  constexpr int NP = Sizes<N>::NP, NG = Sizes<N>::NG, NF = Sizes<N>::NF;
+  __shared__ float IF[NF * NP];
+  for (int i = threadIdx.x; i < NF * NP; i += blockDim.x) IF[i] = (float)I[i];
+  __syncthreads();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)K * M * 3) return;
+  const int fc = (int)(t % 3);
+  const long long rest = t / 3;
+  const int f = (int)(rest % M);
+  const int k = (int)(rest / M);
+  double v[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) v[j] = x[((size_t)k * NP + j) * M + f];
+  const double m = nodal_mean<NP>(v);
+  float dv[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) dv[j] = (float)(v[j] - m);
+  row_traces<NP, NG>(IF, dv, 1, m, fc, T + ((size_t)(k * 3 + fc) * NG) * M + f, M);
+}
+
+template <int N, int M>
+cudaError_t launch_traces_t(const DgDev& d, const double* x, float* T, cudaStream_t s) {
+  const long long n = (long long)d.K * M * 3;
+  const int blocks = (int)((n + 255) / 256);
+  k_mixed_traces<N, M><<<blocks, 256, 0, s>>>(d.K, x, d.I, T);
+  return cudaGetLastError();
+}
+
 template <int EQ, int N>
-cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a0, cudaStream_t s, cudaEvent_t* ev) {
   using C = MixCfg<N, Eq<EQ>::M>;
   if constexpr (!C::FITS) {
     return cudaErrorNotSupported;
   } else {
-  static unsigned configured = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured & (1u << (dev & 31)))) {
-    cudaError_t e = cudaFuncSetAttribute(k_mixed_stage<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
-    if (e != cudaSuccess) return e;
-    configured |= 1u << (dev & 31);
-  }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int per_sm = max_c(1, min(512 / C::TCOLS, (228 * 1024) / (C::BYTES + 1024)));
-  const int ntiles = (d.K + C::E - 1) / C::E;
-  int grid = sms * per_sm;
-  if (grid > ntiles) grid = ntiles;
-  if (a.reset_lambda && a.mode != MODE_STAGE) {
-    cudaError_t e = cudaMemsetAsync(&d.st->lam_bits, 0, sizeof(unsigned long long), s);
-    if (e != cudaSuccess) return e;
-  }
-  if (ev) cudaEventRecord(ev[0], s);
-  k_mixed_stage<EQ, N><<<grid, kMixThreads, C::BYTES, s>>>(d, a, p->rowsum, p->rot);
-  if (ev) {
-    cudaEventRecord(ev[1], s);
-    cudaEventRecord(ev[2], s);
-    cudaEventRecord(ev[3], s);
-  }
-  return cudaGetLastError();
+    static unsigned configured = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured & (1u << (dev & 31)))) {
+      cudaError_t e = cudaFuncSetAttribute(k_mixed_stage<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
+      if (e != cudaSuccess) return e;
+      configured |= 1u << (dev & 31);
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = (d.K + C::E - 1) / C::E;
+    int grid = sms;
+    if (grid > ntiles) grid = ntiles;
+    StageArgs a = a0;
+    if (a.reset_lambda && a.mode != MODE_STAGE) {
+      cudaError_t e = cudaMemsetAsync(&d.st->lam_bits, 0, sizeof(unsigned long long), s);
+      if (e != cudaSuccess) return e;
+    }
+    if (ev) cudaEventRecord(ev[0], s);
+    if (a.mode == MODE_RHS) {
+      // the traces of the input first
+      if (!a.tr_scratch) return cudaErrorInvalidValue;
+      cudaError_t e = launch_traces_t<N, Eq<EQ>::M>(d, a.x, a.tr_scratch, s);
+      if (e != cudaSuccess) return e;
+      a.tr_in = a.tr_scratch;
+      a.tr_out = nullptr;
+    }
+    if (!a.tr_in) return cudaErrorInvalidValue;
+    if (ev) cudaEventRecord(ev[1], s);
+    // bit 0: the state is bulk-copied (16-byte aligned); bit 1: warm L2 with u0
+    const int flags = (((uintptr_t)a.x & 15) == 0 ? 1 : 0) |
+                      (a.mode == MODE_FINAL && ((uintptr_t)a.u0 & 15) == 0 ? 2 : 0);
+    k_mixed_stage<EQ, N><<<grid, kMixThreads, C::BYTES, s>>>(d, a, p->rowsum, flags);
+    if (ev) {
+      cudaEventRecord(ev[2], s);
+      cudaEventRecord(ev[3], s);
+    }
+    return cudaGetLastError();
   }
 }
 
@@ -635,9 +818,21 @@ cudaError_t mixed_dispatch_n(MixedPlan* p, const DgDev& d, const StageArgs& a, c
   }
 }
 
+template <int M>
+cudaError_t traces_dispatch_n(const DgDev& d, const double* x, float* T, cudaStream_t s) {
+  switch (d.N) {
+    case 2: return launch_traces_t<2, M>(d, x, T, s);
+    case 3: return launch_traces_t<3, M>(d, x, T, s);
+    case 4: return launch_traces_t<4, M>(d, x, T, s);
+    case 5: return launch_traces_t<5, M>(d, x, T, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 }  // namespace
 
 MixedPlan* mixed_create(int eq, const RefOps& o, int K, int M) {
+  (void)K;
   if (o.N < 2 || o.N > 5) return nullptr;
   bool fits = false;
   switch (eq) {
@@ -661,20 +856,17 @@ MixedPlan* mixed_create(int eq, const RefOps& o, int K, int M) {
     for (int fc = 0; fc < 3; ++fc)
       for (int g = 0; g < o.Ng; ++g) rs[i * 5 + 2 + fc] += o.Lift(i, fc * o.Ng + g) * o.gw[g];
   }
-  if (o.rot.empty() || cudaMalloc((void**)&p->rowsum, rs.size() * sizeof(double)) != cudaSuccess ||
-      cudaMalloc((void**)&p->rot, o.rot.size() * sizeof(int)) != cudaSuccess) {
+  if (cudaMalloc((void**)&p->rowsum, rs.size() * sizeof(double)) != cudaSuccess) {
     mixed_destroy(p);
     return nullptr;
   }
   cudaMemcpy(p->rowsum, rs.data(), rs.size() * sizeof(double), cudaMemcpyHostToDevice);
-  cudaMemcpy(p->rot, o.rot.data(), o.rot.size() * sizeof(int), cudaMemcpyHostToDevice);
   return p;
 }
 
 void mixed_destroy(MixedPlan* p) {
   if (!p) return;
   if (p->rowsum) cudaFree(p->rowsum);
-  if (p->rot) cudaFree(p->rot);
   delete p;
 }
 
@@ -686,6 +878,17 @@ cudaError_t mixed_launch_rhs(MixedPlan* p, int eq, const DgDev& d, const StageAr
     case EQ_MAXWELL: return mixed_dispatch_n<EQ_MAXWELL>(p, d, a, s, ev);
     case EQ_EULER2D: return mixed_dispatch_n<EQ_EULER2D>(p, d, a, s, ev);
     case EQ_MAXWELL_TM: return mixed_dispatch_n<EQ_MAXWELL_TM>(p, d, a, s, ev);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t mixed_launch_traces(MixedPlan* p, const DgDev& d, const double* x, float* T, cudaStream_t s) {
+  switch (p->M) {
+    case 1: return traces_dispatch_n<1>(d, x, T, s);
+    case 3: return traces_dispatch_n<3>(d, x, T, s);
+    case 4: return traces_dispatch_n<4>(d, x, T, s);
+    case 5: return traces_dispatch_n<5>(d, x, T, s);
+    case 8: return traces_dispatch_n<8>(d, x, T, s);
     default: return cudaErrorInvalidValue;
   }
 }

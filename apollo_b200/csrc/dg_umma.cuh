@@ -26,6 +26,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __host__ __device__ constexpr uint32_t kmajor_offset(int r, int k, int K) {
   return (uint32_t)((r >> 3) * (K * 32) + (k >> 2) * kLBO + (r & 7) * 16 + (k & 3) * 4);
 }
+// The same layout with an explicit 8-row group stride (SBO); a stride of
+// K * 32 + 16 staggers the groups across the shared-memory banks.
+__host__ __device__ constexpr uint32_t kmajor_offset_sbo(int r, int k, int sbo) {
+  return (uint32_t)((r >> 3) * sbo + (k >> 2) * kLBO + (r & 7) * 16 + (k & 3) * 4);
+}
 
 // Shared-memory matrix descriptor (sm_100: version 1, no swizzle).
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -125,6 +130,26 @@ __device__ __forceinline__ float to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
+}
+
+// The same rounding on the bit pattern with two integer operations: adding
+// half a tf32 unit to the magnitude and clearing the 13 dropped bits rounds to
+// nearest with ties away from zero (a carry into the exponent is the correct
+// result).  Finite inputs give the value cvt.rna gives; a NaN may come out as
+// an infinity, which the float64 epilogue's finiteness check still reports.
+__device__ __forceinline__ float round_tf32(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+// One-dimensional bulk copy global -> this CTA's shared memory, completing
+// on an mbarrier (both addresses 16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
 }
 
 }  // namespace umma
