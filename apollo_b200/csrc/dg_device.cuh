@@ -70,7 +70,7 @@ struct StageArgs {
   double t_arg;
   double dt_arg;        // dt used when time_from_state == 0
   int reset_lambda;     // volume kernel zeroes st->lam_bits first
-  // mixed precision only: fp32 face traces [K][3][NG][M] of x (tr_in) and of
+  // mixed precision only: fp32 face traces [K][3][NG M, padded] of x (tr_in) and of
   // the stage result (tr_out, nullptr: not needed); for MODE_RHS the launcher
   // first computes the traces of x into tr_scratch and reads them from there
   const float* tr_in;

@@ -406,7 +406,7 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
   h->K = K;
   h->mixed = mixed_create(h->eq, o, K, h->M);
   if (h->mixed) {
-    const size_t nTr = (size_t)K * o.Nf * M;
+    const size_t nTr = mixed_trace_floats(h->mixed, K);
     CK(cudaMalloc((void**)&h->TU_d, nTr * sizeof(float)), "trace alloc");
     CK(cudaMalloc((void**)&h->T0_d, nTr * sizeof(float)), "trace alloc");
     CK(cudaMalloc((void**)&h->T1_d, nTr * sizeof(float)), "trace alloc");

@@ -19,7 +19,9 @@ void mixed_destroy(MixedPlan* p);
 // the right-hand side); ev[0..3] bracket the trace kernel and the stage kernel.
 cudaError_t mixed_launch_rhs(MixedPlan* p, int eq, const DgDev& d, const StageArgs& a, cudaStream_t s,
                              cudaEvent_t* ev = nullptr);
-// fp32 face traces [K][3][NG][M] of the float64 state x.
+// Floats of one trace buffer: [K][3][NG M padded to a multiple of 4].
+size_t mixed_trace_floats(const MixedPlan* p, int K);
+// fp32 face traces of the float64 state x.
 cudaError_t mixed_launch_traces(MixedPlan* p, const DgDev& d, const double* x, float* T, cudaStream_t s);
 
 }  // namespace apollo
