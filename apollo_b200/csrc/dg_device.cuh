@@ -89,6 +89,8 @@ template <int N> struct Sizes {
 // Host launchers (dg_fp64.cu).
 // ev (optional): 4 events recorded before/between/after the three kernels
 cudaError_t launch_rhs_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// k_lift alone on d.vol / d.flux (used by the tangent of a stage)
+cudaError_t launch_lift_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStream_t s);
 cudaError_t launch_finalize(const DgDev& d, cudaStream_t s);
 cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wJ, cudaStream_t s);

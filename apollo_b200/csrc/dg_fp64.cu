@@ -18,6 +18,7 @@
 #include <stdint.h>
 
 #include "dg_device.cuh"
+#include "dg_dmma.cuh"
 
 namespace apollo {
 
@@ -29,21 +30,6 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   // non-negative doubles order like their bit patterns
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
-
-// ---------------------------------------------------------------------------
-// Float64 tensor-core fragments: mma.sync m8n8k4 f64 (DMMA).  Fragment layout
-// (PTX ISA, mma.m8n8k4 .f64): A 8x4, lane holds A[lane/4][lane%4]; B 4x8, lane
-// holds B[lane%4][lane/4]; C 8x8, lane holds C[lane/4][2*(lane%4) + {0,1}].
-__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c[0]), "+d"(c[1])
-               : "d"(a), "d"(b));
-}
-
-constexpr int round_up(int x, int m) { return (x + m - 1) / m * m; }
-// leading dimension (in doubles) of a shared-memory tile read by fragments:
-// rows 4 apart must land 8 banks apart, i.e. ld = 4 (mod 16)
-constexpr int pad_ld(int x) { return x + ((4 - x % 16) + 16) % 16; }
 
 // Tile of elements for the float64 volume kernel.  Columns of every GEMM are
 // (element, field) pairs; rows are cubature points, Gauss points or nodes.
@@ -70,43 +56,6 @@ template <int N, int M> struct VolTile {
   static constexpr int TOTAL = OFF_RS + RSR * LDB;
   static constexpr size_t BYTES = sizeof(double) * TOTAL;
 };
-
-constexpr int tile_n(int cblocks, int rblocks, int warps) {
-  // widest column tile (4, 2, 1 blocks of 8) that still gives every warp work
-  return (cblocks % 4 == 0 && rblocks * (cblocks / 4) >= warps) ? 4
-         : (cblocks % 2 == 0 && rblocks * (cblocks / 2) >= warps) ? 2 : 1;
-}
-
-// C[ROWS x COLS] = A[ROWS x K] B[K x COLS] over the block's warps; A, B in
-// shared memory; the epilogue gets (row, col, value) per output.
-template <int ROWS, int COLS, int K, int LDA, int LDB, int NWARPS, class Epi>
-__device__ __forceinline__ void block_dgemm(const double* A, const double* B, Epi epi) {
-  constexpr int RB = ROWS / 8, CB = COLS / 8, KS = K / 4;
-  constexpr int TN = tile_n(CB, RB, NWARPS);
-  constexpr int NT = RB * (CB / TN);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int lr = lane >> 2, lc = lane & 3;
-  for (int t = warp; t < NT; t += NWARPS) {
-    const int rb = t % RB, cg = t / RB;
-    double c[TN][2];
-#pragma unroll
-    for (int n = 0; n < TN; ++n) c[n][0] = c[n][1] = 0.0;
-    const double* ap = A + (rb * 8 + lr) * LDA + lc;
-    const double* bp = B + lc * LDB + cg * TN * 8 + lr;
-#pragma unroll 4
-    for (int k = 0; k < KS; ++k) {
-      const double a = ap[k * 4];
-#pragma unroll
-      for (int n = 0; n < TN; ++n) dmma_8x8x4(c[n], a, bp[k * 4 * LDB + n * 8]);
-    }
-#pragma unroll
-    for (int n = 0; n < TN; ++n) {
-      const int col = (cg * TN + n) * 8 + 2 * lc;
-      epi(rb * 8 + lr, col, c[n][0]);
-      epi(rb * 8 + lr, col + 1, c[n][1]);
-    }
-  }
-}
 
 template <int EQ, int N>
 __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
@@ -420,6 +369,42 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
   return cudaGetLastError();
 }
 
+// The LIFT kernel alone (surface contraction, 1/J, stage update) on the given
+// volume and face-flux buffers: the lift and the stage update are linear, so
+// the tangent of a stage applies it to the tangent buffers unchanged.
+template <int EQ, int N>
+cudaError_t launch_lift_t(const DgDev& d, const StageArgs& a, cudaStream_t s) {
+  constexpr int M = Eq<EQ>::M;
+  using LT = LiftTile<N, M>;
+  static unsigned configured = 0;  // bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured & (1u << (dev & 31)))) {
+    cudaError_t e = cudaFuncSetAttribute(k_lift<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LT::BYTES);
+    if (e != cudaSuccess) return e;
+    configured |= 1u << (dev & 31);
+  }
+  const int lt = (d.K + LT::E - 1) / LT::E;
+  int lper = (int)((200 * 1024) / LT::BYTES);
+  if (lper < 1) lper = 1;
+  if (lper > 8) lper = 8;
+  int gl = num_sms() * lper;
+  if (gl > lt) gl = lt;
+  k_lift<EQ, N><<<gl, kThreads, LT::BYTES, s>>>(d, a);
+  return cudaGetLastError();
+}
+
+template <int EQ>
+cudaError_t lift_dispatch_n(const DgDev& d, const StageArgs& a, cudaStream_t s) {
+  switch (d.N) {
+    case 2: return launch_lift_t<EQ, 2>(d, a, s);
+    case 3: return launch_lift_t<EQ, 3>(d, a, s);
+    case 4: return launch_lift_t<EQ, 4>(d, a, s);
+    case 5: return launch_lift_t<EQ, 5>(d, a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <int EQ>
 cudaError_t dispatch_n(const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   switch (d.N) {
@@ -442,6 +427,17 @@ cudaError_t launch_rhs_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStre
     case EQ_MAXWELL: return dispatch_n<EQ_MAXWELL>(d, a, s, ev);
     case EQ_EULER2D: return dispatch_n<EQ_EULER2D>(d, a, s, ev);
     case EQ_MAXWELL_TM: return dispatch_n<EQ_MAXWELL_TM>(d, a, s, ev);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_lift_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStream_t s) {
+  switch (eq) {
+    case EQ_ADVECTION: return lift_dispatch_n<EQ_ADVECTION>(d, a, s);
+    case EQ_EULER: return lift_dispatch_n<EQ_EULER>(d, a, s);
+    case EQ_MAXWELL: return lift_dispatch_n<EQ_MAXWELL>(d, a, s);
+    case EQ_EULER2D: return lift_dispatch_n<EQ_EULER2D>(d, a, s);
+    case EQ_MAXWELL_TM: return lift_dispatch_n<EQ_MAXWELL_TM>(d, a, s);
     default: return cudaErrorInvalidValue;
   }
 }

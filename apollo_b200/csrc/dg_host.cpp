@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "dg_device.cuh"
+#include "dg_adjoint.h"
 #include "dg_mixed.h"
 #include "dg_operators.h"
 
@@ -43,6 +44,17 @@ struct apollo_dg {
   // mixed precision: fp32 face traces of U (TU) and of the stage states (T0, T1)
   float *TU_d = nullptr, *T0_d = nullptr, *T1_d = nullptr;
   bool tu_valid = false;
+  // derivatives (float64): tangent scratch, adjoint scratch and state buffers
+  double *dvol_d = nullptr, *dtrace_d = nullptr, *dflux_d = nullptr, *sbar_d = nullptr;
+  double *tU_d = nullptr, *tW_d = nullptr, *A_d[3] = {nullptr, nullptr, nullptr};
+  // trajectory of the last apollo_dg_forward_fixed: checkpoints every `every`
+  // steps, and the stage states of one segment during apollo_dg_backward
+  std::vector<double*> ckpt;
+  double* seg_d = nullptr;
+  int seg_steps = 0;
+  int tr_nsteps = 0, tr_every = 0;
+  double tr_t0 = 0.0, tr_dt = 0.0;
+  bool tr_valid = false;
   double *vol_d = nullptr, *trace_d = nullptr, *flux_d = nullptr;
   DevState* st_d = nullptr;
   DevState* st_h = nullptr;  // pinned
@@ -94,6 +106,14 @@ void free_mesh(apollo_dg* h) {
   dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
   dfree(h->TU_d); dfree(h->T0_d); dfree(h->T1_d);
   h->tu_valid = false;
+  dfree(h->dvol_d); dfree(h->dtrace_d); dfree(h->dflux_d); dfree(h->sbar_d);
+  dfree(h->tU_d); dfree(h->tW_d);
+  for (auto& p : h->A_d) dfree(p);
+  for (auto& p : h->ckpt) dfree(p);
+  h->ckpt.clear();
+  dfree(h->seg_d);
+  h->seg_steps = 0;
+  h->tr_valid = false;
   dfree(h->vol_d); dfree(h->trace_d); dfree(h->flux_d);
   if (h->mixed) { mixed_destroy(h->mixed); h->mixed = nullptr; }
   h->have_state = false;
@@ -624,6 +644,120 @@ apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int it
 
 }  // extern "C"
 
+// ------------------------------------------------------ derivatives (float64) --
+namespace {
+
+apollo_status ensure_deriv_buffers(apollo_dg* h) {
+  if (h->dvol_d) return APOLLO_OK;
+  const size_t nU = (size_t)h->K * h->ops.Np * h->M, nT = (size_t)h->K * h->ops.Nf * h->M;
+  CK(cudaMalloc((void**)&h->dvol_d, nU * sizeof(double)), "derivative scratch");
+  CK(cudaMalloc((void**)&h->dtrace_d, nT * sizeof(double)), "derivative scratch");
+  CK(cudaMalloc((void**)&h->dflux_d, nT * sizeof(double)), "derivative scratch");
+  CK(cudaMalloc((void**)&h->sbar_d, nT * sizeof(double)), "derivative scratch");
+  CK(cudaMalloc((void**)&h->tU_d, nU * sizeof(double)), "derivative state");
+  CK(cudaMalloc((void**)&h->tW_d, nU * sizeof(double)), "derivative state");
+  for (auto& p : h->A_d) CK(cudaMalloc((void**)&p, nU * sizeof(double)), "adjoint state");
+  return APOLLO_OK;
+}
+
+size_t state_doubles(const apollo_dg* h) { return (size_t)h->K * h->ops.Np * h->M; }
+
+// Time of stage s (0..4) of the SSPRK(5,2) step that starts at tn.
+double stage_time(int s, double tn, double dt) { return tn + dt * (s < 4 ? s / 4.0 : 1.0); }
+
+// Stage s of a float64 step of fixed size dt: out = x + dt/4 L(x) (s < 4) or
+// 4/5 x + dt/5 L(x) + 1/5 u0 (s = 4).
+apollo_status fixed_stage(apollo_dg* h, int s, const double* x, const double* u0, double* out, double tn, double dt) {
+  StageArgs a{};
+  a.x = x;
+  a.u0 = u0;
+  a.out = out;
+  a.mode = s < 4 ? MODE_STAGE : MODE_FINAL;
+  a.time_from_state = 0;
+  a.t_arg = stage_time(s, tn, dt);
+  a.dt_arg = dt;
+  a.reset_lambda = 0;
+  DgDev d = make_dev(h);
+  cudaError_t e = launch_rhs_fp64(h->eq, d, a, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "stage launch");
+  return APOLLO_OK;
+}
+
+// One fixed step in place on u (stages through W).
+apollo_status fixed_step(apollo_dg* h, double* u, double tn, double dt) {
+  for (int s = 0; s < 5; ++s) {
+    apollo_status r = fixed_stage(h, s, s == 0 ? u : h->W_d, u, s < 4 ? h->W_d : u, tn, dt);
+    if (r) return r;
+  }
+  return APOLLO_OK;
+}
+
+// Tangent of stage s at the state x along dx (and du0 on the last stage).
+apollo_status tangent_stage(apollo_dg* h, int s, int mode, const double* x, const double* dx, const double* du0,
+                            double* dout, double tn, double dt) {
+  TanArgs a{};
+  a.x = x;
+  a.dx = dx;
+  a.du0 = du0;
+  a.dout = dout;
+  a.dvol = h->dvol_d;
+  a.dtrace = h->dtrace_d;
+  a.dflux = h->dflux_d;
+  a.mode = mode;
+  a.t = mode == MODE_RHS ? tn : stage_time(s, tn, dt);
+  a.dt = dt;
+  DgDev d = make_dev(h);
+  cudaError_t e = launch_tangent_stage(h->eq, d, a, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "tangent launch");
+  return APOLLO_OK;
+}
+
+// out = alpha wbar + beta L'(x)^T wbar + gamma z at time t.
+apollo_status adjoint_stage(apollo_dg* h, const double* x, const double* wbar, const double* z, double* out,
+                            double alpha, double beta, double gamma, double t) {
+  AdjArgs a{};
+  a.x = x;
+  a.wbar = wbar;
+  a.z = z;
+  a.out = out;
+  a.sbar = h->sbar_d;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.gamma = gamma;
+  a.t = t;
+  DgDev d = make_dev(h);
+  cudaError_t e = launch_adjoint_stage(h->eq, d, a, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "adjoint launch");
+  return APOLLO_OK;
+}
+
+apollo_status copy_in(apollo_dg* h, double* dst, const double* src, int where) {
+  const size_t n = state_doubles(h) * sizeof(double);
+  CK(cudaMemcpyAsync(dst, src, n, where == APOLLO_DEVICE_PTR ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     h->stream), "copy in");
+  return APOLLO_OK;
+}
+
+apollo_status copy_out(apollo_dg* h, double* dst, const double* src, int where) {
+  const size_t n = state_doubles(h) * sizeof(double);
+  CK(cudaMemcpyAsync(dst, src, n, where == APOLLO_DEVICE_PTR ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     h->stream), "copy out");
+  return APOLLO_OK;
+}
+
+apollo_status finish(apollo_dg* h) {
+  CK(cudaMemcpyAsync(h->st_h, h->st_d, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream), "state read");
+  CK(cudaStreamSynchronize(h->stream), "synchronize");
+  return read_errors(h);
+}
+
+apollo_status clear_errors(apollo_dg* h) {
+  CK(cudaMemsetAsync(&h->st_d->err, 0, sizeof(int), h->stream), "clear errors");
+  return APOLLO_OK;
+}
+
+}  // namespace
+
 namespace apollo {
 
 // Read-only view of a handle's discretisation for the no-allocation entry
@@ -647,6 +781,189 @@ void handle_set_error(apollo_dg* h, const char* msg) {
 extern "C" {
 
 const char* apollo_dg_last_error(const apollo_dg* h) { return h ? h->err.c_str() : "null handle"; }
+
+apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, double dt, int checkpoint_every) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (nsteps < 1 || checkpoint_every < 1 || !(dt > 0.0)) return fail(h, APOLLO_ERR_ARG, "nsteps, checkpoint_every >= 1, dt > 0");
+  if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  r = ensure_deriv_buffers(h);
+  if (r) return r;
+  const size_t nU = state_doubles(h);
+  const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  while ((int)h->ckpt.size() < nck) {
+    double* p = nullptr;
+    CK(cudaMalloc((void**)&p, nU * sizeof(double)), "checkpoint alloc");
+    h->ckpt.push_back(p);
+  }
+  h->tr_valid = false;
+  h->tu_valid = false;
+  r = clear_errors(h);
+  if (r) return r;
+  for (int n = 0; n < nsteps; ++n) {
+    if (n % checkpoint_every == 0)
+      CK(cudaMemcpyAsync(h->ckpt[n / checkpoint_every], h->U_d, nU * sizeof(double), cudaMemcpyDeviceToDevice,
+                         h->stream), "checkpoint");
+    r = fixed_step(h, h->U_d, t0 + n * dt, dt);
+    if (r) return r;
+  }
+  r = finish(h);
+  if (r) return r;
+  h->tr_nsteps = nsteps;
+  h->tr_every = checkpoint_every;
+  h->tr_t0 = t0;
+  h->tr_dt = dt;
+  h->tr_valid = true;
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* ubar_0, int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!ubar_T || !ubar_0) return APOLLO_ERR_ARG;
+  if (!h->tr_valid) return fail(h, APOLLO_ERR_STATE, "no trajectory: call apollo_dg_forward_fixed first");
+  const size_t nU = state_doubles(h);
+  const int C = h->tr_every, nsteps = h->tr_nsteps, nseg = (nsteps + C - 1) / C;
+  const double dt = h->tr_dt, c = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
+  if (h->seg_steps < C) {
+    dfree(h->seg_d);
+    h->seg_steps = 0;
+    CK(cudaMalloc((void**)&h->seg_d, (size_t)5 * C * nU * sizeof(double)), "segment alloc");
+    h->seg_steps = C;
+  }
+  auto S = [&](int j, int s) { return h->seg_d + ((size_t)j * 5 + s) * nU; };
+  double *A0 = h->A_d[0], *A1 = h->A_d[1], *A2 = h->A_d[2];
+  r = clear_errors(h);
+  if (r) return r;
+  r = copy_in(h, A0, ubar_T, where);
+  if (r) return r;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int n0 = seg * C, ns = std::min(nsteps, n0 + C) - n0;
+    // re-run the segment from its checkpoint, keeping every stage state
+    CK(cudaMemcpyAsync(S(0, 0), h->ckpt[seg], nU * sizeof(double), cudaMemcpyDeviceToDevice, h->stream), "restore");
+    for (int j = 0; j < ns; ++j) {
+      const double tn = h->tr_t0 + (n0 + j) * dt;
+      for (int s = 0; s < 4; ++s) {
+        r = fixed_stage(h, s, S(j, s), nullptr, S(j, s + 1), tn, dt);
+        if (r) return r;
+      }
+      if (j + 1 < ns) {
+        r = fixed_stage(h, 4, S(j, 4), S(j, 0), S(j + 1, 0), tn, dt);
+        if (r) return r;
+      }
+    }
+    // reverse through the segment's steps: A0 holds the adjoint of the step's result
+    for (int j = ns - 1; j >= 0; --j) {
+      const double tn = h->tr_t0 + (n0 + j) * dt;
+      r = adjoint_stage(h, S(j, 4), A0, nullptr, A1, c_al, c_be, 0.0, stage_time(4, tn, dt));
+      if (!r) r = adjoint_stage(h, S(j, 3), A1, nullptr, A2, 1.0, c, 0.0, stage_time(3, tn, dt));
+      if (!r) r = adjoint_stage(h, S(j, 2), A2, nullptr, A1, 1.0, c, 0.0, stage_time(2, tn, dt));
+      if (!r) r = adjoint_stage(h, S(j, 1), A1, nullptr, A2, 1.0, c, 0.0, stage_time(1, tn, dt));
+      if (!r) r = adjoint_stage(h, S(j, 0), A2, A0, A0, 1.0, c, c_ga, stage_time(0, tn, dt));
+      if (r) return r;
+    }
+  }
+  r = copy_out(h, ubar_0, A0, where);
+  if (r) return r;
+  return finish(h);
+}
+
+apollo_status apollo_dg_tangent(apollo_dg* h, int nsteps, double t0, double dt, const double* du0, double* duT,
+                                int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (nsteps < 0 || !(dt > 0.0) || !du0 || !duT) return APOLLO_ERR_ARG;
+  if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  r = ensure_deriv_buffers(h);
+  if (r) return r;
+  h->tu_valid = false;
+  r = clear_errors(h);
+  if (r) return r;
+  r = copy_in(h, h->tU_d, du0, where);
+  if (r) return r;
+  for (int n = 0; n < nsteps; ++n) {
+    const double tn = t0 + n * dt;
+    for (int s = 0; s < 5; ++s) {
+      // the tangent stage reads the stage's input state before the value stage overwrites it
+      const double* x = s == 0 ? h->U_d : h->W_d;
+      const double* dx = s == 0 ? h->tU_d : h->tW_d;
+      double* dout = s < 4 ? h->tW_d : h->tU_d;
+      r = tangent_stage(h, s, s < 4 ? MODE_STAGE : MODE_FINAL, x, dx, s < 4 ? nullptr : h->tU_d, dout, tn, dt);
+      if (!r) r = fixed_stage(h, s, x, h->U_d, s < 4 ? h->W_d : h->U_d, tn, dt);
+      if (r) return r;
+    }
+  }
+  r = copy_out(h, duT, h->tU_d, where);
+  if (r) return r;
+  return finish(h);
+}
+
+apollo_status apollo_dg_rhs_jvp(apollo_dg* h, double t, const double* x, const double* v, double* out, int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!x || !v || !out) return APOLLO_ERR_ARG;
+  r = ensure_deriv_buffers(h);
+  if (r) return r;
+  r = clear_errors(h);
+  if (r) return r;
+  const double *xd = x, *vd = v;
+  double* od = out;
+  if (where != APOLLO_DEVICE_PTR) {
+    r = copy_in(h, h->in_d, x, where);
+    if (!r) r = copy_in(h, h->tU_d, v, where);
+    if (r) return r;
+    xd = h->in_d;
+    vd = h->tU_d;
+    od = h->out_d;
+  }
+  r = tangent_stage(h, 0, MODE_RHS, xd, vd, nullptr, od, t, 0.0);
+  if (r) return r;
+  if (where != APOLLO_DEVICE_PTR) {
+    r = copy_out(h, out, h->out_d, where);
+    if (r) return r;
+  }
+  return finish(h);
+}
+
+apollo_status apollo_dg_rhs_vjp(apollo_dg* h, double t, const double* x, const double* w, double* out, int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!x || !w || !out) return APOLLO_ERR_ARG;
+  if (where == APOLLO_DEVICE_PTR && (out == x || out == w))
+    return fail(h, APOLLO_ERR_ARG, "the adjoint needs an output distinct from x and w");
+  r = ensure_deriv_buffers(h);
+  if (r) return r;
+  r = clear_errors(h);
+  if (r) return r;
+  const double *xd = x, *wd = w;
+  double* od = out;
+  if (where != APOLLO_DEVICE_PTR) {
+    r = copy_in(h, h->in_d, x, where);
+    if (!r) r = copy_in(h, h->A_d[0], w, where);
+    if (r) return r;
+    xd = h->in_d;
+    wd = h->A_d[0];
+    od = h->out_d;
+  }
+  r = adjoint_stage(h, xd, wd, nullptr, od, 0.0, 1.0, 0.0, t);
+  if (r) return r;
+  if (where != APOLLO_DEVICE_PTR) {
+    r = copy_out(h, out, h->out_d, where);
+    if (r) return r;
+  }
+  return finish(h);
+}
+
+apollo_status apollo_dg_adjoint_memory(const apollo_dg* h, size_t* bytes) {
+  if (!h || !bytes) return APOLLO_ERR_ARG;
+  const size_t nU = (size_t)h->K * h->ops.Np * h->M, nT = (size_t)h->K * h->ops.Nf * h->M;
+  size_t b = 0;
+  if (h->dvol_d) b += (nU * 6 + nT * 3) * sizeof(double);
+  b += h->ckpt.size() * nU * sizeof(double);
+  b += (size_t)5 * h->seg_steps * nU * sizeof(double);
+  *bytes = b;
+  return APOLLO_OK;
+}
 
 apollo_status apollo_dg_destroy(apollo_dg* h) {
   if (!h) return APOLLO_ERR_ARG;

@@ -79,6 +79,12 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_integrals": (C.c_int, [H, C.c_void_p, C.c_int, _dp]),
         "apollo_dg_kernel_times": (C.c_int, [H, C.c_int, C.c_int, _dp, _ip]),
         "apollo_dg_rhs_noalloc": (C.c_int, [H, C.c_double, C.c_double, C.c_void_p, C.c_void_p, _dp, C.c_void_p]),
+        "apollo_dg_forward_fixed": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_int]),
+        "apollo_dg_backward": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_int]),
+        "apollo_dg_tangent": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_int]),
+        "apollo_dg_rhs_jvp": (C.c_int, [H, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+        "apollo_dg_rhs_vjp": (C.c_int, [H, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+        "apollo_dg_adjoint_memory": (C.c_int, [H, C.POINTER(C.c_size_t)]),
         "apollo_dg_last_error": (C.c_char_p, [H]),
         "apollo_dg_destroy": (C.c_int, [H]),
     }
@@ -218,3 +224,48 @@ class NodalDG2d:
             p, where = _ptr(U)
             self._check(self.lib.apollo_dg_integrals(self.h, p, where, sums.ctypes.data_as(_dp)))
         return sums
+
+    # ---- derivatives (float64; fixed step size dt) ------------------------------
+    def _like(self, a, out):
+        if out is not None:
+            return out
+        return np.empty(self.shape) if isinstance(a, np.ndarray) else a.new_empty(a.shape)
+
+    def forward_fixed(self, nsteps: int, t0: float, dt: float, checkpoint_every: int):
+        """Advance the resident state by nsteps fixed steps, keeping checkpoints for backward()."""
+        self._check(self.lib.apollo_dg_forward_fixed(self.h, nsteps, t0, dt, checkpoint_every))
+
+    def backward(self, ubar_T, out=None):
+        """dJ/dU(0) of the last forward_fixed trajectory, given dJ/dU(T)."""
+        out = self._like(ubar_T, out)
+        pi, wi = _ptr(ubar_T)
+        po, wo = _ptr(out)
+        assert wi == wo
+        self._check(self.lib.apollo_dg_backward(self.h, pi, po, wi))
+        return out
+
+    def tangent(self, nsteps: int, t0: float, dt: float, du0, out=None):
+        """Advance the resident state and return (dU(T)/dU(0)) du0."""
+        out = self._like(du0, out)
+        pi, wi = _ptr(du0)
+        po, wo = _ptr(out)
+        assert wi == wo
+        self._check(self.lib.apollo_dg_tangent(self.h, nsteps, t0, dt, pi, po, wi))
+        return out
+
+    def rhs_jvp(self, t: float, x, v, out=None):
+        out = self._like(x, out)
+        (px, wx), (pv, _), (po, _) = _ptr(x), _ptr(v), _ptr(out)
+        self._check(self.lib.apollo_dg_rhs_jvp(self.h, t, px, pv, po, wx))
+        return out
+
+    def rhs_vjp(self, t: float, x, w, out=None):
+        out = self._like(x, out)
+        (px, wx), (pw, _), (po, _) = _ptr(x), _ptr(w), _ptr(out)
+        self._check(self.lib.apollo_dg_rhs_vjp(self.h, t, px, pw, po, wx))
+        return out
+
+    def adjoint_memory(self) -> int:
+        b = C.c_size_t()
+        self._check(self.lib.apollo_dg_adjoint_memory(self.h, C.byref(b)))
+        return b.value

@@ -171,6 +171,36 @@ apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int it
 apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt, const double* in, double* out,
                                     double* suggested_dt, void* stream);
 
+/* ---- Derivatives (float64).  No counterpart in Apollo, which has no adjoint.
+ * A trajectory here is nsteps SSPRK(5,2) steps of FIXED size dt (the adaptive
+ * dt policy of apollo_dg_step is not differentiated); stage times are
+ * t0 + n dt + dt {0, 1/4, 1/2, 3/4, 1}, as in apollo_dg_step. */
+
+/* Advance the resident state by nsteps fixed steps, keeping every
+ * checkpoint_every-th state on the device (ceil(nsteps / checkpoint_every)
+ * states) for apollo_dg_backward. */
+apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, double dt, int checkpoint_every);
+
+/* Discrete adjoint of the last apollo_dg_forward_fixed trajectory: given
+ * ubar_T = dJ/dU(T) (any terminal functional J), writes ubar_0 = dJ/dU(0).
+ * Each checkpoint segment is re-run once, keeping its 5 x checkpoint_every
+ * stage states; then every stage is reversed with the exact transpose of the
+ * float64 right-hand side's linearisation.  [K][Np][m] arrays, host or device. */
+apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* ubar_0, int where);
+
+/* Forward-mode derivative: advances the resident state by nsteps fixed steps
+ * and writes duT = (dU(T)/dU(0)) du0. */
+apollo_status apollo_dg_tangent(apollo_dg* h, int nsteps, double t0, double dt, const double* du0, double* duT,
+                                int where);
+
+/* One right-hand side's derivatives at the state x (time t):
+ * out = L'(x) v (jvp), out = L'(x)^T w (vjp; out distinct from x and w). */
+apollo_status apollo_dg_rhs_jvp(apollo_dg* h, double t, const double* x, const double* v, double* out, int where);
+apollo_status apollo_dg_rhs_vjp(apollo_dg* h, double t, const double* x, const double* w, double* out, int where);
+
+/* Device bytes held for derivatives (scratch, checkpoints, segment states). */
+apollo_status apollo_dg_adjoint_memory(const apollo_dg* h, size_t* bytes);
+
 /* Error text of the last failing call on this handle. */
 const char* apollo_dg_last_error(const apollo_dg* h);
 
