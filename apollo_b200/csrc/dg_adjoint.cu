@@ -214,6 +214,183 @@ __global__ void __launch_bounds__(kDThreads) k_tan_face(DgDev d, const double* _
 }
 
 // ---------------------------------------------------------------- adjoint ----
+// Pointwise transposed Jacobian products, all inline (no calls, so the
+// kernel's stack size is static).  The generic form differentiates the
+// equation's own flux code with Dual<M>: it serves the linear equations
+// (advection, Maxwell), where the dual arithmetic is a few multiply-adds.
+// The Euler form is the reverse sweep of the same computation graph
+// (state -> rho, velocities, pressure -> directional flux; Lax-Friedrichs
+// with the wave speed of the primitive variables).
+template <int M> struct DVec {
+  double v[M];
+};
+
+template <int EQ> struct AdjPhys {
+  static constexpr int M = Eq<EQ>::M;
+  // (dR/dq)^T aR + (dS/dq)^T aS,  R = rx F + ry G,  S = sx F + sy G
+  __device__ __forceinline__ static DVec<M> vol(const EqParams& P, const DVec<M>& q, double rx, double ry,
+                                                double sx, double sy, const DVec<M>& aR, const DVec<M>& aS,
+                                                int* err) {
+    Dual<M> qc[M], F[M], G[M];
+#pragma unroll
+    for (int f = 0; f < M; ++f) {
+      qc[f] = Dual<M>(q.v[f]);
+      qc[f].d[f] = 1.0;
+    }
+    Eq<EQ>::flux2(P, qc, F, G, err);
+    DVec<M> r;
+#pragma unroll
+    for (int j = 0; j < M; ++j) r.v[j] = 0.0;
+#pragma unroll
+    for (int f = 0; f < M; ++f) {
+      const double cF = rx * aR.v[f] + sx * aS.v[f], cG = ry * aR.v[f] + sy * aS.v[f];
+#pragma unroll
+      for (int j = 0; j < M; ++j) r.v[j] += cF * F[f].d[j] + cG * G[f].d[j];
+    }
+    return r;
+  }
+  // (d f*(n, a, b) / d a)^T dv and (d f* / d b)^T dv
+  __device__ __forceinline__ static void face(const EqParams& P, double nx, double ny, const DVec<M>& a,
+                                              const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
+                                              bool want_b, int* err) {
+    for (int side = 0; side < (want_b ? 2 : 1); ++side) {
+      Dual<M> A[M], B[M], nf[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) {
+        A[f] = Dual<M>(a.v[f]);
+        B[f] = Dual<M>(b.v[f]);
+        if (side == 0) A[f].d[f] = 1.0;
+        else B[f].d[f] = 1.0;
+      }
+      Eq<EQ>::numflux(P, Dual<M>(nx), Dual<M>(ny), A, B, nf, err);
+      DVec<M>& out = side == 0 ? abar : bbar;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        double sum = 0.0;
+#pragma unroll
+        for (int f = 0; f < M; ++f) sum += dv.v[f] * nf[f].d[j];
+        out.v[j] = sum;
+      }
+    }
+  }
+};
+
+template <int MF> struct EulerAdj {
+  static constexpr int IE = MF - 1;
+  // qbar += (dR/dq)^T r for the flux R along (ax, ay): reverse sweep of the
+  // flux's own graph with its clamps (rho = max(q0, minD) as a constant when
+  // clamped; p = minP as a constant when clamped),
+  // rho, v = m / rho, p = g1 (E - rho |v|^2 / 2), u = v . a,
+  // R = (rho u, rho vx u + p ax, rho vy u + p ay, [rho vz u], (E + p) u)
+  __device__ __forceinline__ static void dir(const EqParams& P, const double* q, double ax, double ay,
+                                             const double* r, double* qbar, int* err) {
+    const double g1 = P.p[0] - 1.0, minP = P.p[1], minD = P.p[2];
+    double rho = q[0];
+    if (minD == 0.0 && rho <= 0.0) *err |= ERRB_NONPHYS;
+    const bool rho_c = rho < minD;
+    if (rho_c) rho = minD;
+    const double ir = 1.0 / rho;
+    const double vx = q[1] * ir, vy = q[2] * ir, vz = MF == 5 ? q[3] * ir : 0.0, E = q[IE];
+    const double v2 = vx * vx + vy * vy + vz * vz;
+    double p = g1 * (E - 0.5 * rho * v2);
+    bool p_c = false;
+    if (p <= 0.0) {
+      if (minP == 0.0) *err |= ERRB_NONPHYS;
+      else { p = minP; p_c = true; }
+    }
+    const double u = vx * ax + vy * ay;
+    const double r3 = MF == 5 ? r[3] : 0.0;
+    const double ub = r[0] * rho + r[1] * rho * vx + r[2] * rho * vy + r3 * rho * vz + r[IE] * (E + p);
+    const double pb = p_c ? 0.0 : r[1] * ax + r[2] * ay + r[IE] * u;
+    double rhob = (r[0] + r[1] * vx + r[2] * vy + r3 * vz) * u - 0.5 * g1 * v2 * pb;
+    const double vxb = r[1] * rho * u + ub * ax - g1 * rho * vx * pb;
+    const double vyb = r[2] * rho * u + ub * ay - g1 * rho * vy * pb;
+    const double vzb = r3 * rho * u - g1 * rho * vz * pb;
+    rhob -= (vxb * vx + vyb * vy + vzb * vz) * ir;
+    if (!rho_c) qbar[0] += rhob;
+    qbar[1] += vxb * ir;
+    qbar[2] += vyb * ir;
+    if (MF == 5) qbar[3] += vzb * ir;
+    qbar[IE] += r[IE] * u + g1 * pb;
+  }
+  // Lax-Friedrichs wave speed of the primitive variables and its gradient.
+  // Where the primitive variables clamp (non-physical states) the gradient is
+  // taken as zero and NONPHYS is flagged.
+  __device__ __forceinline__ static double speed(const EqParams& P, const double* q, double* grad, int* err) {
+    const double gamma = P.p[0], g1 = gamma - 1.0, minP = P.p[1], minD = P.p[2];
+    const double q3 = MF == 5 ? q[3] : 0.0;
+    if (!(q[0] > 0.0)) {
+      *err |= ERRB_NONPHYS;
+#pragma unroll
+      for (int j = 0; j < MF; ++j) grad[j] = 0.0;
+      return sqrt(gamma * minP / minD);
+    }
+    const double rho = q[0], ir = 1.0 / rho;
+    const double u = q[1] / rho, v = q[2] / rho, w = q3 / rho;
+    double p = g1 * (q[IE] - 0.5 * (q[1] * q[1] + q[2] * q[2] + q3 * q3) / q[0]);
+    const double sp = sqrt(u * u + v * v + w * w);
+    if (p <= 0.0) {
+      *err |= ERRB_NONPHYS;
+#pragma unroll
+      for (int j = 0; j < MF; ++j) grad[j] = 0.0;
+      return sp + sqrt(gamma * minP / rho);
+    }
+    const double cs = sqrt(gamma * p / rho);
+    const double ks = sp > 0.0 ? ir / sp : 0.0;  // d|v|/dm = v / (|v| rho)
+    const double kc = 0.5 * gamma / (cs * rho);   // dcs/dp = kc, dcs/drho = -kc p / rho
+    grad[0] = -sp * ir + kc * (0.5 * g1 * (u * u + v * v + w * w) - p * ir);
+    grad[1] = u * ks - kc * g1 * u;
+    grad[2] = v * ks - kc * g1 * v;
+    if (MF == 5) grad[3] = w * ks - kc * g1 * w;
+    grad[IE] = kc * g1;
+    return sp + cs;
+  }
+};
+
+template <int MF> struct EulerAdjPhys {
+  static constexpr int M = MF;
+  __device__ __forceinline__ static DVec<M> vol(const EqParams& P, const DVec<M>& q, double rx, double ry,
+                                                double sx, double sy, const DVec<M>& aR, const DVec<M>& aS,
+                                                int* err) {
+    DVec<M> r;
+#pragma unroll
+    for (int j = 0; j < M; ++j) r.v[j] = 0.0;
+    EulerAdj<MF>::dir(P, q.v, rx, ry, aR.v, r.v, err);
+    EulerAdj<MF>::dir(P, q.v, sx, sy, aS.v, r.v, err);
+    return r;
+  }
+  // f* = 1/2 [Fn(a) + Fn(b) + lambda (a - b)], lambda = max(c(a), c(b)):
+  // abar = 1/2 [ (dFn(a)/da)^T dv + lambda dv + (dv . (a - b)) grad c(a) [a wins] ]
+  // bbar = 1/2 [ (dFn(b)/db)^T dv - lambda dv + (dv . (a - b)) grad c(b) [b wins] ]
+  __device__ __forceinline__ static void face(const EqParams& P, double nx, double ny, const DVec<M>& a,
+                                              const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
+                                              bool want_b, int* err) {
+    double ga[M], gb[M];
+    const double ca = EulerAdj<MF>::speed(P, a.v, ga, err), cb = EulerAdj<MF>::speed(P, b.v, gb, err);
+    const bool a_wins = ca > cb;  // the branch the forward flux takes
+    const double lam = a_wins ? ca : cb;
+    double jump = 0.0;
+#pragma unroll
+    for (int f = 0; f < M; ++f) jump += dv.v[f] * (a.v[f] - b.v[f]);
+    double fa[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) fa[j] = 0.0;
+    EulerAdj<MF>::dir(P, a.v, nx, ny, dv.v, fa, err);
+#pragma unroll
+    for (int j = 0; j < M; ++j) abar.v[j] = 0.5 * (fa[j] + lam * dv.v[j] + (a_wins ? jump * ga[j] : 0.0));
+    if (want_b) {
+      double fb[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) fb[j] = 0.0;
+      EulerAdj<MF>::dir(P, b.v, nx, ny, dv.v, fb, err);
+#pragma unroll
+      for (int j = 0; j < M; ++j) bbar.v[j] = 0.5 * (fb[j] - lam * dv.v[j] + (a_wins ? 0.0 : jump * gb[j]));
+    }
+  }
+};
+template <> struct AdjPhys<EQ_EULER> : EulerAdjPhys<5> {};
+template <> struct AdjPhys<EQ_EULER2D> : EulerAdjPhys<4> {};
+
 template <int N, int M> struct AdjTile {
   static constexpr int NP = Sizes<N>::NP, NC = Sizes<N>::NC, NF = Sizes<N>::NF;
   static constexpr int E = M == 1 ? 32 : (M >= 5 ? 4 : 8);  // main tile <= 189 KB up to N = 5
@@ -293,7 +470,7 @@ __global__ void __launch_bounds__(kDThreads) k_adj_pre(DgDev d, const double* __
 }
 
 template <int EQ, int N>
-__global__ void __launch_bounds__(kDThreads) k_adj_main(DgDev d, AdjArgs a) {
+__global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
   using P = Eq<EQ>;
   constexpr int M = P::M;
   using T = AdjTile<N, M>;
@@ -347,26 +524,17 @@ __global__ void __launch_bounds__(kDThreads) k_adj_main(DgDev d, AdjArgs a) {
     // volume: g = (dR/dqc)^T a_R + (dS/dqc)^T a_S at every cubature point
     for (int idx = tid; idx < ne * NC; idx += kDThreads) {
       const int e = idx / NC, c = idx - e * NC;
-      Dual<M> qc[M], F[M], G[M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) {
-        qc[f] = Dual<M>(sQC[c * LDB + e * M + f]);
-        qc[f].d[f] = 1.0;
-      }
-      P::flux2(d.eqp, qc, F, G, &err);
       const ElemGeo& g = d.geo[k0 + e];
-      double gbar[M];
-#pragma unroll
-      for (int j = 0; j < M; ++j) gbar[j] = 0.0;
+      DVec<M> q, aR, aS;
 #pragma unroll
       for (int f = 0; f < M; ++f) {
-        const double aR = sAB[c * LDB + e * M + f], aS = sAB[(NC + c) * LDB + e * M + f];
-        const double cF = g.rx * aR + g.sx * aS, cG = g.ry * aR + g.sy * aS;
-#pragma unroll
-        for (int j = 0; j < M; ++j) gbar[j] += cF * F[f].d[j] + cG * G[f].d[j];
+        q.v[f] = sQC[c * LDB + e * M + f];
+        aR.v[f] = sAB[c * LDB + e * M + f];
+        aS.v[f] = sAB[(NC + c) * LDB + e * M + f];
       }
+      const DVec<M> gbar = AdjPhys<EQ>::vol(d.eqp, q, g.rx, g.ry, g.sx, g.sy, aR, aS, &err);
 #pragma unroll
-      for (int j = 0; j < M; ++j) sQC[c * LDB + e * M + j] = gbar[j];
+      for (int j = 0; j < M; ++j) sQC[c * LDB + e * M + j] = gbar.v[j];
     }
     // faces: w_g (s_own - s_partner) d f*(n_own, a, b) / d a at every Gauss point
     for (int idx = tid; idx < ne * NF; idx += kDThreads) {
@@ -375,24 +543,24 @@ __global__ void __launch_bounds__(kDThreads) k_adj_main(DgDev d, AdjArgs a) {
       const ElemGeo& g = d.geo[k];
       const int nb = d.conn[(size_t)k * 6 + 2 * fc];
       const size_t own = ((size_t)k * NF + fg) * M;
-      Dual<M> A[M], B[M], nf[M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) {
-        A[f] = Dual<M>(d.trace[own + f]);
-        A[f].d[f] = 1.0;
-      }
-      double dvec[M];
+      DVec<M> abar;
       if (nb >= 0) {
         const int f2 = d.conn[(size_t)k * 6 + 2 * fc + 1];
         const size_t par = ((size_t)nb * NF + f2 * NG + (NG - 1 - gq)) * M;
         // the flux's Gauss weight is its first side's (face list: 3 nb + f2 > 3 k + fc)
         const double w = d.gw[(3 * nb + f2 > 3 * k + fc) ? gq : NG - 1 - gq] * g.sJ[fc];
+        DVec<M> qa, qb, dvec;
 #pragma unroll
         for (int f = 0; f < M; ++f) {
-          B[f] = Dual<M>(d.trace[par + f]);
-          dvec[f] = w * (a.sbar[own + f] - a.sbar[par + f]);
+          qa.v[f] = d.trace[own + f];
+          qb.v[f] = d.trace[par + f];
+          dvec.v[f] = w * (a.sbar[own + f] - a.sbar[par + f]);
         }
+        DVec<M> unused;
+        AdjPhys<EQ>::face(d.eqp, g.nx[fc], g.ny[fc], qa, qb, dvec, abar, unused, false, &err);
       } else {
+        // boundary: ghost state b = A a + c (every supported boundary hook is
+        // affine in the trace); abar = (df*/da)^T dv + A^T (df*/db)^T dv
         const double w = d.gw[gq] * g.sJ[fc];
         const double z = d.gz[gq];
         double r, s;
@@ -401,18 +569,30 @@ __global__ void __launch_bounds__(kDThreads) k_adj_main(DgDev d, AdjArgs a) {
         else { r = -1.0; s = -z; }
         const double xx = 0.5 * (-g.vx[0] * (r + s) + g.vx[1] * (1. + r) + g.vx[2] * (1. + s));
         const double yy = 0.5 * (-g.vy[0] * (r + s) + g.vy[1] * (1. + r) + g.vy[2] * (1. + s));
-        apply_bc<EQ, Dual<M>>(d.bcs, -nb, a.t, xx, yy, Dual<M>(g.nx[fc]), Dual<M>(g.ny[fc]), A, B);
+        DVec<M> qa, qb, dvec, bbar;
+        double unit[M], col[M], base[M], zero[M];
 #pragma unroll
-        for (int f = 0; f < M; ++f) dvec[f] = w * a.sbar[own + f];
+        for (int f = 0; f < M; ++f) {
+          qa.v[f] = d.trace[own + f];
+          dvec.v[f] = w * a.sbar[own + f];
+          zero[f] = 0.0;
+        }
+        apply_bc<EQ, double>(d.bcs, -nb, a.t, xx, yy, g.nx[fc], g.ny[fc], qa.v, qb.v);
+        AdjPhys<EQ>::face(d.eqp, g.nx[fc], g.ny[fc], qa, qb, dvec, abar, bbar, true, &err);
+        apply_bc<EQ, double>(d.bcs, -nb, a.t, xx, yy, g.nx[fc], g.ny[fc], zero, base);
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+#pragma unroll
+          for (int f = 0; f < M; ++f) unit[f] = f == j ? 1.0 : 0.0;
+          apply_bc<EQ, double>(d.bcs, -nb, a.t, xx, yy, g.nx[fc], g.ny[fc], unit, col);
+          double sum = 0.0;
+#pragma unroll
+          for (int f = 0; f < M; ++f) sum += (col[f] - base[f]) * bbar.v[f];
+          abar.v[j] += sum;
+        }
       }
-      P::numflux(d.eqp, Dual<M>(g.nx[fc]), Dual<M>(g.ny[fc]), A, B, nf, &err);
 #pragma unroll
-      for (int j = 0; j < M; ++j) {
-        double s = 0.0;
-#pragma unroll
-        for (int f = 0; f < M; ++f) s += dvec[f] * nf[f].d[j];
-        sAF[fg * LDB + e * M + j] = s;
-      }
+      for (int j = 0; j < M; ++j) sAF[fg * LDB + e * M + j] = abar.v[j];
     }
     __syncthreads();
     block_dgemm<T::NPR, T::COLS, T::NCK, T::LDAC, LDB, kDWarps>(

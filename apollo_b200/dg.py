@@ -103,7 +103,14 @@ def _ptr(a):
         return C.c_void_p(a.ctypes.data), APOLLO_HOST_PTR
     # torch tensor
     assert a.dtype.__repr__().endswith("float64") and a.is_contiguous()
-    return C.c_void_p(a.data_ptr()), APOLLO_DEVICE_PTR if a.is_cuda else APOLLO_HOST_PTR
+    if a.is_cuda:
+        # the library works on its own stream: whatever torch queued that
+        # produces or still reads this tensor must finish first (the library's
+        # calls return with their own stream synchronised)
+        import torch
+        torch.cuda.current_stream(a.device).synchronize()
+        return C.c_void_p(a.data_ptr()), APOLLO_DEVICE_PTR
+    return C.c_void_p(a.data_ptr()), APOLLO_HOST_PTR
 
 
 class NodalDG2d:

@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-l2-500", action="store_true", help="skip the 500-step mixed vs float64 comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint measurement")
+    ap.add_argument("--adjoint-dirs", type=int, default=32,
+                    help="random directions of the adjoint's finite-difference check")
     ap.add_argument("--rhs-only", type=int, default=0,
                     help="profiling driver: set up the workload, run this many RHS evaluations, exit")
     return ap.parse_args()
@@ -65,6 +68,84 @@ def rhs_only(args):
                       "checksum": float(out.abs().sum().item())}))
     s.close()
     return 0
+
+
+def adjoint_measure(args, device: int):
+    """The discrete-adjoint configuration: Euler vortex on a 128 x 128 vertex
+    grid (K = 32,258), N = 3, 400 fixed SSPRK(5,2) steps, checkpoints every 20.
+    J = 0.5 ||U(T) - U_target||^2 with U_target the float64 forward of the
+    vortex and U(0) = vortex + N(0, 1e-3^2) (seeded).  Reports the time of the
+    forward (with checkpoints) and of the backward (segment re-runs + reverse
+    stages), the derivative memory, and the gradient checked against central
+    finite differences and the forward-mode derivative on random directions."""
+    import torch
+    from apollo_b200 import NodalDG2d, problems
+    p = problems.euler_vortex(n=128, N=3)
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=device)
+    x, y = s.node_coords()
+    u_ic = np.ascontiguousarray(p.ic(x, y))
+    s.set_state(u_ic)
+    dt = s.init_dt()
+    nsteps, every = 400, 20
+    s.forward_fixed(nsteps, 0.0, dt, every)
+    target = torch.from_numpy(s.get_state()).cuda(device)
+    rng = np.random.default_rng(0)
+    u0 = torch.from_numpy(u_ic + 1e-3 * rng.standard_normal(u_ic.shape)).cuda(device)
+    uT = torch.empty_like(u0)
+    grad = torch.empty_like(u0)
+
+    def J(u):
+        s.set_state(u)
+        s.forward_fixed(nsteps, 0.0, dt, every)
+        s.get_state(uT)
+        return 0.5 * float(((uT - target) ** 2).sum())
+
+    J(u0)
+    s.backward(uT - target, out=grad)  # warm-up: buffers allocated
+    torch.cuda.synchronize()
+    fwd, bwd = [], []
+    for _ in range(3):
+        s.set_state(u0)
+        t0 = time.perf_counter()
+        s.forward_fixed(nsteps, 0.0, dt, every)
+        t1 = time.perf_counter()
+        s.get_state(uT)
+        gT = uT - target
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        s.backward(gT, out=grad)
+        t3 = time.perf_counter()
+        fwd.append(t1 - t0)
+        bwd.append(t3 - t2)
+    g = grad.cpu().numpy()
+    gT_host = (uT - target).cpu().numpy()
+    fd_err, tan_err = [], []
+    drng = np.random.default_rng(1)
+    for i in range(args.adjoint_dirs):
+        d = torch.from_numpy(drng.standard_normal(u_ic.shape)).cuda(device)
+        eps = 1e-6
+        fd = (J(u0 + eps * d) - J(u0 - eps * d)) / (2 * eps)
+        ga = float(np.vdot(g, d.cpu().numpy()))
+        fd_err.append(abs(ga - fd) / abs(fd))
+        if i < 4:
+            s.set_state(u0)
+            du = s.tangent(nsteps, 0.0, dt, d)
+            gt = float(np.vdot(gT_host, du.cpu().numpy()))
+            tan_err.append(abs(ga - gt) / abs(gt))
+    nU = s.K * s.Np * s.m * 8
+    out = {
+        "config": {"workload": "euler_vortex_N3_K32258_400steps", "K": s.K, "N": 3, "fields": s.m, "steps": nsteps,
+                   "checkpoint_every": every, "dt": dt, "functional": "0.5 ||U(T) - U_target||^2"},
+        "forward_ms": 1000 * float(np.median(fwd)), "backward_ms": 1000 * float(np.median(bwd)),
+        "adjoint_over_forward": float(np.median(bwd) / np.median(fwd)),
+        "derivative_memory_mb": s.adjoint_memory() / 2**20,
+        "state_mb": nU / 2**20,
+        "fd_directions": args.adjoint_dirs, "fd_max_rel_err": max(fd_err) if fd_err else None,
+        "tangent_max_rel_err": max(tan_err) if tan_err else None,
+        "how": "wall clock around the synchronous C-ABI calls (median of 3); float64; fixed dt",
+    }
+    s.close()
+    return out
 
 
 def dist_env():
@@ -362,6 +443,15 @@ def ours_arm(args):
             cpu = cpu_sample()
         except Exception as exc:  # the CPU arm never hides a GPU result
             cpu = {"value": None, "error": str(exc)}
+
+    adj = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        try:
+            adj = adjoint_measure(args, local)
+        except Exception as exc:  # reported, never hides the headline
+            adj = {"error": str(exc)}
+    if adj is not None:
+        extra["adjoint"] = adj
 
     if rank == 0:
         # our kernels per step: float64 5 x (volume, face, lift) + finalize;
