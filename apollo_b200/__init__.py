@@ -5,7 +5,7 @@ in include/apollo_dg.h); this package holds its Python binding (``dg``), mesh
 generation (``mesh``) and the benchmark problems (``problems``).
 """
 from .mesh import Mesh, jittered_square, grid_for_elements
-from .dg import NodalDG2d, ApolloError, load_library, LIB_PATH, FIELDS
+from .dg import NodalDG2d, NodalDG2dBatch, ApolloError, load_library, LIB_PATH, FIELDS
 
-__all__ = ["Mesh", "jittered_square", "grid_for_elements", "NodalDG2d", "ApolloError", "load_library",
+__all__ = ["Mesh", "jittered_square", "grid_for_elements", "NodalDG2d", "NodalDG2dBatch", "ApolloError", "load_library",
            "LIB_PATH", "FIELDS"]

@@ -30,7 +30,7 @@ struct DevState {
   double t;          // time at the start of the current step
   double dt;         // dt of the current step
   double tend;       // end time (<= 0: none)
-  double pad0;
+  double dtfac;      // 2/3 * cfl * dtscale of this instance (the dt policy's factor)
   unsigned long long lam_bits;  // max numerical-flux speed of the current stage (bits of a double >= 0)
   int err;           // ErrBits
   int steps;         // steps completed
@@ -49,6 +49,12 @@ struct DgDev {
   const ElemGeo* geo;
   const FaceRec* faces;
   const int* conn;  // [K][6]: per face (neighbour element, its face) or (-tag, -1) on a boundary
+  // batched ensembles: instance of each element (nullptr: one instance) and the
+  // number of instances; st then holds one DevState per instance (the error
+  // word of st[0] serves them all)
+  const int* einst;
+  int ninst;
+  int grid_div;  // launch shape: persistent grids use SMs / grid_div (>= 1; 0 means 1)
   const double *V, *Dr, *Ds, *I, *L, *gz, *gw;
   double *vol, *trace, *flux;  // scratch: [K][NP][M], [K][NF][M], [K][NF][M]
   DevState* st;
@@ -57,6 +63,44 @@ struct DgDev {
   double dtfac;  // 2/3 * cfl * dtscale
   double rmin;
 };
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ int inst_of(const DgDev& d, int k) { return d.einst ? d.einst[k] : 0; }
+
+// Per-instance maximum of non-negative wave speeds: a thread accumulates while
+// its points stay in one instance and flushes (atomic max on the bit pattern,
+// which orders like the value for non-negative doubles) when the instance
+// changes; flush_warp, called by all 32 lanes, combines a warp whose lanes end
+// in one instance.
+struct LamAcc {
+  int inst = -1;
+  double v = 0.0;
+  __device__ __forceinline__ void add(DevState* st, int i, double l) {
+    if (i != inst) {
+      if (inst >= 0 && v > 0.0) atomicMax(&st[inst].lam_bits, (unsigned long long)__double_as_longlong(v));
+      inst = i;
+      v = 0.0;
+    }
+    v = l > v ? l : v;
+  }
+  __device__ __forceinline__ void flush_warp(DevState* st) {
+    const unsigned grp = __match_any_sync(0xffffffffu, inst);
+    if (grp == 0xffffffffu) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = t > v ? t : v;
+      }
+      if ((threadIdx.x & 31) == 0 && inst >= 0 && v > 0.0)
+        atomicMax(&st[inst].lam_bits, (unsigned long long)__double_as_longlong(v));
+    } else if (inst >= 0 && v > 0.0) {
+      atomicMax(&st[inst].lam_bits, (unsigned long long)__double_as_longlong(v));
+    }
+    inst = -1;
+    v = 0.0;
+  }
+};
+#endif
 
 enum StageMode : int { MODE_RHS = 0, MODE_STAGE = 1, MODE_FINAL = 2 };
 
@@ -93,6 +137,8 @@ cudaError_t launch_rhs_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStre
 cudaError_t launch_lift_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStream_t s);
 cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStream_t s);
 cudaError_t launch_finalize(const DgDev& d, cudaStream_t s);
+// st[i].lam_bits = 0 for every instance
+cudaError_t launch_reset_lambda(const DgDev& d, cudaStream_t s);
 cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wJ, cudaStream_t s);
 int fp64_supported(int eq, int N);
 

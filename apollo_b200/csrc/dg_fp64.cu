@@ -26,10 +26,6 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
-  // non-negative doubles order like their bit patterns
-  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
-}
 
 // Tile of elements for the float64 volume kernel.  Columns of every GEMM are
 // (element, field) pairs; rows are cubature points, Gauss points or nodes.
@@ -71,7 +67,8 @@ __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
   double* sQ = smem + T::OFF_Q;
   double* sRS = smem + T::OFF_RS;
   const int tid = threadIdx.x;
-  if (a.reset_lambda && blockIdx.x == 0 && tid == 0) d.st->lam_bits = 0ull;
+  if (a.reset_lambda && blockIdx.x == 0)
+    for (int i = tid; i < d.ninst; i += kThreads) d.st[i].lam_bits = 0ull;
   // operators, zero-padded: V [NCR][NPK], D = [Dr | Ds] [NPR][K2], I [NFR][NPK]
   for (int i = tid; i < T::NCR * T::LDA1; i += kThreads) {
     const int r = i / T::LDA1, c = i % T::LDA1;
@@ -142,13 +139,18 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
   using P = Eq<EQ>;
   constexpr int M = P::M;
   constexpr int NG = Sizes<N>::NG, NF = Sizes<N>::NF;
-  const double t = a.time_from_state ? d.st->t + d.st->dt * a.frac : a.t_arg;
   int err = 0;
-  double lmax = 0.0;
+  LamAcc lam_acc;
+  // each block takes a contiguous range of face points, so a thread's points
+  // stay within one instance of a batched ensemble
   const int total = d.nfaces * NG;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+  const int per_block = (total + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per_block, i1 = min(total, i0 + per_block);
+  for (int idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
     const int fi = idx / NG, gq = idx - fi * NG;
     const FaceRec fr = d.faces[fi];
+    const int inst = inst_of(d, fr.k1);
+    const double t = a.time_from_state ? d.st[inst].t + d.st[inst].dt * a.frac : a.t_arg;
     const ElemGeo& g = d.geo[fr.k1];
     const double nx = g.nx[fr.f1], ny = g.ny[fr.f1], sJ = g.sJ[fr.f1];
     double qM[M], qP[M], nf[M];
@@ -172,8 +174,7 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
       apply_bc<EQ, double>(d.bcs, -fr.k2, t, x, y, nx, ny, qM, qP);
     }
     double lam = P::numflux(d.eqp, nx, ny, qM, qP, nf, &err);
-    lam = fabs(lam);
-    lmax = lam > lmax ? lam : lmax;
+    lam_acc.add(d.st, inst, fabs(lam));
     const double w = d.gw[gq] * sJ;
     double* om = d.flux + ((size_t)fr.k1 * NF + fr.f1 * NG + gq) * M;
 #pragma unroll
@@ -184,13 +185,7 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
       for (int f = 0; f < M; ++f) op[f] = -(nf[f] * w);
     }
   }
-  // block max of the wave speed, one atomic per warp
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    double v = __shfl_xor_sync(0xffffffffu, lmax, o);
-    lmax = v > lmax ? v : lmax;
-  }
-  if ((threadIdx.x & 31) == 0 && lmax > 0.0) atomic_max_nonneg(&d.st->lam_bits, lmax);
+  lam_acc.flush_warp(d.st);
   if (err) atomicOr(&d.st->err, err);
 }
 
@@ -222,9 +217,6 @@ __global__ void __launch_bounds__(kThreads) k_lift(DgDev d, StageArgs a) {
     sL[i] = (r < NP && c < NF) ? d.L[r * NF + c] : 0.0;
   }
   for (int i = tid; i < T::NFK * LDB; i += kThreads) sF[i] = 0.0;
-  const double dt = a.time_from_state ? d.st->dt : a.dt_arg;
-  const double c_stage = dt / 4.0;  // dt/(s-1), s = 5
-  const double c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
   int err = 0;
   const int ntiles = (d.K + E - 1) / E;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -243,6 +235,9 @@ __global__ void __launch_bounds__(kThreads) k_lift(DgDev d, StageArgs a) {
       if (i >= NP || e >= ne) return;
       const int k = k0 + e;
       const size_t off = ((size_t)k * NP + i) * M + f;
+      const double dt = a.time_from_state ? d.st[inst_of(d, k)].dt : a.dt_arg;
+      const double c_stage = dt / 4.0;  // dt/(s-1), s = 5
+      const double c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
       const double r = d.vol[off] - d.geo[k].invJ * v;
       if (r != r) err |= ERRB_NAN;
       double o;
@@ -258,30 +253,29 @@ __global__ void __launch_bounds__(kThreads) k_lift(DgDev d, StageArgs a) {
 template <int EQ>
 __global__ void k_init_speed(DgDev d, const double* u, int nnodes) {
   constexpr int M = Eq<EQ>::M;
-  double lmax = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnodes; i += gridDim.x * blockDim.x) {
+  LamAcc lam_acc;
+  const int per_block = (nnodes + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per_block, i1 = min(nnodes, i0 + per_block);
+  const int np = nnodes / d.K;
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     double q[M];
 #pragma unroll
     for (int f = 0; f < M; ++f) q[f] = u[(size_t)i * M + f];
     double s2 = Eq<EQ>::speed2(d.eqp, q);
-    double lam = sqrt(s2 > 0.0 ? s2 : 0.0);
-    lmax = lam > lmax ? lam : lmax;
+    lam_acc.add(d.st, inst_of(d, i / np), sqrt(s2 > 0.0 ? s2 : 0.0));
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    double v = __shfl_xor_sync(0xffffffffu, lmax, o);
-    lmax = v > lmax ? v : lmax;
-  }
-  if ((threadIdx.x & 31) == 0 && lmax > 0.0) atomic_max_nonneg(&d.st->lam_bits, lmax);
+  lam_acc.flush_warp(d.st);
 }
 
 // After a step: t += dt; dt = min(dt, suggestion of the last stage), clipped
 // to the end time (ApSolver::ComputeRHSforTS + MonitorVTK,
 // src/solvers/apsolver.cc:421-480).
 __global__ void k_finalize(DgDev d) {
-  DevState* st = d.st;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.ninst) return;
+  DevState* st = d.st + i;
   const double lam = __longlong_as_double((long long)st->lam_bits);
-  const double sugg = d.dtfac * (d.rmin / lam);
+  const double sugg = (st->dtfac > 0.0 ? st->dtfac : d.dtfac) * (d.rmin / lam);
   st->last_sugg = sugg;
   const double dt = st->dt;
   const double t = st->t + dt;
@@ -342,7 +336,7 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
     if (e != cudaSuccess) return e;
     configured |= 1u << (dev & 31);
   }
-  const int sms = num_sms();
+  const int sms = d.grid_div > 1 ? (num_sms() + d.grid_div - 1) / d.grid_div : num_sms();
   const int vt = (d.K + VT::E - 1) / VT::E;
   int per_sm = (int)((200 * 1024) / VT::BYTES);
   if (per_sm < 1) per_sm = 1;
@@ -459,8 +453,18 @@ cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStrea
   return cudaGetLastError();
 }
 
+__global__ void k_reset_lambda(DevState* st, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) st[i].lam_bits = 0ull;
+}
+
 cudaError_t launch_finalize(const DgDev& d, cudaStream_t s) {
-  k_finalize<<<1, 1, 0, s>>>(d);
+  k_finalize<<<(d.ninst + 127) / 128, 128, 0, s>>>(d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reset_lambda(const DgDev& d, cudaStream_t s) {
+  k_reset_lambda<<<(d.ninst + 127) / 128, 128, 0, s>>>(d.st, d.ninst);
   return cudaGetLastError();
 }
 

@@ -38,6 +38,11 @@ struct apollo_dg {
   FaceRec* faces_d = nullptr;
   int* conn_d = nullptr;
   std::vector<int> conn_h;
+  // batched ensembles: instance of each element, number of instances (st_d and
+  // st_h then hold one DevState per instance)
+  int* einst_d = nullptr;
+  int ninst = 1;
+  int grid_div = 1;  // launch shape picked by the batch autotuner
   double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
          *gw_d = nullptr, *wmass_d = nullptr;
   double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
@@ -100,7 +105,7 @@ void dfree(T*& p) {
 void free_mesh(apollo_dg* h) {
   for (auto& g : h->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-  dfree(h->geo_d); dfree(h->faces_d); dfree(h->conn_d);
+  dfree(h->geo_d); dfree(h->faces_d); dfree(h->conn_d); dfree(h->einst_d);
   dfree(h->V_d); dfree(h->Dr_d); dfree(h->Ds_d); dfree(h->I_d); dfree(h->L_d); dfree(h->gz_d); dfree(h->gw_d);
   dfree(h->wmass_d);
   dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
@@ -117,6 +122,7 @@ void free_mesh(apollo_dg* h) {
   dfree(h->vol_d); dfree(h->trace_d); dfree(h->flux_d);
   if (h->mixed) { mixed_destroy(h->mixed); h->mixed = nullptr; }
   h->have_state = false;
+  h->ninst = 1;
 }
 
 template <class T>
@@ -137,6 +143,9 @@ DgDev make_dev(const apollo_dg* h) {
   d.V = h->V_d; d.Dr = h->Dr_d; d.Ds = h->Ds_d; d.I = h->I_d; d.L = h->L_d; d.gz = h->gz_d; d.gw = h->gw_d;
   d.vol = h->vol_d; d.trace = h->trace_d; d.flux = h->flux_d;
   d.st = h->st_d;
+  d.einst = h->einst_d;
+  d.ninst = h->ninst;
+  d.grid_div = h->grid_div;
   d.eqp = h->eqp;
   d.bcs = h->bcs;
   d.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
@@ -535,6 +544,7 @@ apollo_status apollo_dg_step_async(apollo_dg* h, int nsteps, double t, double dt
   s.t = t;
   s.dt = dt;
   s.tend = 0.0;
+  s.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
   std::memcpy(h->st_h, &s, sizeof(DevState));
   CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
   cudaGraphExec_t g = nullptr;
@@ -576,6 +586,7 @@ apollo_status apollo_dg_step(apollo_dg* h, int nsteps, double* t, double* dt, do
     s.t = tt;
     s.dt = dd;
     s.tend = tend;
+    s.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
     std::memcpy(h->st_h, &s, sizeof(DevState));
     CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
     cudaGraphExec_t g = nullptr;
@@ -774,6 +785,94 @@ bool handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size
 
 void handle_set_error(apollo_dg* h, const char* msg) {
   if (h) h->err = msg;
+}
+
+// ---- batched ensembles (dg_batch.cpp): one handle holds several independent
+// meshes of one order, element ranges by instance
+apollo_status handle_set_instances(apollo_dg* h, int ninst, const int* einst) {
+  if (!h || h->K == 0 || ninst < 1) return APOLLO_ERR_ARG;
+  DevState* st_d = nullptr;
+  DevState* st_h = nullptr;
+  CK(cudaMalloc((void**)&st_d, (size_t)ninst * sizeof(DevState)), "instance states");
+  if (cudaMallocHost((void**)&st_h, (size_t)ninst * sizeof(DevState)) != cudaSuccess) {
+    cudaFree(st_d);
+    return fail(h, APOLLO_ERR_ALLOC, "instance states");
+  }
+  std::memset(st_h, 0, (size_t)ninst * sizeof(DevState));
+  CK(cudaMemcpy(st_d, st_h, (size_t)ninst * sizeof(DevState), cudaMemcpyHostToDevice), "instance states");
+  dfree(h->st_d);
+  if (h->st_h) cudaFreeHost(h->st_h);
+  h->st_d = st_d;
+  h->st_h = st_h;
+  dfree(h->einst_d);
+  CK(upload(&h->einst_d, einst, (size_t)h->K), "instance map");
+  h->ninst = ninst;
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return APOLLO_OK;
+}
+
+cudaStream_t handle_stream(const apollo_dg* h) { return h->stream; }
+DevState* handle_states_host(apollo_dg* h) { return h->st_h; }
+
+// host states <-> device states (all instances), on the handle's stream
+apollo_status handle_push_states(apollo_dg* h) {
+  CK(cudaMemcpyAsync(h->st_d, h->st_h, (size_t)h->ninst * sizeof(DevState), cudaMemcpyHostToDevice, h->stream),
+     "states");
+  return APOLLO_OK;
+}
+apollo_status handle_pull_states(apollo_dg* h) {
+  CK(cudaMemcpyAsync(h->st_h, h->st_d, (size_t)h->ninst * sizeof(DevState), cudaMemcpyDeviceToHost, h->stream),
+     "states");
+  return APOLLO_OK;
+}
+
+// per-instance wave speed of the resident state (into st_d[i].lam_bits)
+apollo_status handle_init_speed(apollo_dg* h) {
+  DgDev d = make_dev(h);
+  CK(launch_reset_lambda(d, h->stream), "init speed");
+  CK(launch_init_speed(h->eq, d, h->U_d, h->stream), "init speed");
+  return APOLLO_OK;
+}
+
+double handle_rmin(const apollo_dg* h) { return h->ops.rmin; }
+double handle_cfl(const apollo_dg* h) { return h->cfg.cfl; }
+size_t handle_state_doubles(const apollo_dg* h) { return (size_t)h->K * h->ops.Np * h->M; }
+double* handle_state_device(apollo_dg* h) { return h->U_d; }
+void handle_mark_state(apollo_dg* h) {
+  h->have_state = true;
+  h->tu_valid = false;
+}
+
+// one step (5 stages + finalize) of every instance into the handle's stream,
+// as a captured graph; the mixed form first rebuilds the traces of U if stale
+apollo_status handle_enqueue_step(apollo_dg* h, apollo_precision prec) {
+  cudaGraphExec_t g = nullptr;
+  apollo_status r = step_graph(h, prec, &g);
+  if (r) return r;
+  CK(cudaGraphLaunch(g, h->stream), "graph launch");
+  return APOLLO_OK;
+}
+apollo_status handle_enqueue_step_raw(apollo_dg* h, apollo_precision prec) { return enqueue_step(h, prec); }
+apollo_status handle_prepare_step(apollo_dg* h, apollo_precision prec) {
+  if (prec == APOLLO_PREC_MIXED && h->mixed && !h->tu_valid) {
+    DgDev d = make_dev(h);
+    CK(mixed_launch_traces(h->mixed, d, h->U_d, h->TU_d, h->stream), "trace launch");
+    h->tu_valid = true;
+  }
+  if (prec != APOLLO_PREC_MIXED) h->tu_valid = false;
+  if (prec == APOLLO_PREC_MIXED && !h->mixed)
+    return fail(h, APOLLO_ERR_CONFIG, "mixed precision is not available for this equation/order");
+  return APOLLO_OK;
+}
+apollo_status handle_read_errors(apollo_dg* h) { return read_errors(h); }
+void handle_set_grid_div(apollo_dg* h, int div) {
+  if (div < 1) div = 1;
+  if (div != h->grid_div) {
+    h->grid_div = div;
+    for (auto& g : h->graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
 }
 
 }  // namespace apollo

@@ -517,11 +517,15 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     // ======================= workers =======================
     const int wtid = tid;  // 0 .. NW-1
     const uint32_t tlane = tb + ((uint32_t)(32 * (warp & 3)) << 16);
-    const double tstage = a.time_from_state ? d.st->t + d.st->dt * a.frac : a.t_arg;
-    const double dt = a.time_from_state ? d.st->dt : a.dt_arg;
+    // stage time and dt of an element's instance (batched ensembles)
+    auto stage_t = [&](int k) {
+      const DevState& S = d.st[inst_of(d, k)];
+      return a.time_from_state ? S.t + S.dt * a.frac : a.t_arg;
+    };
+    auto stage_dt = [&](int k) { return a.time_from_state ? d.st[inst_of(d, k)].dt : a.dt_arg; };
     const bool want_lambda = a.mode != MODE_STAGE;
     const bool write_traces = a.tr_out != nullptr && a.mode != MODE_RHS;
-    double lmax = 0.0;
+    LamAcc lam_acc;
     // this thread's tile row (element, field)
     const int rr = tid & 127, rq = rr >> 5, rln = rr & 31;
     const int rel = rln / M, rf = rln - rel * M, re = rq * EPQ + rel;
@@ -797,13 +801,10 @@ __global__ void __launch_bounds__(kMixThreads, 1)
               if (nb < 0) {
                 double x, y;
                 bc_coords(k, fc, g, x, y);
-                apply_bc<EQ, float>(d.bcs, -nb, tstage, x, y, nx, ny, qM, qP);
+                apply_bc<EQ, float>(d.bcs, -nb, stage_t(k), x, y, nx, ny, qM, qP);
               }
               const float lam = Q::lf(d.eqp, nx, ny, qM, qP, nf, &err);
-              if (want_lambda) {
-                const double l = fabs((double)lam);
-                lmax = l > lmax ? l : lmax;
-              }
+              if (want_lambda) lam_acc.add(d.st, inst_of(d, k), fabs((double)lam));
               const float w = GEO[(10 + fc) * E + e];
 #pragma unroll
               for (int f = 0; f < M; ++f) dev[f] = w * (nf[f] - P0[((2 + fc) * M + f) * E + e]);
@@ -850,6 +851,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         const int k = k0 + re;
         const double Rbar = Rb[rf * E + re], Sbar = Rb[(M + rf) * E + re];
         const double F0 = Fb[(0 * M + rf) * E + re], F1 = Fb[(1 * M + rf) * E + re], F2 = Fb[(2 * M + rf) * E + re];
+        const double dt = stage_dt(k);
         const double c_stage = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
         const double* XSb = xs_buf(i);
         const int nx = x_bulk ? x_copy_doubles(tile) : 0;
@@ -943,14 +945,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     }
     // partner-trace copies still in flight after an abort land before the exit
     asm volatile("cp.async.wait_all;" ::: "memory");
-    if (want_lambda) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double v = __shfl_xor_sync(0xffffffffu, lmax, o);
-        lmax = v > lmax ? v : lmax;
-      }
-      if (lane == 0 && lmax > 0.0) atomicMax(&d.st->lam_bits, (unsigned long long)__double_as_longlong(lmax));
-    }
+    if (want_lambda) lam_acc.flush_warp(d.st);
   }
   if (err) atomicOr(&d.st->err, err);
   umma::fence_before_sync();
@@ -1022,12 +1017,13 @@ cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a0, cu
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (d.grid_div > 1) sms = (sms + d.grid_div - 1) / d.grid_div;
     const int ntiles = (d.K + C::E - 1) / C::E;
     int grid = sms;
     if (grid > ntiles) grid = ntiles;
     StageArgs a = a0;
     if (a.reset_lambda && a.mode != MODE_STAGE) {
-      cudaError_t e = cudaMemsetAsync(&d.st->lam_bits, 0, sizeof(unsigned long long), s);
+      cudaError_t e = launch_reset_lambda(d, s);
       if (e != cudaSuccess) return e;
     }
     if (ev) cudaEventRecord(ev[0], s);

@@ -82,6 +82,8 @@ extern "C" apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt
   // per-call state starts at zero (wave-speed maximum, error word); the three
   // arrays are written in full by the kernels before they are read
   d.st = (DevState*)p;
+  d.einst = nullptr;  // one DevState in the array's header: a single instance
+  d.ninst = 1;
   d.vol = (double*)(p + kHeader);
   d.trace = (double*)(p + kHeader + align256(nU * sizeof(double)));
   d.flux = (double*)(p + kHeader + align256(nU * sizeof(double)) + align256(nT * sizeof(double)));

@@ -85,6 +85,20 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_rhs_jvp": (C.c_int, [H, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
         "apollo_dg_rhs_vjp": (C.c_int, [H, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
         "apollo_dg_adjoint_memory": (C.c_int, [H, C.POINTER(C.c_size_t)]),
+        "apollo_dg_batch_create": (C.c_int, [C.POINTER(_Config), C.c_char_p, _dp, C.c_int, C.POINTER(H)]),
+        "apollo_dg_batch_add_bc": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
+        "apollo_dg_batch_add_mesh": (C.c_int, [H, C.c_int, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip]),
+        "apollo_dg_batch_finalize": (C.c_int, [H]),
+        "apollo_dg_batch_size": (C.c_int, [H]),
+        "apollo_dg_batch_instance_info": (C.c_int, [H, C.c_int, _ip, _ip, _ip, _ip]),
+        "apollo_dg_batch_node_coords": (C.c_int, [H, C.c_int, _dp, _dp]),
+        "apollo_dg_batch_set_state": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
+        "apollo_dg_batch_get_state": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
+        "apollo_dg_batch_init_dt": (C.c_int, [H, _dp]),
+        "apollo_dg_batch_step": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int]),
+        "apollo_dg_batch_autotune": (C.c_int, [H, C.c_int, _ip]),
+        "apollo_dg_batch_last_error": (C.c_char_p, [H]),
+        "apollo_dg_batch_destroy": (C.c_int, [H]),
         "apollo_dg_last_error": (C.c_char_p, [H]),
         "apollo_dg_destroy": (C.c_int, [H]),
     }
@@ -276,3 +290,100 @@ class NodalDG2d:
         b = C.c_size_t()
         self._check(self.lib.apollo_dg_adjoint_memory(self.h, C.byref(b)))
         return b.value
+
+
+class NodalDG2dBatch:
+    """Independent meshes of one equation (any sizes, orders 2..5) stepped
+    together: each order's instances share one discretisation and every stage
+    is one persistent launch; one CUDA graph per step (apollo_dg_batch_*)."""
+
+    def __init__(self, cfl: float, equation: str, eq_params, bcs=(), device: int = 0):
+        self.lib = load_library()
+        cfg = _Config(0, cfl, device, None)
+        h = C.c_void_p()
+        p = np.asarray(list(eq_params), dtype=np.float64)
+        self._check(self.lib.apollo_dg_batch_create(C.byref(cfg), equation.encode(), p.ctypes.data_as(_dp), len(p),
+                                                    C.byref(h)), h=None)
+        self.h = h
+        for kind, params in bcs:
+            bp = np.asarray(list(params), dtype=np.float64)
+            self._check(self.lib.apollo_dg_batch_add_bc(h, kind.encode(), bp.ctypes.data_as(_dp), len(bp)))
+        self.info = []
+
+    def _check(self, code, h=0):
+        if code != 0:
+            hh = self.h if h == 0 else h
+            msg = self.lib.apollo_dg_batch_last_error(hh).decode() if hh else ""
+            raise ApolloError(code, msg)
+
+    def add_mesh(self, N: int, mesh: Mesh) -> int:
+        inst = C.c_int()
+        canon = mesh.vert_canon.ctypes.data_as(_ip) if mesh.vert_canon is not None else None
+        tag = mesh.face_tag.ctypes.data_as(_ip) if mesh.face_tag is not None else None
+        self._check(self.lib.apollo_dg_batch_add_mesh(self.h, N, mesh.nverts, mesh.vx.ctypes.data_as(_dp),
+                                                      mesh.vy.ctypes.data_as(_dp), mesh.K, mesh.etov.ctypes.data_as(_ip),
+                                                      tag, canon, C.byref(inst)))
+        return inst.value
+
+    def finalize(self):
+        self._check(self.lib.apollo_dg_batch_finalize(self.h))
+        self.info = []
+        for i in range(self.lib.apollo_dg_batch_size(self.h)):
+            N, K, Np, m = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+            self._check(self.lib.apollo_dg_batch_instance_info(self.h, i, C.byref(N), C.byref(K), C.byref(Np),
+                                                               C.byref(m)))
+            self.info.append({"N": N.value, "K": K.value, "Np": Np.value, "m": m.value})
+
+    def __len__(self):
+        return len(self.info)
+
+    def shape(self, i):
+        d = self.info[i]
+        return (d["K"], d["Np"], d["m"])
+
+    def node_coords(self, i):
+        K, Np, _ = self.shape(i)
+        x, y = np.empty((K, Np)), np.empty((K, Np))
+        self._check(self.lib.apollo_dg_batch_node_coords(self.h, i, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp)))
+        return x, y
+
+    def set_state(self, i, U):
+        p, where = _ptr(U)
+        self._check(self.lib.apollo_dg_batch_set_state(self.h, i, p, where))
+
+    def get_state(self, i, out=None):
+        if out is None:
+            out = np.empty(self.shape(i))
+        p, where = _ptr(out)
+        self._check(self.lib.apollo_dg_batch_get_state(self.h, i, p, where))
+        return out
+
+    def init_dt(self):
+        dt = np.zeros(len(self))
+        self._check(self.lib.apollo_dg_batch_init_dt(self.h, dt.ctypes.data_as(_dp)))
+        return dt
+
+    def step(self, nsteps: int, t, dt, precision: str = "fp64"):
+        """Advance every instance nsteps steps from its (t[i], dt[i]); returns the new (t, dt) arrays."""
+        t = np.ascontiguousarray(t, dtype=np.float64).copy()
+        dt = np.ascontiguousarray(dt, dtype=np.float64).copy()
+        self._check(self.lib.apollo_dg_batch_step(self.h, nsteps, t.ctypes.data_as(_dp), dt.ctypes.data_as(_dp),
+                                                  PREC[precision]))
+        return t, dt
+
+    def autotune(self, precision: str = "mixed"):
+        """Pick each order group's persistent-grid share by timing; returns {order: share}."""
+        ch = np.zeros(4, dtype=np.int32)
+        self._check(self.lib.apollo_dg_batch_autotune(self.h, PREC[precision], ch.ctypes.data_as(_ip)))
+        return {N: int(ch[N - 2]) for N in range(2, 6) if ch[N - 2]}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.apollo_dg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

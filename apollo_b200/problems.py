@@ -12,7 +12,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .mesh import Mesh, jittered_square
+from .mesh import Mesh, grid_for_elements, jittered_square
 
 
 @dataclass
@@ -99,3 +99,23 @@ def maxwell_tm(n: int = 512, N: int = 5, seed: int = 0, steps: int = 1000, field
     return Problem("maxwell_tm", N, cfl, kind, params, mesh, (("maxwellTransverseMagneticBC", ()),), steps,
                    ic=lambda x, y: tm_ic(x, y, fields),
                    exact=lambda x, y, t: tm_ic(x, y, fields, t=t))
+
+
+def euler_ensemble(count: int = 64, k_range=(1000, 64000), orders=(2, 3, 4, 5), beta_range=(1.0, 5.0),
+                   seed: int = 0, cfl: float = 0.5, fields: int = 4) -> list:
+    """Ensemble of independent isentropic vortices: per instance a seed-drawn
+    element count K uniform in k_range (a jittered periodic [0,10]^2 grid of
+    about that many elements), an order from ``orders`` and a vortex strength
+    uniform in beta_range.  Returns a list of Problems."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        K = int(rng.integers(k_range[0], k_range[1] + 1))
+        N = int(rng.choice(orders))
+        beta = float(rng.uniform(beta_range[0], beta_range[1]))
+        n = grid_for_elements(K)
+        p = euler_vortex(n=n, N=N, seed=seed * 1000 + i, fields=fields, beta=beta, cfl=cfl)
+        p.name = f"ensemble_{i}"
+        p.meta.update({"K_drawn": K})
+        out.append(p)
+    return out

@@ -201,6 +201,41 @@ apollo_status apollo_dg_rhs_vjp(apollo_dg* h, double t, const double* x, const d
 /* Device bytes held for derivatives (scratch, checkpoints, segment states). */
 apollo_status apollo_dg_adjoint_memory(const apollo_dg* h, size_t* bytes);
 
+/* ---- Batched ensembles.  No counterpart in Apollo (one mesh per run there).
+ * Many independent meshes of one equation, of any sizes and orders 2..5,
+ * advance together: the instances of one order share one discretisation
+ * (their elements concatenated, each with its own dt, time, dt policy and
+ * wave-speed reduction), each stage is one persistent launch over all of them,
+ * and one CUDA graph per step runs the order groups concurrently. */
+typedef struct apollo_dg_batch apollo_dg_batch;
+
+apollo_status apollo_dg_batch_create(const apollo_dg_config* cfg, const char* eq_kind, const double* eq_params,
+                                     int n_params, apollo_dg_batch** out);
+apollo_status apollo_dg_batch_add_bc(apollo_dg_batch* b, const char* kind, const double* params, int n_params);
+/* Adds one mesh (the arguments of apollo_dg_set_mesh) of order N; *instance
+ * receives its index. */
+apollo_status apollo_dg_batch_add_mesh(apollo_dg_batch* b, int N, int nverts, const double* vx, const double* vy,
+                                       int K, const int* etov, const int* face_tag, const int* vert_canon,
+                                       int* instance);
+/* Builds the discretisations; no meshes can be added afterwards. */
+apollo_status apollo_dg_batch_finalize(apollo_dg_batch* b);
+int apollo_dg_batch_size(const apollo_dg_batch* b);
+apollo_status apollo_dg_batch_instance_info(const apollo_dg_batch* b, int inst, int* N, int* K, int* Np, int* fields);
+apollo_status apollo_dg_batch_node_coords(const apollo_dg_batch* b, int inst, double* x, double* y);
+apollo_status apollo_dg_batch_set_state(apollo_dg_batch* b, int inst, const double* U, int where);
+apollo_status apollo_dg_batch_get_state(apollo_dg_batch* b, int inst, double* U, int where);
+/* Initial dt of every instance (Apollo's init policy), dt[instances]. */
+apollo_status apollo_dg_batch_init_dt(apollo_dg_batch* b, double* dt);
+/* nsteps steps of every instance from its own (t[i], dt[i]); both arrays are
+ * updated in place (dt policy of apollo_dg_step, no end time). */
+apollo_status apollo_dg_batch_step(apollo_dg_batch* b, int nsteps, double* t, double* dt, apollo_precision prec);
+/* Times the candidate launch shapes of each order group (persistent CTAs per
+ * SM share) for this precision and keeps the fastest; choice[4] receives the
+ * picked share per order 2..5 (0: order absent). */
+apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec, int* choice);
+const char* apollo_dg_batch_last_error(const apollo_dg_batch* b);
+apollo_status apollo_dg_batch_destroy(apollo_dg_batch* b);
+
 /* Error text of the last failing call on this handle. */
 const char* apollo_dg_last_error(const apollo_dg* h);
 
