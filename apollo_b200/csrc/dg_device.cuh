@@ -120,7 +120,13 @@ struct StageArgs {
   const float* tr_in;
   float* tr_out;
   float* tr_scratch;
+  // float64 launches of a partitioned mesh split around the trace exchange:
+  // PHASE_ALL, PHASE_VOLUME (volume term and traces) or PHASE_FACE (face
+  // fluxes and LIFT)
+  int phase;
 };
+
+enum { PHASE_ALL = 0, PHASE_VOLUME = 1, PHASE_FACE = 2 };
 
 template <int N> struct Sizes {
   static constexpr int NP = (N + 1) * (N + 2) / 2;
@@ -139,6 +145,10 @@ cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStrea
 cudaError_t launch_finalize(const DgDev& d, cudaStream_t s);
 // st[i].lam_bits = 0 for every instance
 cudaError_t launch_reset_lambda(const DgDev& d, cudaStream_t s);
+// Halo trace blocks (dg_halo.cu): gather (dst[j] = src[idx[j]]) or scatter
+// (dst[idx[j]] = src[j]) of n blocks of block_bytes (a multiple of 16) each
+cudaError_t launch_halo_blocks(const void* src, void* dst, const int* idx, int n, int block_bytes, bool scatter,
+                               cudaStream_t s);
 cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wJ, cudaStream_t s);
 int fp64_supported(int eq, int N);
 

@@ -343,9 +343,12 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
   if (per_sm > 8) per_sm = 8;
   int gv = sms * per_sm;
   if (gv > vt) gv = vt;
-  if (ev) cudaEventRecord(ev[0], s);
-  k_volume<EQ, N><<<gv, kThreads, VT::BYTES, s>>>(d, a);
-  if (ev) cudaEventRecord(ev[1], s);
+  if (a.phase != PHASE_FACE) {
+    if (ev) cudaEventRecord(ev[0], s);
+    k_volume<EQ, N><<<gv, kThreads, VT::BYTES, s>>>(d, a);
+    if (ev) cudaEventRecord(ev[1], s);
+  }
+  if (a.phase == PHASE_VOLUME) return cudaGetLastError();
   const int fthreads = d.nfaces * Sizes<N>::NG;
   int gf = (fthreads + kThreads - 1) / kThreads;
   if (gf > sms * 8) gf = sms * 8;

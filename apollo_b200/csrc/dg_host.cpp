@@ -16,6 +16,7 @@
 #include "dg_adjoint.h"
 #include "dg_mixed.h"
 #include "dg_operators.h"
+#include "dg_partition.h"
 
 using namespace apollo;
 
@@ -66,6 +67,17 @@ struct apollo_dg {
   bool have_state = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   MixedPlan* mixed = nullptr;
+  // partitioned mesh (apollo_dg_set_mesh_partition): KG ghost slots after the
+  // K local elements in the geometry and trace/flux buffers; per stage the
+  // blocks of halo_src (local face blocks k*3+f) are packed into hsend and the
+  // blocks of hrecv unpacked to halo_dst (ghost face blocks)
+  bool partitioned = false;
+  int KG = 0;
+  std::vector<int> peers, send_count, recv_count;
+  int n_send = 0, n_recv = 0;
+  int *halo_src_d = nullptr, *halo_dst_d = nullptr;
+  void *hsend = nullptr, *hrecv = nullptr, *hlam = nullptr;
+  size_t hsend_bytes = 0, hrecv_bytes = 0;
 };
 
 namespace {
@@ -123,6 +135,13 @@ void free_mesh(apollo_dg* h) {
   if (h->mixed) { mixed_destroy(h->mixed); h->mixed = nullptr; }
   h->have_state = false;
   h->ninst = 1;
+  dfree(h->halo_src_d); dfree(h->halo_dst_d);
+  h->partitioned = false;
+  h->KG = 0;
+  h->peers.clear(); h->send_count.clear(); h->recv_count.clear();
+  h->n_send = h->n_recv = 0;
+  h->hsend = h->hrecv = h->hlam = nullptr;
+  h->hsend_bytes = h->hrecv_bytes = 0;
 }
 
 template <class T>
@@ -160,6 +179,15 @@ apollo_status check_ready(apollo_dg* h) {
   return APOLLO_OK;
 }
 
+// calls that need the whole mesh on this handle (no trace exchange)
+apollo_status check_whole(apollo_dg* h) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!h->peers.empty())
+    return fail(h, APOLLO_ERR_STATE, "partitioned mesh with peers: use the staged calls (apollo_dg_stage_begin/end)");
+  return APOLLO_OK;
+}
+
 apollo_status read_errors(apollo_dg* h) {
   if (h->st_h->err & ERRB_NONPHYS) return fail(h, APOLLO_ERR_NONPHYSICAL, "negative density or pressure in the Euler flux");
   if (h->st_h->err & ERRB_NAN) return fail(h, APOLLO_ERR_NAN, "NaN in the right-hand side");
@@ -183,30 +211,36 @@ apollo_status enqueue_stage(apollo_dg* h, const StageArgs& a, apollo_precision p
   return APOLLO_OK;
 }
 
-apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
+// Stage i of SSPRK(5,2).  Stages update W in place: the float64 kernels read
+// neighbour data only in the volume/face kernels, before the LIFT kernel
+// writes, and the mixed kernel reads only its own elements' state plus the
+// face traces of the previous stage, which alternate between T0 and T1 (TU
+// holds those of U).
+StageArgs stage_args(const apollo_dg* h, int i) {
   const int s = 5;
-  // Stages update W in place: the float64 kernels read neighbour data only in
-  // the volume/face kernels, before the LIFT kernel writes, and the mixed
-  // kernel reads only its own elements' state plus the face traces of the
-  // previous stage, which alternate between T0 and T1 (TU holds those of U).
-  for (int i = 0; i < s; ++i) {
-    StageArgs a{};
-    a.time_from_state = 1;
-    a.reset_lambda = 1;
-    if (i < s - 1) {
-      a.x = i == 0 ? h->U_d : h->W_d;
-      a.out = h->W_d;
-      a.mode = MODE_STAGE;
-      a.frac = i / (s - 1.);
-    } else {
-      a.x = h->W_d;
-      a.u0 = h->U_d;
-      a.out = h->U_d;
-      a.mode = MODE_FINAL;
-      a.frac = 1.0;
-    }
-    a.tr_in = i == 0 ? h->TU_d : (i & 1) ? h->T0_d : h->T1_d;
-    a.tr_out = i == s - 1 ? h->TU_d : (i & 1) ? h->T1_d : h->T0_d;
+  StageArgs a{};
+  a.time_from_state = 1;
+  a.reset_lambda = 1;
+  if (i < s - 1) {
+    a.x = i == 0 ? h->U_d : h->W_d;
+    a.out = h->W_d;
+    a.mode = MODE_STAGE;
+    a.frac = i / (s - 1.);
+  } else {
+    a.x = h->W_d;
+    a.u0 = h->U_d;
+    a.out = h->U_d;
+    a.mode = MODE_FINAL;
+    a.frac = 1.0;
+  }
+  a.tr_in = i == 0 ? h->TU_d : (i & 1) ? h->T0_d : h->T1_d;
+  a.tr_out = i == s - 1 ? h->TU_d : (i & 1) ? h->T1_d : h->T0_d;
+  return a;
+}
+
+apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
+  for (int i = 0; i < 5; ++i) {
+    const StageArgs a = stage_args(h, i);
     apollo_status r = enqueue_stage(h, a, prec);
     if (r != APOLLO_OK) return r;
   }
@@ -313,50 +347,85 @@ apollo_status apollo_dg_add_bc(apollo_dg* h, const char* kind, const double* par
   return APOLLO_OK;
 }
 
-apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, const double* vy, int K,
-                                 const int* etov, const int* face_tag, const int* vert_canon) {
-  if (!h || !vx || !vy || !etov || nverts < 3 || K < 1) return APOLLO_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// The handle's mesh: the whole mesh (part == nullptr) or the elements of one
+// rank plus ghost slots for their remote neighbours' traces.
+apollo_status set_mesh_impl(apollo_dg* h, int nverts, const double* vx, const double* vy, int Kg, const int* etov,
+                            const int* face_tag, const int* vert_canon, const int* part, int rank) {
+  if (!h || !vx || !vy || !etov || nverts < 3 || Kg < 1) return APOLLO_ERR_ARG;
   if (h->eq < 0) return fail(h, APOLLO_ERR_STATE, "set the equation before the mesh");
   CK(cudaSetDevice(h->cfg.device), "set device");
   free_mesh(h);
   const RefOps& o = h->ops;
   const int Np = o.Np, M = h->M;
   h->K = 0;
-  h->geo_h.assign(K, ElemGeo{});
-  h->xn.assign((size_t)K * Np, 0.0);
-  h->yn.assign((size_t)K * Np, 0.0);
+  for (size_t i = 0; i < (size_t)Kg * 3; ++i)
+    if (etov[i] < 0 || etov[i] >= nverts) return fail(h, APOLLO_ERR_MESH, "vertex index out of range");
+  // smallest inscribed radius over the whole mesh, Apollo
+  // CalculateNodeCoordinates2d (wxnodaldggeometry2d.cc:220-227)
   double dtscale = 1.0e6;
-  for (int k = 0; k < K; ++k) {
-    int v[3] = {etov[3 * k], etov[3 * k + 1], etov[3 * k + 2]};
-    for (int j = 0; j < 3; ++j)
-      if (v[j] < 0 || v[j] >= nverts) return fail(h, APOLLO_ERR_MESH, "vertex index out of range");
+  for (int k = 0; k < Kg; ++k) {
+    const int* v = etov + 3 * k;
     const double p1x = vx[v[0]], p1y = vy[v[0]], p2x = vx[v[1]], p2y = vy[v[1]], p3x = vx[v[2]], p3y = vy[v[2]];
-    for (int n = 0; n < Np; ++n) {
-      const double r = o.r[n], s = o.s[n];
-      h->xn[(size_t)k * Np + n] = 0.5 * (-p1x * (r + s) + p2x * (1. + r) + p3x * (1. + s));
-      h->yn[(size_t)k * Np + n] = 0.5 * (-p1y * (r + s) + p2y * (1. + r) + p3y * (1. + s));
-    }
-    // inscribed radius, Apollo CalculateNodeCoordinates2d (wxnodaldggeometry2d.cc:220-227)
     const double l1 = std::sqrt(std::pow(p1x - p2x, 2) + std::pow(p1y - p2y, 2));
     const double l2 = std::sqrt(std::pow(p2x - p3x, 2) + std::pow(p2y - p3y, 2));
     const double l3 = std::sqrt(std::pow(p3x - p1x, 2) + std::pow(p3y - p1y, 2));
     const double sp = 0.5 * (l1 + l2 + l3);
     const double area = std::sqrt(std::fabs(sp * (sp - l1) * (sp - l2) * (sp - l3)));
     dtscale = std::min(dtscale, area / sp);
+  }
+  h->dtscale = dtscale;
+  // face map: faces sharing both (canonical) vertices pair up
+  std::vector<int> partner;
+  std::string perr = pair_faces(nverts, Kg, etov, face_tag, vert_canon, partner);
+  if (!perr.empty()) return fail(h, APOLLO_ERR_MESH, perr);
+  HaloPlan plan;
+  if (part) {
+    for (int k = 0; k < Kg; ++k)
+      if (part[k] < 0) return fail(h, APOLLO_ERR_ARG, "negative part id");
+    perr = build_halo(Kg, partner, part, rank, plan);
+    if (!perr.empty()) return fail(h, APOLLO_ERR_ARG, perr);
+  } else {
+    plan.local.resize(Kg);
+    for (int k = 0; k < Kg; ++k) plan.local[k] = k;
+  }
+  const int K = (int)plan.local.size(), G = (int)plan.ghost.size();
+  // slot of every held element: local ones first, then the ghosts
+  std::vector<int> slot(Kg, -1);
+  for (int i = 0; i < K; ++i) slot[plan.local[i]] = i;
+  for (int g = 0; g < G; ++g) slot[plan.ghost[g]] = K + g;
+  h->geo_h.assign((size_t)K + G, ElemGeo{});
+  h->xn.assign((size_t)K * Np, 0.0);
+  h->yn.assign((size_t)K * Np, 0.0);
+  std::vector<double> xg(Np), yg(Np);
+  for (int i = 0; i < K + G; ++i) {
+    const int kg = i < K ? plan.local[i] : plan.ghost[i - K];
+    const int* v = etov + 3 * kg;
+    const double p1x = vx[v[0]], p1y = vy[v[0]], p2x = vx[v[1]], p2y = vy[v[1]], p3x = vx[v[2]], p3y = vy[v[2]];
+    double* xs = i < K ? &h->xn[(size_t)i * Np] : xg.data();
+    double* ys = i < K ? &h->yn[(size_t)i * Np] : yg.data();
+    for (int n = 0; n < Np; ++n) {
+      const double r = o.r[n], s = o.s[n];
+      xs[n] = 0.5 * (-p1x * (r + s) + p2x * (1. + r) + p3x * (1. + s));
+      ys[n] = 0.5 * (-p1y * (r + s) + p2y * (1. + r) + p3y * (1. + s));
+    }
     // GeometricFactors2d and Normals2d from the vertex nodes (:382-442)
-    const double x1 = h->xn[(size_t)k * Np + o.fmask[0]], y1 = h->yn[(size_t)k * Np + o.fmask[0]];
-    const double x2 = h->xn[(size_t)k * Np + o.fmask[o.N + 1]], y2 = h->yn[(size_t)k * Np + o.fmask[o.N + 1]];
-    const double x3 = h->xn[(size_t)k * Np + o.fmask[2 * (o.N + 1)]], y3 = h->yn[(size_t)k * Np + o.fmask[2 * (o.N + 1)]];
+    const double x1 = xs[o.fmask[0]], y1 = ys[o.fmask[0]];
+    const double x2 = xs[o.fmask[o.N + 1]], y2 = ys[o.fmask[o.N + 1]];
+    const double x3 = xs[o.fmask[2 * (o.N + 1)]], y3 = ys[o.fmask[2 * (o.N + 1)]];
     const double dxdr = (x2 - x1) / 2, dxds = (x3 - x1) / 2, dydr = (y2 - y1) / 2, dyds = (y3 - y1) / 2;
     const double J = -dxds * dydr + dxdr * dyds;
-    if (!(J > 0)) return fail(h, APOLLO_ERR_MESH, "non-positive Jacobian in element " + std::to_string(k));
-    ElemGeo& g = h->geo_h[k];
+    if (!(J > 0)) return fail(h, APOLLO_ERR_MESH, "non-positive Jacobian in element " + std::to_string(kg));
+    ElemGeo& g = h->geo_h[i];
     g.rx = dyds / J; g.sx = -dydr / J; g.ry = -dxds / J; g.sy = dxdr / J;
     g.J = J; g.invJ = 1.0 / J;
     double nr[3][2] = {{(y2 - y1), -(x2 - x1)}, {(y3 - y2), -(x3 - x2)}, {(y1 - y3), -(x1 - x3)}};
     for (int f = 0; f < 3; ++f) {
       const double sJ = std::sqrt(nr[f][0] * nr[f][0] + nr[f][1] * nr[f][1]);
-      if (!(sJ > 0)) return fail(h, APOLLO_ERR_MESH, "zero edge length in element " + std::to_string(k));
+      if (!(sJ > 0)) return fail(h, APOLLO_ERR_MESH, "zero edge length in element " + std::to_string(kg));
       g.nx[f] = nr[f][0] / sJ;
       g.ny[f] = nr[f][1] / sJ;
       g.sJ[f] = sJ / 2.;
@@ -364,54 +433,37 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
     g.vx[0] = p1x; g.vx[1] = p2x; g.vx[2] = p3x;
     g.vy[0] = p1y; g.vy[1] = p2y; g.vy[2] = p3y;
   }
-  h->dtscale = dtscale;
-  // face map: faces sharing both (canonical) vertices pair up
-  static const int vn[3][2] = {{0, 1}, {1, 2}, {2, 0}};
-  std::unordered_map<unsigned long long, int> open;
-  open.reserve((size_t)K * 2);
-  std::vector<int> partner((size_t)K * 3, -1);
-  for (int k = 0; k < K; ++k)
-    for (int f = 0; f < 3; ++f) {
-      const int tag = face_tag ? face_tag[3 * k + f] : 0;
-      if (tag < 0) return fail(h, APOLLO_ERR_MESH, "negative face tag");
-      if (tag > 0) continue;
-      int a = etov[3 * k + vn[f][0]], b = etov[3 * k + vn[f][1]];
-      if (vert_canon) { a = vert_canon[a]; b = vert_canon[b]; }
-      if (a == b) return fail(h, APOLLO_ERR_MESH, "degenerate face");
-      const unsigned long long key = ((unsigned long long)(unsigned)std::min(a, b) << 32) | (unsigned)std::max(a, b);
-      auto it = open.find(key);
-      if (it == open.end()) {
-        open.emplace(key, 3 * k + f);
-      } else {
-        const int kf = it->second;
-        if (kf < 0) return fail(h, APOLLO_ERR_MESH, "face shared by more than two elements");
-        partner[3 * k + f] = kf;
-        partner[kf] = 3 * k + f;
-        it->second = -1;
-      }
-    }
+  // face list and connectivity of the local elements.  An interior face is
+  // listed once, from the side that comes first in the global mesh (the one
+  // whose global face id 3k+f is lower), so a cut face is computed by both
+  // ranks exactly as one handle on the whole mesh computes it.
   h->faces_h.clear();
   h->faces_h.reserve((size_t)K * 2);
   h->conn_h.assign((size_t)K * 6, -1);
-  for (int k = 0; k < K; ++k)
+  for (int i = 0; i < K; ++i) {
+    const int kg = plan.local[i];
     for (int f = 0; f < 3; ++f) {
-      const int tag = face_tag ? face_tag[3 * k + f] : 0;
-      const int p = partner[3 * k + f];
+      const int tag = face_tag ? face_tag[3 * kg + f] : 0;
+      const int p = partner[3 * kg + f];
       if (tag > 0 || p < 0) {
         const int t = tag > 0 ? tag : 1;
         if (t > std::max(1, h->bcs.n)) return fail(h, APOLLO_ERR_MESH, "face tag without a boundary condition");
         if (h->bcs.n == 0) return fail(h, APOLLO_ERR_MESH, "boundary face but no boundary condition added");
-        h->faces_h.push_back(FaceRec{k, f, -t, -1});
-        h->conn_h[6 * k + 2 * f] = -t;
-        h->conn_h[6 * k + 2 * f + 1] = -1;
+        h->faces_h.push_back(FaceRec{i, f, -t, -1});
+        h->conn_h[6 * i + 2 * f] = -t;
+        h->conn_h[6 * i + 2 * f + 1] = -1;
       } else {
-        if (p > 3 * k + f) h->faces_h.push_back(FaceRec{k, f, p / 3, p % 3});
-        h->conn_h[6 * k + 2 * f] = p / 3;
-        h->conn_h[6 * k + 2 * f + 1] = p % 3;
+        const int sp = slot[p / 3];
+        if (p > 3 * kg + f) h->faces_h.push_back(FaceRec{i, f, sp, p % 3});
+        else if (sp >= K) h->faces_h.push_back(FaceRec{sp, p % 3, i, f});
+        h->conn_h[6 * i + 2 * f] = sp;
+        h->conn_h[6 * i + 2 * f + 1] = p % 3;
       }
     }
-  // device buffers
-  const size_t nU = (size_t)K * Np * M, nT = (size_t)K * o.Nf * M;
+  }
+  // device buffers: state-sized ones for the local elements, geometry and
+  // trace/flux scratch with the ghost slots
+  const size_t nU = (size_t)K * Np * M, nT = (size_t)(K + G) * o.Nf * M;
   CK(upload(&h->geo_d, h->geo_h.data(), h->geo_h.size()), "geometry upload");
   CK(upload(&h->faces_d, h->faces_h.data(), h->faces_h.size()), "face map upload");
   CK(upload(&h->conn_d, h->conn_h.data(), h->conn_h.size()), "connectivity upload");
@@ -432,15 +484,50 @@ apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, con
   CK(cudaMalloc((void**)&h->trace_d, nT * sizeof(double)), "scratch alloc");
   CK(cudaMalloc((void**)&h->flux_d, nT * sizeof(double)), "scratch alloc");
   CK(cudaMemset(h->U_d, 0, nU * sizeof(double)), "state clear");
+  CK(cudaMemset(h->trace_d, 0, nT * sizeof(double)), "scratch clear");
   h->K = K;
   h->mixed = mixed_create(h->eq, o, K, h->M);
   if (h->mixed) {
-    const size_t nTr = mixed_trace_floats(h->mixed, K);
+    const size_t nTr = mixed_trace_floats(h->mixed, K + G);
     CK(cudaMalloc((void**)&h->TU_d, nTr * sizeof(float)), "trace alloc");
     CK(cudaMalloc((void**)&h->T0_d, nTr * sizeof(float)), "trace alloc");
     CK(cudaMalloc((void**)&h->T1_d, nTr * sizeof(float)), "trace alloc");
+    CK(cudaMemset(h->TU_d, 0, nTr * sizeof(float)), "trace clear");
+    CK(cudaMemset(h->T0_d, 0, nTr * sizeof(float)), "trace clear");
+    CK(cudaMemset(h->T1_d, 0, nTr * sizeof(float)), "trace clear");
+  }
+  // halo: face-block indices of the blocks sent (local) and received (ghost)
+  h->partitioned = part != nullptr;
+  h->KG = G;
+  h->peers = plan.peers;
+  h->send_count = plan.send_count;
+  h->recv_count = plan.recv_count;
+  h->n_send = (int)plan.send_face.size();
+  h->n_recv = (int)plan.recv_face.size();
+  if (h->n_send) {
+    std::vector<int> src(h->n_send), dst(h->n_recv);
+    for (int j = 0; j < h->n_send; ++j) src[j] = slot[plan.send_face[j] / 3] * 3 + plan.send_face[j] % 3;
+    for (int j = 0; j < h->n_recv; ++j) dst[j] = slot[plan.recv_face[j] / 3] * 3 + plan.recv_face[j] % 3;
+    CK(upload(&h->halo_src_d, src.data(), src.size()), "halo upload");
+    CK(upload(&h->halo_dst_d, dst.data(), dst.size()), "halo upload");
   }
   return APOLLO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+apollo_status apollo_dg_set_mesh(apollo_dg* h, int nverts, const double* vx, const double* vy, int K,
+                                 const int* etov, const int* face_tag, const int* vert_canon) {
+  return set_mesh_impl(h, nverts, vx, vy, K, etov, face_tag, vert_canon, nullptr, 0);
+}
+
+apollo_status apollo_dg_set_mesh_partition(apollo_dg* h, int nverts, const double* vx, const double* vy, int K,
+                                           const int* etov, const int* face_tag, const int* vert_canon,
+                                           const int* part, int rank) {
+  if (!part || rank < 0) return APOLLO_ERR_ARG;
+  return set_mesh_impl(h, nverts, vx, vy, K, etov, face_tag, vert_canon, part, rank);
 }
 
 int apollo_dg_num_fields(const apollo_dg* h) { return h ? h->M : 0; }
@@ -500,7 +587,7 @@ apollo_status apollo_dg_init_dt(apollo_dg* h, double* dt) {
 
 apollo_status apollo_dg_rhs(apollo_dg* h, double t, double dt, const double* in, double* out, double* suggested_dt,
                             int where, apollo_precision prec) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (!in || !out) return APOLLO_ERR_ARG;
   if (prec == APOLLO_PREC_MIXED && where == APOLLO_DEVICE_PTR && (const double*)out == in)
@@ -536,7 +623,7 @@ apollo_status apollo_dg_rhs(apollo_dg* h, double t, double dt, const double* in,
 }
 
 apollo_status apollo_dg_step_async(apollo_dg* h, int nsteps, double t, double dt, apollo_precision prec) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (nsteps < 0) return APOLLO_ERR_ARG;
   if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
@@ -570,7 +657,7 @@ apollo_status apollo_dg_get_time(apollo_dg* h, double* t, double* dt) {
 }
 
 apollo_status apollo_dg_step(apollo_dg* h, int nsteps, double* t, double* dt, double tend, apollo_precision prec) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (!t || !dt || nsteps < 0) return APOLLO_ERR_ARG;
   if (tend <= 0.0) {
@@ -625,7 +712,7 @@ apollo_status apollo_dg_integrals(apollo_dg* h, const double* U, int where, doub
 }
 
 apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int iters, double* ms, int* nk) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (!ms || !nk || iters < 1) return APOLLO_ERR_ARG;
   cudaEvent_t ev[4];
@@ -774,7 +861,7 @@ namespace apollo {
 // Read-only view of a handle's discretisation for the no-allocation entry
 // point (dg_noalloc.cu); the scratch pointers are left for the caller to set.
 bool handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size_t* nU, size_t* nT) {
-  if (!h || h->eq < 0 || h->K == 0) return false;
+  if (!h || h->eq < 0 || h->K == 0 || !h->peers.empty()) return false;
   *d = make_dev(h);
   *eq = h->eq;
   *device = h->cfg.device;
@@ -882,7 +969,7 @@ extern "C" {
 const char* apollo_dg_last_error(const apollo_dg* h) { return h ? h->err.c_str() : "null handle"; }
 
 apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, double dt, int checkpoint_every) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (nsteps < 1 || checkpoint_every < 1 || !(dt > 0.0)) return fail(h, APOLLO_ERR_ARG, "nsteps, checkpoint_every >= 1, dt > 0");
   if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
@@ -917,7 +1004,7 @@ apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, doubl
 }
 
 apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* ubar_0, int where) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (!ubar_T || !ubar_0) return APOLLO_ERR_ARG;
   if (!h->tr_valid) return fail(h, APOLLO_ERR_STATE, "no trajectory: call apollo_dg_forward_fixed first");
@@ -969,7 +1056,7 @@ apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* uba
 
 apollo_status apollo_dg_tangent(apollo_dg* h, int nsteps, double t0, double dt, const double* du0, double* duT,
                                 int where) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (nsteps < 0 || !(dt > 0.0) || !du0 || !duT) return APOLLO_ERR_ARG;
   if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
@@ -998,7 +1085,7 @@ apollo_status apollo_dg_tangent(apollo_dg* h, int nsteps, double t0, double dt, 
 }
 
 apollo_status apollo_dg_rhs_jvp(apollo_dg* h, double t, const double* x, const double* v, double* out, int where) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (!x || !v || !out) return APOLLO_ERR_ARG;
   r = ensure_deriv_buffers(h);
@@ -1025,7 +1112,7 @@ apollo_status apollo_dg_rhs_jvp(apollo_dg* h, double t, const double* x, const d
 }
 
 apollo_status apollo_dg_rhs_vjp(apollo_dg* h, double t, const double* x, const double* w, double* out, int where) {
-  apollo_status r = check_ready(h);
+  apollo_status r = check_whole(h);
   if (r) return r;
   if (!x || !w || !out) return APOLLO_ERR_ARG;
   if (where == APOLLO_DEVICE_PTR && (out == x || out == w))
@@ -1073,6 +1160,118 @@ apollo_status apollo_dg_destroy(apollo_dg* h) {
   if (h->st_h) cudaFreeHost(h->st_h);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
+  return APOLLO_OK;
+}
+
+
+// ---- partitioned meshes: halo info, buffers and staged stepping
+
+apollo_status apollo_dg_halo_info(const apollo_dg* h, apollo_precision prec, int* n_peers, int* peers,
+                                  int* send_count, int* recv_count, int* block_bytes) {
+  if (!h || h->K == 0) return APOLLO_ERR_ARG;
+  if (n_peers) *n_peers = (int)h->peers.size();
+  for (size_t i = 0; i < h->peers.size(); ++i) {
+    if (peers) peers[i] = h->peers[i];
+    if (send_count) send_count[i] = h->send_count[i];
+    if (recv_count) recv_count[i] = h->recv_count[i];
+  }
+  if (block_bytes) {
+    if (prec == APOLLO_PREC_MIXED) {
+      if (!h->mixed) return APOLLO_ERR_CONFIG;
+      *block_bytes = (int)(mixed_trace_floats(h->mixed, 1) / 3 * sizeof(float));
+    } else {
+      *block_bytes = h->ops.Ng * h->M * (int)sizeof(double);
+    }
+  }
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_halo_bind(apollo_dg* h, void* send, size_t send_bytes, void* recv, size_t recv_bytes,
+                                  void* lam) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  const size_t blk = (size_t)h->ops.Ng * h->M * sizeof(double);  // the larger (float64) block
+  if ((h->n_send && (!send || send_bytes < blk * h->n_send)) || (h->n_recv && (!recv || recv_bytes < blk * h->n_recv)))
+    return fail(h, APOLLO_ERR_ARG, "halo buffers too small");
+  if (((uintptr_t)send | (uintptr_t)recv | (uintptr_t)lam) % 16)
+    return fail(h, APOLLO_ERR_ARG, "halo buffers must be 16-byte aligned");
+  h->hsend = send;
+  h->hsend_bytes = send_bytes;
+  h->hrecv = recv;
+  h->hrecv_bytes = recv_bytes;
+  h->hlam = lam;
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_dist_start(apollo_dg* h, double t, double dt, apollo_precision prec) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  if (prec == APOLLO_PREC_MIXED && !h->mixed)
+    return fail(h, APOLLO_ERR_CONFIG, "mixed precision is not available for this equation/order");
+  if (!h->peers.empty() && (!h->hsend || !h->hrecv || !h->hlam))
+    return fail(h, APOLLO_ERR_STATE, "bind the halo buffers first (apollo_dg_halo_bind)");
+  DevState s{};
+  s.t = t;
+  s.dt = dt;
+  s.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
+  std::memcpy(h->st_h, &s, sizeof(DevState));
+  CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
+  return handle_prepare_step(h, prec);
+}
+
+apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision prec) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
+  if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");
+  StageArgs a = stage_args(h, stage);
+  DgDev d = make_dev(h);
+  if (prec == APOLLO_PREC_MIXED) {
+    // the stage input's traces were written by the previous stage (or the
+    // trace kernel for U)
+    const int blk = (int)(mixed_trace_floats(h->mixed, 1) / 3 * sizeof(float));
+    CK(launch_halo_blocks(a.tr_in, h->hsend, h->halo_src_d, h->n_send, blk, false, h->stream), "halo pack");
+  } else {
+    a.phase = PHASE_VOLUME;
+    CK(launch_rhs_fp64(h->eq, d, a, h->stream), "volume launch");
+    const int blk = h->ops.Ng * h->M * (int)sizeof(double);
+    CK(launch_halo_blocks(h->trace_d, h->hsend, h->halo_src_d, h->n_send, blk, false, h->stream), "halo pack");
+  }
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_stage_end(apollo_dg* h, int stage, apollo_precision prec) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
+  if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");
+  StageArgs a = stage_args(h, stage);
+  DgDev d = make_dev(h);
+  if (prec == APOLLO_PREC_MIXED) {
+    const int blk = (int)(mixed_trace_floats(h->mixed, 1) / 3 * sizeof(float));
+    CK(launch_halo_blocks(h->hrecv, (void*)a.tr_in, h->halo_dst_d, h->n_recv, blk, true, h->stream), "halo unpack");
+    CK(mixed_launch_rhs(h->mixed, h->eq, d, a, h->stream, nullptr), "stage launch");
+  } else {
+    const int blk = h->ops.Ng * h->M * (int)sizeof(double);
+    CK(launch_halo_blocks(h->hrecv, h->trace_d, h->halo_dst_d, h->n_recv, blk, true, h->stream), "halo unpack");
+    a.phase = PHASE_FACE;
+    CK(launch_rhs_fp64(h->eq, d, a, h->stream), "face launch");
+  }
+  if (stage == 4 && h->hlam)
+    CK(cudaMemcpyAsync(h->hlam, &h->st_d->lam_bits, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, h->stream),
+       "wave speed out");
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_step_end(apollo_dg* h) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (h->hlam)
+    CK(cudaMemcpyAsync(&h->st_d->lam_bits, h->hlam, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, h->stream),
+       "wave speed in");
+  DgDev d = make_dev(h);
+  CK(launch_finalize(d, h->stream), "finalize launch");
   return APOLLO_OK;
 }
 

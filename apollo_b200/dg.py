@@ -43,6 +43,11 @@ class _Config(C.Structure):
     _fields_ = [("polynomial_order", C.c_int), ("cfl", C.c_double), ("device", C.c_int), ("stream", C.c_void_p)]
 
 
+class HaloSizes(C.Structure):
+    _fields_ = [("n_local", C.c_int), ("n_ghost", C.c_int), ("n_peers", C.c_int), ("n_send", C.c_int),
+                ("n_recv", C.c_int)]
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _lib = None
@@ -99,6 +104,16 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_batch_autotune": (C.c_int, [H, C.c_int, _ip]),
         "apollo_dg_batch_last_error": (C.c_char_p, [H]),
         "apollo_dg_batch_destroy": (C.c_int, [H]),
+        "apollo_dg_partition": (C.c_int, [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, _ip]),
+        "apollo_dg_halo_plan": (C.c_int, [C.c_int, C.c_int, _ip, _ip, _ip, _ip, C.c_int, C.POINTER(HaloSizes),
+                                          _ip, _ip, _ip, _ip, _ip, _ip, _ip]),
+        "apollo_dg_set_mesh_partition": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip, C.c_int]),
+        "apollo_dg_halo_info": (C.c_int, [H, C.c_int, _ip, _ip, _ip, _ip, _ip]),
+        "apollo_dg_halo_bind": (C.c_int, [H, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p]),
+        "apollo_dg_dist_start": (C.c_int, [H, C.c_double, C.c_double, C.c_int]),
+        "apollo_dg_stage_begin": (C.c_int, [H, C.c_int, C.c_int]),
+        "apollo_dg_stage_end": (C.c_int, [H, C.c_int, C.c_int]),
+        "apollo_dg_step_end": (C.c_int, [H]),
         "apollo_dg_last_error": (C.c_char_p, [H]),
         "apollo_dg_destroy": (C.c_int, [H]),
     }
@@ -131,7 +146,10 @@ class NodalDG2d:
     """One nodal-DG discretisation on the GPU (Apollo ``Kind = nodalDG2d``)."""
 
     def __init__(self, N: int, cfl: float, equation: str, eq_params, mesh: Mesh, bcs=(), device: int = 0,
-                 stream: int | None = None):
+                 stream: int | None = None, part=None, rank: int = 0):
+        """``part`` (int32 [K], optional): a partition of ``mesh``; the handle then
+        holds the elements with ``part == rank`` (apollo_dg_set_mesh_partition)
+        and steps through ``apollo_b200.distributed.DistNodalDG2d``."""
         self.lib = load_library()
         cfg = _Config(N, cfl, device, C.c_void_p(stream) if stream else None)
         h = C.c_void_p()
@@ -143,9 +161,19 @@ class NodalDG2d:
             bp = np.asarray(list(params), dtype=np.float64)
             self._check(self.lib.apollo_dg_add_bc(h, kind.encode(), bp.ctypes.data_as(_dp), len(bp)))
         self.mesh = mesh
-        self._check(self.lib.apollo_dg_set_mesh(
-            h, mesh.nverts, mesh.vx.ctypes.data_as(_dp), mesh.vy.ctypes.data_as(_dp), mesh.K,
-            mesh.etov.ctypes.data_as(_ip), mesh.face_tag.ctypes.data_as(_ip), mesh.vert_canon.ctypes.data_as(_ip)))
+        if part is None:
+            self._check(self.lib.apollo_dg_set_mesh(
+                h, mesh.nverts, mesh.vx.ctypes.data_as(_dp), mesh.vy.ctypes.data_as(_dp), mesh.K,
+                mesh.etov.ctypes.data_as(_ip), mesh.face_tag.ctypes.data_as(_ip), mesh.vert_canon.ctypes.data_as(_ip)))
+        else:
+            self.part = np.ascontiguousarray(part, dtype=np.int32)
+            assert self.part.shape == (mesh.K,)
+            self._check(self.lib.apollo_dg_set_mesh_partition(
+                h, mesh.nverts, mesh.vx.ctypes.data_as(_dp), mesh.vy.ctypes.data_as(_dp), mesh.K,
+                mesh.etov.ctypes.data_as(_ip), mesh.face_tag.ctypes.data_as(_ip), mesh.vert_canon.ctypes.data_as(_ip),
+                self.part.ctypes.data_as(_ip), rank))
+        self.rank = rank
+        self.stream = stream
         self.N = N
         self.equation = equation
         self.K = self.lib.apollo_dg_num_elements(h)

@@ -236,6 +236,79 @@ apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec
 const char* apollo_dg_batch_last_error(const apollo_dg_batch* b);
 apollo_status apollo_dg_batch_destroy(apollo_dg_batch* b);
 
+/* ---- Partitioned meshes (one handle per rank, one rank per GPU).  Replaces
+ * Apollo's PETSc DMPlex distribution with an overlap-1 halo refreshed by
+ * DMGlobalToLocal before every right-hand side (src/solvers/apsolver.cc:318-392)
+ * and its MPI_Allreduce of the dt estimate (apsolver.cc:431-433): here only the
+ * face traces of cut faces cross between ranks, once per stage, and the
+ * caller's communicator (NCCL, MPI, ...) moves them.
+ *
+ * Host-only calls (no device needed): */
+/* Recursive coordinate bisection of the element centroids: part[K] receives
+ * a rank in 0..nparts-1 per element, parts within one element of K/nparts. */
+apollo_status apollo_dg_partition(int nverts, const double* vx, const double* vy, int K, const int* etov,
+                                  int nparts, int* part);
+
+typedef struct {
+  int n_local;  /* elements owned by the rank */
+  int n_ghost;  /* remote elements sharing a face with a local one */
+  int n_peers;  /* ranks exchanged with */
+  int n_send;   /* trace blocks sent per stage (one per cut face) */
+  int n_recv;   /* trace blocks received per stage */
+} apollo_dg_halo_sizes;
+
+/* The halo plan of one rank of the global mesh (apollo_dg_set_mesh's mesh
+ * arguments) under the partition part[K].  Fills *sizes; each array that is
+ * not NULL receives: local_elems[n_local] and ghost_elems[n_ghost] (global
+ * element ids), peers[n_peers] (ascending), send_count / recv_count[n_peers]
+ * (blocks per peer), send_faces[n_send] (global face id 3k+f of the local side
+ * of each block sent, peer-major) and recv_faces[n_recv] (global face id of the
+ * remote side of each block received).  Within one peer, blocks go in
+ * ascending order of the sending side's face id, on both ranks. */
+apollo_status apollo_dg_halo_plan(int nverts, int K, const int* etov, const int* face_tag, const int* vert_canon,
+                                  const int* part, int rank, apollo_dg_halo_sizes* sizes, int* local_elems,
+                                  int* ghost_elems, int* peers, int* send_count, int* recv_count, int* send_faces,
+                                  int* recv_faces);
+
+/* Device calls: */
+/* Like apollo_dg_set_mesh with the GLOBAL mesh, keeping the elements with
+ * part[k] == rank (in global order; node coordinates, states and
+ * apollo_dg_num_elements refer to them) plus ghost slots for the traces of
+ * their remote neighbours.  Every face keeps the orientation it has in the
+ * global mesh and dt uses the global inscribed radius, so the ranks together
+ * compute bit for bit what one handle on the whole mesh computes.  With
+ * peers, apollo_dg_rhs, apollo_dg_step(_async) and the derivative calls are
+ * refused (APOLLO_ERR_STATE): step with the staged calls below. */
+apollo_status apollo_dg_set_mesh_partition(apollo_dg* h, int nverts, const double* vx, const double* vy, int K,
+                                           const int* etov, const int* face_tag, const int* vert_canon,
+                                           const int* part, int rank);
+/* Peers (ascending), blocks per peer and the bytes of one trace block in this
+ * precision (float64 or float32 traces); any pointer may be NULL. */
+apollo_status apollo_dg_halo_info(const apollo_dg* h, apollo_precision prec, int* n_peers, int* peers,
+                                  int* send_count, int* recv_count, int* block_bytes);
+/* Caller-owned device buffers, 16-byte aligned: send and recv hold the blocks
+ * of all peers back to back in peer order (the largest block size of the two
+ * precisions times n_send / n_recv bytes), lam one 8-byte word that the caller
+ * reduces with MAX across ranks as a signed 64-bit integer (the bits of a
+ * non-negative double). */
+apollo_status apollo_dg_halo_bind(apollo_dg* h, void* send, size_t send_bytes, void* recv, size_t recv_bytes,
+                                  void* lam);
+/* Staged stepping, all on the handle's stream (nothing waits on the host):
+ *   apollo_dg_dist_start(t, dt)          once, before the first step
+ *   per step, for stage = 0..4:
+ *     apollo_dg_stage_begin(stage)       traces of the stage input, packed into send
+ *     <caller: send -> peers, peers -> recv>
+ *     apollo_dg_stage_end(stage)         recv unpacked into the ghost slots, the stage
+ *   <caller: MAX all-reduce of the lam word> (stage 4 wrote it)
+ *   apollo_dg_step_end()                 the dt policy of apollo_dg_step
+ * then apollo_dg_get_time as after apollo_dg_step_async.  The caller orders
+ * its transfers after the begin call's work and before the end call's on the
+ * handle's stream (or synchronises it). */
+apollo_status apollo_dg_dist_start(apollo_dg* h, double t, double dt, apollo_precision prec);
+apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision prec);
+apollo_status apollo_dg_stage_end(apollo_dg* h, int stage, apollo_precision prec);
+apollo_status apollo_dg_step_end(apollo_dg* h);
+
 /* Error text of the last failing call on this handle. */
 const char* apollo_dg_last_error(const apollo_dg* h);
 
