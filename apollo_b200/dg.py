@@ -104,6 +104,10 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_batch_autotune": (C.c_int, [H, C.c_int, _ip]),
         "apollo_dg_batch_last_error": (C.c_char_p, [H]),
         "apollo_dg_batch_destroy": (C.c_int, [H]),
+        "apollo_dg_mesh_read_gmsh": (C.c_int, [C.c_char_p, C.POINTER(H), C.c_char_p, C.c_int]),
+        "apollo_dg_mesh_info": (C.c_int, [H, _ip, _ip]),
+        "apollo_dg_mesh_arrays": (C.c_int, [H, _dp, _dp, _ip, _ip]),
+        "apollo_dg_mesh_destroy": (C.c_int, [H]),
         "apollo_dg_partition": (C.c_int, [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, _ip]),
         "apollo_dg_halo_plan": (C.c_int, [C.c_int, C.c_int, _ip, _ip, _ip, _ip, C.c_int, C.POINTER(HaloSizes),
                                           _ip, _ip, _ip, _ip, _ip, _ip, _ip]),

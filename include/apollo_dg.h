@@ -236,6 +236,23 @@ apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec
 const char* apollo_dg_batch_last_error(const apollo_dg_batch* b);
 apollo_status apollo_dg_batch_destroy(apollo_dg_batch* b);
 
+/* ---- Gmsh 2.2 ASCII meshes (host only).  Replaces PETSc's DMPlexCreateGmsh
+ * (src/solvers/apsolver.cc:318-327) and the "Face Sets" labels of
+ * wxNodalDGgeometry2D::FacePair2d (src/lib/wxnodaldggeometry2d.cc:334-356).
+ * Triangles become cells, oriented counter-clockwise; lines carry the physical
+ * tag (their first tag) of a boundary.  An element with a labelled face applies
+ * its label to all its unpaired faces, as Apollo does; unpaired faces of
+ * unlabelled elements get tag 1 (Apollo's default -1, boundary condition 1);
+ * where one element's faces carry different labels, each labelled face keeps
+ * its own.  The arrays are apollo_dg_set_mesh's (no periodic map). */
+typedef struct apollo_dg_mesh apollo_dg_mesh;
+/* err (optional, err_len bytes) receives the reason on failure. */
+apollo_status apollo_dg_mesh_read_gmsh(const char* path, apollo_dg_mesh** out, char* err, int err_len);
+apollo_status apollo_dg_mesh_info(const apollo_dg_mesh* m, int* nverts, int* K);
+/* vx, vy [nverts], etov [K][3], face_tag [K][3]; NULL arrays are skipped. */
+apollo_status apollo_dg_mesh_arrays(const apollo_dg_mesh* m, double* vx, double* vy, int* etov, int* face_tag);
+apollo_status apollo_dg_mesh_destroy(apollo_dg_mesh* m);
+
 /* ---- Partitioned meshes (one handle per rank, one rank per GPU).  Replaces
  * Apollo's PETSc DMPlex distribution with an overlap-1 halo refreshed by
  * DMGlobalToLocal before every right-hand side (src/solvers/apsolver.cc:318-392)

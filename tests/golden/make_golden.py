@@ -25,6 +25,18 @@ from oracle import oracle as orc  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
+VORTEX_BC = (1.0, 0.0, 5.0, 5.0, 1.4, 5.0)  # u0, v0, x0, y0, gas_gamma, beta
+
+
+def gmsh_vortex(N: int = 3):
+    """The Euler vortex on the unstructured Gmsh mesh square_delaunay.msh
+    (make_gmsh.py), the exact vortex imposed on both boundary tags, as Apollo's
+    isentropicVortex example does with isentropicVortexBC."""
+    from apollo_b200.gmsh import read_gmsh
+    mesh = read_gmsh(os.path.join(HERE, "square_delaunay.msh"))
+    return problems.Problem("gmsh_vortex", N, 0.5, "eulerEqn", (1.4, 0.0, 0.0), mesh, (), 0,
+                            ic=lambda x, y: problems.vortex_ic(x, y, 5, beta=5.0))
+
 CASES = [
     # name, builder, kwargs, oracle eq, eq params, ref kind, ref params, bcs, steps
     ("adv_N3", problems.advection, dict(n=8, N=3), orc.EQ_ADVECTION, (1.0, 0.5, 0.0), "advectionEqn",
@@ -39,6 +51,8 @@ CASES = [
      dict(c0=1.0), ((orc.BC_TM, ()),), 3),
     ("maxwell_N2", problems.maxwell_tm, dict(n=7, N=2, fields=8, seed=2), orc.EQ_MAXWELL, (1.0, 0.0, 0.0),
      "phMaxwellEqn", dict(c0=1.0), ((orc.BC_TM, ()),), 3),
+    ("gmsh_euler_N3", gmsh_vortex, dict(N=3), orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn", dict(gas_gamma=1.4),
+     ((orc.BC_VORTEX, VORTEX_BC), (orc.BC_VORTEX, VORTEX_BC)), 3),
 ]
 
 
@@ -59,17 +73,21 @@ def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref)
         os.path.join(HERE, f"{name}.npz"),
         vx=mesh.vx, vy=mesh.vy, etov=mesh.etov, face_tag=mesh.face_tag, vert_canon=mesh.vert_canon,
         N=prob.N, cfl=prob.cfl, eq=eq, eqp=np.asarray(eqp, dtype=np.float64), equation=ref_kind,
-        bc_kinds=np.asarray([b[0] for b in bcs], dtype=np.int32), x=x, y=y, U0=U0, rhs=rhs, sugg=sugg, dt0=dt0,
+        bc_kinds=np.asarray([b[0] for b in bcs], dtype=np.int32),
+        bc_params=np.asarray([list(b[1]) + [0.0] * (8 - len(b[1])) for b in bcs], dtype=np.float64).reshape(-1, 8),
+        x=x, y=y, U0=U0, rhs=rhs, sugg=sugg, dt0=dt0,
         steps=steps, U_end=U, t_end=t, dt_end=dt)
     return name, U0.shape, float(np.abs(rhs).max())
 
 
-def main():
+def main(names=()):
+    """All cases, or only those named on the command line."""
     orc.build(with_ref=True)
     ref = orc.RefPlugins()
     for case in CASES:
-        print(make_case(*case, ref=ref))
+        if not names or case[0] in names:
+            print(make_case(*case, ref=ref))
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

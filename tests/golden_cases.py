@@ -19,7 +19,8 @@ def load(name):
                 lo=(0, 0), hi=(1, 1), periodic=False)
     d["mesh"] = mesh
     d["equation"] = str(d["equation"])
-    d["bcs"] = tuple((BC_NAMES[int(k)], ()) for k in d["bc_kinds"])
+    par = d.get("bc_params", np.zeros((len(d["bc_kinds"]), 0)))
+    d["bcs"] = tuple((BC_NAMES[int(k)], tuple(par[i]) if par.shape[1] else ()) for i, k in enumerate(d["bc_kinds"]))
     return d
 
 

@@ -18,7 +18,7 @@ def test_oracle_port_reproduces_golden(oracle_lib, name):
     """The restated plugins reproduce fixtures made with the reference's plugin code."""
     orc = oracle_lib
     g = load(name)
-    bcs = tuple((int(k), ()) for k in g["bc_kinds"])
+    bcs = tuple((int(k), tuple(g["bc_params"][i]) if "bc_params" in g else ()) for i, k in enumerate(g["bc_kinds"]))
     o = orc.Oracle(g["mesh"], int(g["N"]), int(g["eq"]), g["eqp"], bcs=bcs, cfl=float(g["cfl"]))
     x, y = o.node_coords()
     np.testing.assert_array_equal(x, g["x"])
