@@ -51,7 +51,7 @@ CASES = [
      dict(c0=1.0), ((orc.BC_TM, ()),), 3),
     ("maxwell_N2", problems.maxwell_tm, dict(n=7, N=2, fields=8, seed=2), orc.EQ_MAXWELL, (1.0, 0.0, 0.0),
      "phMaxwellEqn", dict(c0=1.0), ((orc.BC_TM, ()),), 3),
-    ("gmsh_euler_N3", gmsh_vortex, dict(N=3), orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn", dict(gas_gamma=1.4),
+    ("euler_gmsh_N3", gmsh_vortex, dict(N=3), orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn", dict(gas_gamma=1.4),
      ((orc.BC_VORTEX, VORTEX_BC), (orc.BC_VORTEX, VORTEX_BC)), 3),
 ]
 

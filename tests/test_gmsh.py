@@ -112,7 +112,7 @@ def test_malformed_input_is_refused(tmp_path, body, why):
 
 
 def test_fixture_reads_as_the_golden_case():
-    g = load("gmsh_euler_N3")
+    g = load("euler_gmsh_N3")
     m = read_gmsh(os.path.join(HERE, "golden", "square_delaunay.msh"))
     np.testing.assert_array_equal(m.etov, g["etov"])
     np.testing.assert_array_equal(m.face_tag, g["face_tag"])
