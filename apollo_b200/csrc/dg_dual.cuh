@@ -82,6 +82,8 @@ struct Dual {
     return r;
   }
   APOLLO_HD friend Dual fabs(const Dual& a) { return a.v < 0.0 ? -a : a; }
+  // piecewise constant: derivative 0
+  APOLLO_HD friend Dual abs_int(const Dual& a) { return Dual(::apollo::abs_int(a.v)); }
 };
 
 }  // namespace apollo

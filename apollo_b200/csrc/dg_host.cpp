@@ -179,6 +179,20 @@ apollo_status check_ready(apollo_dg* h) {
   return APOLLO_OK;
 }
 
+// the mixed stage's fp32 face flux is the Lax-Friedrichs flux
+apollo_status check_mixed_flux(apollo_dg* h) {
+  if ((h->eq == EQ_EULER || h->eq == EQ_EULER2D) && (int)h->eqp.p[3] != NF_LF)
+    return fail(h, APOLLO_ERR_CONFIG, "mixed precision supports the Lax-Friedrichs flux only");
+  return APOLLO_OK;
+}
+
+// the adjoint's face terms are written for the Lax-Friedrichs flux
+apollo_status check_adjoint_flux(apollo_dg* h) {
+  if ((h->eq == EQ_EULER || h->eq == EQ_EULER2D) && (int)h->eqp.p[3] != NF_LF)
+    return fail(h, APOLLO_ERR_CONFIG, "the adjoint supports the Lax-Friedrichs flux only");
+  return APOLLO_OK;
+}
+
 // calls that need the whole mesh on this handle (no trace exchange)
 apollo_status check_whole(apollo_dg* h) {
   apollo_status r = check_ready(h);
@@ -201,6 +215,8 @@ apollo_status enqueue_stage(apollo_dg* h, const StageArgs& a, apollo_precision p
   cudaError_t e;
   if (prec == APOLLO_PREC_MIXED) {
     if (!h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision is not available for this equation/order");
+    apollo_status rf = check_mixed_flux(h);
+    if (rf) return rf;
     StageArgs am = a;
     if (am.mode == MODE_RHS) am.tr_scratch = h->T0_d;
     e = mixed_launch_rhs(h->mixed, h->eq, d, am, h->stream, ev);
@@ -316,6 +332,8 @@ apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const doubl
   else if (k == "maxwellTM") eq = EQ_MAXWELL_TM;
   else return fail(h, APOLLO_ERR_CONFIG, "unknown equation kind " + k);
   if (nparams < 0 || nparams > 4 || (nparams > 0 && !params)) return fail(h, APOLLO_ERR_ARG, "bad parameter list");
+  // the Euler kinds take three parameters; p[3] holds their numerical flux
+  if ((eq == EQ_EULER || eq == EQ_EULER2D) && nparams > 3) return fail(h, APOLLO_ERR_ARG, "eulerEqn takes 3 parameters");
   EqParams p{};
   for (int i = 0; i < nparams; ++i) p.p[i] = params[i];
   if ((eq == EQ_EULER || eq == EQ_EULER2D) && !(p.p[0] > 1.0))
@@ -336,14 +354,62 @@ apollo_status apollo_dg_add_bc(apollo_dg* h, const char* kind, const double* par
   if (nparams < 0 || nparams > 8 || (nparams > 0 && !params)) return fail(h, APOLLO_ERR_ARG, "bad parameter list");
   std::string k(kind);
   int b = -1;
+  double bp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int j = 0; j < nparams; ++j) bp[j] = params[j];
+  const bool euler_bc = k == "eulerWallBC" || k == "eulerZeroGradientBC" || k == "eulerInflowBC" || k == "eulerDirichletBC";
+  if (euler_bc && h->eq >= 0 && h->eq != EQ_EULER && h->eq != EQ_EULER2D)
+    return fail(h, APOLLO_ERR_CONFIG, k + " needs an Euler equation");
   if (k == "gridFixedBC") b = BC_FIXED;
   else if (k == "isentropicVortexBC") b = BC_VORTEX;
   else if (k == "maxwellTransverseMagneticBC") b = BC_TM;
   else if (k == "phmConductingWallBC") b = BC_PEC;
-  else return fail(h, APOLLO_ERR_CONFIG, "unknown boundary condition kind " + k);
+  else if (k == "eulerWallBC") b = BC_EULER_WALL;
+  else if (k == "eulerZeroGradientBC") b = BC_EULER_ZEROGRAD;
+  else if (k == "eulerInflowBC") {
+    // WxEulerInflowBC (wxeulerinflowbc.cc): Mach_number, Flow_angle (degrees),
+    // gas_gamma, Pressure, density -> the constant inflow state
+    if (nparams != 5) return fail(h, APOLLO_ERR_ARG, "eulerInflowBC takes Mach_number, Flow_angle, gas_gamma, Pressure, density");
+    const double mach = bp[0], angle = bp[1], gamma = bp[2], pres = bp[3], rho = bp[4];
+    const double pi = 3.141592653589793;
+    const double sound = std::sqrt(gamma * pres / rho);
+    const double u = mach * sound * std::cos(angle * pi / 180.), v = mach * sound * std::sin(angle * pi / 180.);
+    const double st[5] = {rho, rho * u, rho * v, 0.0, pres / (gamma - 1) + 0.5 * rho * (u * u + v * v)};
+    b = BC_EULER_STATE;
+    for (int j = 0; j < 8; ++j) bp[j] = j < 5 ? st[j] : 0.0;
+  } else if (k == "eulerDirichletBC") {
+    // WxEulerDirichletBC (wxeulerdirichletbc.cc): density, xvelocity,
+    // yvelocity, zvelocity, gas_gamma, pressure -> the constant state
+    if (nparams != 6)
+      return fail(h, APOLLO_ERR_ARG, "eulerDirichletBC takes density, xvelocity, yvelocity, zvelocity, gas_gamma, pressure");
+    const double rho = bp[0], u = bp[1], v = bp[2], w = bp[3], gamma = bp[4], pres = bp[5];
+    if (h->eq == EQ_EULER2D && w != 0.0) return fail(h, APOLLO_ERR_CONFIG, "eulerEqn2d has no z velocity");
+    const double st[5] = {rho, rho * u, rho * v, rho * w, pres / (gamma - 1) + 0.5 * rho * (u * u + v * v + w * w)};
+    b = BC_EULER_STATE;
+    for (int j = 0; j < 8; ++j) bp[j] = j < 5 ? st[j] : 0.0;
+  } else {
+    return fail(h, APOLLO_ERR_CONFIG, "unknown boundary condition kind " + k);
+  }
   int i = h->bcs.n++;
   h->bcs.kind[i] = b;
-  for (int j = 0; j < 8; ++j) h->bcs.p[i][j] = j < nparams ? params[j] : 0.0;
+  for (int j = 0; j < 8; ++j) h->bcs.p[i][j] = bp[j];
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name) {
+  if (!h || !name) return APOLLO_ERR_ARG;
+  if (h->eq < 0) return fail(h, APOLLO_ERR_STATE, "set the equation first");
+  const std::string n(name);
+  int kind = NF_LF;
+  if (h->eq == EQ_EULER || h->eq == EQ_EULER2D) {
+    if (n == "HLL") kind = NF_HLL;
+    else if (n == "Roe") kind = NF_ROE;
+    else if (n == "Wave") kind = NF_WAVE;
+    else if (n != "LF") h->err = "numerical flux " + n + " not recognised: Lax-Friedrichs used";
+    h->eqp.p[3] = kind;
+  }
+  // captured graphs hold the equation parameters
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return APOLLO_OK;
 }
 
@@ -942,6 +1008,10 @@ apollo_status handle_enqueue_step(apollo_dg* h, apollo_precision prec) {
 }
 apollo_status handle_enqueue_step_raw(apollo_dg* h, apollo_precision prec) { return enqueue_step(h, prec); }
 apollo_status handle_prepare_step(apollo_dg* h, apollo_precision prec) {
+  if (prec == APOLLO_PREC_MIXED) {
+    apollo_status rf = check_mixed_flux(h);
+    if (rf) return rf;
+  }
   if (prec == APOLLO_PREC_MIXED && h->mixed && !h->tu_valid) {
     DgDev d = make_dev(h);
     CK(mixed_launch_traces(h->mixed, d, h->U_d, h->TU_d, h->stream), "trace launch");
@@ -1006,6 +1076,7 @@ apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, doubl
 apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* ubar_0, int where) {
   apollo_status r = check_whole(h);
   if (r) return r;
+  if ((r = check_adjoint_flux(h))) return r;
   if (!ubar_T || !ubar_0) return APOLLO_ERR_ARG;
   if (!h->tr_valid) return fail(h, APOLLO_ERR_STATE, "no trajectory: call apollo_dg_forward_fixed first");
   const size_t nU = state_doubles(h);
@@ -1114,6 +1185,7 @@ apollo_status apollo_dg_rhs_jvp(apollo_dg* h, double t, const double* x, const d
 apollo_status apollo_dg_rhs_vjp(apollo_dg* h, double t, const double* x, const double* w, double* out, int where) {
   apollo_status r = check_whole(h);
   if (r) return r;
+  if ((r = check_adjoint_flux(h))) return r;
   if (!x || !w || !out) return APOLLO_ERR_ARG;
   if (where == APOLLO_DEVICE_PTR && (out == x || out == w))
     return fail(h, APOLLO_ERR_ARG, "the adjoint needs an output distinct from x and w");
@@ -1223,6 +1295,7 @@ apollo_status apollo_dg_dist_start(apollo_dg* h, double t, double dt, apollo_pre
 apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision prec) {
   apollo_status r = check_ready(h);
   if (r) return r;
+  if (prec == APOLLO_PREC_MIXED && (r = check_mixed_flux(h))) return r;
   if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
   if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");
   StageArgs a = stage_args(h, stage);
@@ -1244,6 +1317,7 @@ apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision pr
 apollo_status apollo_dg_stage_end(apollo_dg* h, int stage, apollo_precision prec) {
   apollo_status r = check_ready(h);
   if (r) return r;
+  if (prec == APOLLO_PREC_MIXED && (r = check_mixed_flux(h))) return r;
   if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
   if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");
   StageArgs a = stage_args(h, stage);

@@ -23,7 +23,16 @@ enum EqKind : int {
   EQ_MAXWELL_TM = 4  // phMaxwellEqn restricted to (Ez, Bx, By) with chi = gamma = 0, 3 fields
 };
 
-enum BcKind : int { BC_FIXED = 0, BC_VORTEX = 1, BC_TM = 2, BC_PEC = 3 };
+enum BcKind : int {
+  BC_FIXED = 0, BC_VORTEX = 1, BC_TM = 2, BC_PEC = 3,
+  BC_EULER_WALL = 4,      // eulerWallBC
+  BC_EULER_ZEROGRAD = 5,  // eulerZeroGradientBC
+  BC_EULER_STATE = 6      // eulerInflowBC / eulerDirichletBC: a constant ghost state, p = (rho, rhou, rhov, rhow, E)
+};
+
+// Euler numerical fluxes by Apollo's Numerical_Flux codes (wxeulereqn.cc:10-15);
+// stored in EqParams::p[3] of the Euler kinds
+enum NumFlux : int { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4 };
 
 enum ErrBits : int { ERRB_NONPHYS = 1, ERRB_NAN = 2, ERRB_TIMEOUT = 4 };
 
@@ -42,6 +51,12 @@ struct BcTable {
 template <int EQ> struct Eq;
 
 APOLLO_HD double dmax2(double a, double b) { return a > b ? a : b; }
+// |x| after conversion to int (truncation toward zero).  Apollo's HLL flux
+// calls abs() on a double where only int abs(int) is declared
+// (wxeulereqn.cc:1170), so its wave-speed bound |S_R| enters truncated;
+// reproduced for |x| < 2^31.
+APOLLO_HD double abs_int(double x) { return (double)abs((int)x); }
+APOLLO_HD float abs_int(float x) { return (float)abs((int)x); }
 APOLLO_HD double dmax3(double a, double b, double c) {
   double m1 = a > b ? a : b;
   return m1 > c ? m1 : c;
@@ -129,8 +144,22 @@ struct EulerBase {
       qc[IE] = minP / (gamma - T(1.)) + T(0.5) * qp[0] * (qp[1] * qp[1] + qp[2] * qp[2] + qp[3] * qp[3]);
     }
   }
+  // DGnumericalFlux by the Numerical_Flux code in P.p[3] (wxeulereqn.cc:876-893).
+  // qM and qP are modified as the reference modifies them (primitive-variable
+  // floors, the rotation of HLL, Roe and Wave).
   template <class T>
   APOLLO_HD static T numflux(const EqParams& P, T nx, T ny, T* qM, T* qP, T* nf, int* err) {
+    const int kind = (int)P.p[3];
+    if (kind == NF_HLL) return hll(P, nx, ny, qM, qP, nf, err);
+    if (kind == NF_ROE) return roe(P, nx, ny, qM, qP, nf, err);
+    // case 4 (Wave) falls through to the Lax-Friedrichs flux (:888-892): what
+    // remains of the wave-propagation flux is its effect on the traces
+    if (kind == NF_WAVE) wave_prelude(P, nx, ny, qM, qP, err);
+    return lf(P, nx, ny, qM, qP, nf, err);
+  }
+  // Lax-Friedrichs (:1097-1117)
+  template <class T>
+  APOLLO_HD static T lf(const EqParams& P, T nx, T ny, T* qM, T* qP, T* nf, int* err) {
     T fM[MF], fP[MF], gM[MF], gP[MF], pM[5], pP[5];
     flux2(P, qM, fM, gM, err);
     flux2(P, qP, fP, gP, err);
@@ -144,6 +173,142 @@ struct EulerBase {
     for (int c = 0; c < MF; ++c)
       nf[c] = T(0.5) * (nx * (fM[c] + fP[c]) + ny * (gM[c] + gP[c]) + lambda * (qM[c] - qP[c]));
     return lambda;
+  }
+  // momentum into the face's normal-tangent frame, in place
+  template <class T>
+  APOLLO_HD static void rotate_in(T nx, T ny, T* q) {
+    T ru = q[1], rv = q[2];
+    q[1] = nx * ru + ny * rv;
+    q[2] = -ny * ru + nx * rv;
+  }
+  template <class T>
+  APOLLO_HD static T max_speed(const EqParams& P, const T* pM, const T* pP) {
+    T gamma = T(P.p[0]);
+    T c0M = sqrt(pM[1] * pM[1] + pM[2] * pM[2] + pM[3] * pM[3]) + sqrt(gamma * pM[4] / pM[0]);
+    T c0P = sqrt(pP[1] * pP[1] + pP[2] * pP[2] + pP[3] * pP[3]) + sqrt(gamma * pP[4] / pP[0]);
+    return c0M > c0P ? c0M : c0P;
+  }
+  // Roe-averaged velocity and enthalpy of the rotated, floored traces
+  template <class T>
+  APOLLO_HD static void roe_avg(const EqParams& P, const T* qM, const T* qP, const T* pM, const T* pP, T& rMs,
+                                T& rPs, T& u, T& v, T& w, T& H) {
+    T HM = (qM[IE] + pM[4]) / pM[0];
+    T HP = (qP[IE] + pP[4]) / pP[0];
+    rMs = sqrt(pM[0]);
+    rPs = sqrt(pP[0]);
+    u = (rMs * pM[1] + rPs * pP[1]) / (rMs + rPs);
+    v = (rMs * pM[2] + rPs * pP[2]) / (rMs + rPs);
+    w = (rMs * pM[3] + rPs * pP[3]) / (rMs + rPs);
+    H = (rMs * HM + rPs * HP) / (rMs + rPs);
+  }
+  // HLL (:1121-1202), with the reference's truncated |S_R| (abs_int)
+  template <class T>
+  APOLLO_HD static T hll(const EqParams& P, T nx, T ny, T* qM, T* qP, T* nf, int* err) {
+    T fM[MF], fP[MF], gM[MF], gP[MF], pM[5], pP[5], fx[MF];
+    rotate_in(nx, ny, qM);
+    rotate_in(nx, ny, qP);
+    flux2(P, qM, fM, gM, err);  // the y fluxes are evaluated (and checked), not used
+    flux2(P, qP, fP, gP, err);
+    prim(P, qM, pM);
+    prim(P, qP, pP);
+    const T gamma = T(P.p[0]);
+    const T cM = sqrt(gamma * pM[4] / pM[0]), cP = sqrt(gamma * pP[4] / pP[0]);
+    T rMs, rPs, u, v, w, H;
+    roe_avg(P, qM, qP, pM, pP, rMs, rPs, u, v, w, H);
+    const T c2 = (gamma - T(1.)) * (H - T(0.5) * (u * u + v * v + w * w)), c = sqrt(c2);
+    T a = pM[1] - cM, b = u - c;
+    const T SL = a < b ? a : b;
+    a = pP[1] + cP;
+    b = u + c;
+    const T SR = a > b ? a : b;
+    const T zero = T(0.0);
+    const T t1 = ((SR < zero ? SR : zero) - (zero < SL ? zero : SL)) / (SR - SL);
+    const T t2 = T(1.) - t1;
+    const T t3 = (SR * fabs(SL) - SL * abs_int(SR)) / (T(2.) * (SR - SL));
+#pragma unroll
+    for (int n = 0; n < MF; ++n) fx[n] = t1 * fP[n] + t2 * fM[n] - t3 * (qP[n] - qM[n]);
+    nf[0] = fx[0];
+    nf[1] = nx * fx[1] - ny * fx[2];
+    nf[2] = ny * fx[1] + nx * fx[2];
+    if (MF == 5) nf[3] = T(0.0);
+    nf[IE] = fx[IE];
+    return max_speed(P, pM, pP);
+  }
+  // Roe (:1206-1275).  The reference assigns nflux[1] twice (:1267-1268), the
+  // second time with the y-momentum flux, and never sets nflux[2]: its
+  // zero-initialised flux buffer (wxnodaldg2dmethod.cc:98) keeps 0 there.
+  template <class T>
+  APOLLO_HD static T roe(const EqParams& P, T nx, T ny, T* qM, T* qP, T* nf, int* err) {
+    T fM[MF], fP[MF], pM[5], pP[5], fx[MF];
+    rotate_in(nx, ny, qM);
+    rotate_in(nx, ny, qP);
+    prim(P, qM, pM);
+    prim(P, qP, pP);
+    const T gamma = T(P.p[0]);
+    T rMs, rPs, u, v, w, H;
+    roe_avg(P, qM, qP, pM, pP, rMs, rPs, u, v, w, H);
+    const T rho = rMs * rPs;
+    const T c2 = (gamma - T(1.)) * (H - T(0.5) * (u * u + v * v + w * w)), c = sqrt(c2);
+    T dw1 = T(-0.5) * rho * (pP[1] - pM[1]) / c + T(0.5) * (pP[4] - pM[4]) / c2;
+    T dw2 = (pP[0] - pM[0]) - (pP[4] - pM[4]) / c2;
+    T dw3 = rho * (pP[2] - pM[2]);
+    T dw4 = T(0.5) * rho * (pP[1] - pM[1]) / c + T(0.5) * (pP[4] - pM[4]) / c2;
+    dw1 = fabs(u - c) * dw1;
+    dw2 = fabs(u) * dw2;
+    dw3 = fabs(u) * dw3;
+    dw4 = fabs(u + c) * dw4;
+    flux_dir(P, 0, qM, fM, err);
+    flux_dir(P, 0, qP, fP, err);
+#pragma unroll
+    for (int n = 0; n < MF; ++n) fx[n] = T(0.5) * (fM[n] + fP[n]);
+    fx[0] = fx[0] - T(0.5) * (dw1 * T(1.) + dw2 * T(1.) + dw3 * T(0.) + dw4 * T(1.));
+    fx[1] = fx[1] - T(0.5) * (dw1 * (u - c) + dw2 * u + dw3 * T(0.) + dw4 * (u + c));
+    fx[2] = fx[2] - T(0.5) * (dw1 * v + dw2 * v + dw3 * T(1.) + dw4 * v);
+    fx[IE] = fx[IE] - T(0.5) * (dw1 * (H - u * c) + dw2 * (u * u + v * v) / T(2.) + dw3 * v + dw4 * (H + u * c));
+    nf[0] = fx[0];
+    nf[1] = ny * fx[1] + nx * fx[2];
+    nf[2] = T(0.0);
+    if (MF == 5) nf[3] = T(0.0);
+    nf[IE] = fx[IE];
+    return max_speed(P, pM, pP);
+  }
+  // The part of the wave-propagation flux (:1279-1322) that outlives the
+  // fall-through: the traces rotated in place, the x fluxes' checks, and the
+  // Riemann solver rp(0, ql = qP, qr = qM) (:94-235) with its checks and
+  // pressure floor on the traces' energies.
+  template <class T>
+  APOLLO_HD static void wave_prelude(const EqParams& P, T nx, T ny, T* qM, T* qP, int* err) {
+    T fM[MF], fP[MF];
+    rotate_in(nx, ny, qM);
+    rotate_in(nx, ny, qP);
+    flux_dir(P, 0, qM, fM, err);
+    flux_dir(P, 0, qP, fP, err);
+    T* ql = qP;
+    T* qr = qM;
+    if (ql[0] < T(0) || qr[0] < T(0)) {
+      *err |= ERRB_NONPHYS;
+      return;
+    }
+    const T g1 = T(P.p[0]) - T(1), minP = T(P.p[1]);
+    const T l3 = MF == 5 ? ql[3] : T(0), r3 = MF == 5 ? qr[3] : T(0);
+    const T rl = sqrt(ql[0]), rr = sqrt(qr[0]);
+    T pl = g1 * (ql[IE] - T(0.5) * (ql[1] * ql[1] + ql[2] * ql[2] + l3 * l3) / ql[0]);
+    T pr = g1 * (qr[IE] - T(0.5) * (qr[1] * qr[1] + qr[2] * qr[2] + r3 * r3) / qr[0]);
+    if (minP == T(0) && (pl < T(0) || pr < T(0))) *err |= ERRB_NONPHYS;
+    if (pl < minP) {
+      ql[IE] = minP / (T(P.p[0]) - T(1)) + T(0.5) * (ql[1] * ql[1] + ql[2] * ql[2] + l3 * l3) / ql[0];
+      pl = minP;
+    }
+    if (pr < minP) {
+      qr[IE] = minP / (T(P.p[0]) - T(1)) + T(0.5) * (qr[1] * qr[1] + qr[2] * qr[2] + r3 * r3) / qr[0];
+      pr = minP;
+    }
+    const T rsq2 = rl + rr;
+    const T u = (ql[1] / rl + qr[1] / rr) / rsq2;
+    const T v = (ql[2] / rl + qr[2] / rr) / rsq2;
+    const T w = (l3 / rl + r3 / rr) / rsq2;
+    const T enth = ((ql[IE] + pl) / rl + (qr[IE] + pr) / rr) / rsq2;
+    if (g1 * (enth - T(0.5) * (u * u + v * v + w * w)) < T(0)) *err |= ERRB_NONPHYS;
   }
   APOLLO_HD static double lf_lambda(const EqParams& P, const double* qM, const double* qP) {
     double a[MF], b[MF], pM[5], pP[5];
@@ -296,6 +461,24 @@ APOLLO_HD void apply_bc(const BcTable& B, int tag, double t, double x, double y,
       qb[2] = T(rho1 * v);
       if (M == 5) qb[3] = T(0.0);
       qb[M - 1] = T(p1 / (gamma - 1) + 0.5 * rho1 * (u * u + v * v));
+    }
+  } else if (kind == BC_EULER_WALL) {
+    // WxEulerWallBC::applyBC (wxeulerwallbc.cc:13-22): normal momentum reflected
+    if (EQ == EQ_EULER || EQ == EQ_EULER2D) {
+      qb[1] = q[1] - T(2.) * (nx * q[1] + ny * q[2]) * nx;
+      qb[2] = q[2] - T(2.) * (nx * q[1] + ny * q[2]) * ny;
+      if (M == 5) qb[3] = T(0.0);
+    }
+  } else if (kind == BC_EULER_ZEROGRAD) {
+    // WxEulerZeroGradientBC::applyBC: the interior trace (copied above)
+  } else if (kind == BC_EULER_STATE) {
+    // WxEulerInflowBC / WxEulerDirichletBC::applyBC: a state fixed at setup
+    if (EQ == EQ_EULER || EQ == EQ_EULER2D) {
+      qb[0] = T(p[0]);
+      qb[1] = T(p[1]);
+      qb[2] = T(p[2]);
+      if (M == 5) qb[3] = T(p[3]);
+      qb[M - 1] = T(p[4]);
     }
   } else if (kind == BC_TM) {
     if (EQ == EQ_MAXWELL) qb[2] = -q[2];

@@ -66,6 +66,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_create": (C.c_int, [C.POINTER(_Config), C.POINTER(H)]),
         "apollo_dg_set_equation": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_add_bc": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
+        "apollo_dg_set_numerical_flux": (C.c_int, [H, C.c_char_p]),
         "apollo_dg_set_mesh": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip]),
         "apollo_dg_num_fields": (C.c_int, [H]),
         "apollo_dg_num_nodes": (C.c_int, [H]),
@@ -150,7 +151,7 @@ class NodalDG2d:
     """One nodal-DG discretisation on the GPU (Apollo ``Kind = nodalDG2d``)."""
 
     def __init__(self, N: int, cfl: float, equation: str, eq_params, mesh: Mesh, bcs=(), device: int = 0,
-                 stream: int | None = None, part=None, rank: int = 0):
+                 stream: int | None = None, part=None, rank: int = 0, numerical_flux: str = "LF"):
         """``part`` (int32 [K], optional): a partition of ``mesh``; the handle then
         holds the elements with ``part == rank`` (apollo_dg_set_mesh_partition)
         and steps through ``apollo_b200.distributed.DistNodalDG2d``."""
@@ -161,6 +162,7 @@ class NodalDG2d:
         self.h = h
         p = np.asarray(list(eq_params), dtype=np.float64)
         self._check(self.lib.apollo_dg_set_equation(h, equation.encode(), p.ctypes.data_as(_dp), len(p)))
+        self._check(self.lib.apollo_dg_set_numerical_flux(h, numerical_flux.encode()))
         for kind, params in bcs:
             bp = np.asarray(list(params), dtype=np.float64)
             self._check(self.lib.apollo_dg_add_bc(h, kind.encode(), bp.ctypes.data_as(_dp), len(bp)))

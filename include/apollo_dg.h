@@ -81,12 +81,27 @@ apollo_status apollo_dg_create(const apollo_dg_config* cfg, apollo_dg** out);
  * Numerical flux: Lax-Friedrichs ("Numerical_Flux = LF"). */
 apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const double* params, int nparams);
 
+/* Euler numerical flux by Apollo's "Numerical_Flux" name (WxEulerEqn::setup,
+ * src/hyperapps/euler/wxeulereqn.cc:45-87): "LF" (default), "HLL", "Roe",
+ * "Wave"; any other name selects LF, as Apollo does (the call succeeds and
+ * apollo_dg_last_error says so).  The fluxes reproduce Apollo's arithmetic,
+ * including its HLL bound |S_R| truncated to an integer, its Roe flux's
+ * y-momentum component of 0 and x-momentum component set from the rotated
+ * y-momentum flux, and Wave's fall-through to LF on rotated traces.  Other
+ * equations have only LF (the name is ignored).  Mixed precision and the
+ * adjoint support LF only (APOLLO_ERR_CONFIG otherwise). */
+apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
+
 /* Boundary-condition plugin, appended to the list; a face tagged t uses the
  * t-th condition added (Apollo's boundaryConditions[t-1]).  Kinds and params:
  *   "gridFixedBC"                   value
  *   "isentropicVortexBC"            u0, v0, x0, y0, gas_gamma, beta
  *   "maxwellTransverseMagneticBC"   (none)
- *   "phmConductingWallBC"           (none)                                      */
+ *   "phmConductingWallBC"           (none)
+ *   "eulerWallBC"                   (none)      normal momentum reflected
+ *   "eulerZeroGradientBC"           (none)      interior state
+ *   "eulerInflowBC"                 Mach_number, Flow_angle (degrees), gas_gamma, Pressure, density
+ *   "eulerDirichletBC"              density, xvelocity, yvelocity, zvelocity, gas_gamma, pressure  */
 apollo_status apollo_dg_add_bc(apollo_dg* h, const char* kind, const double* params, int nparams);
 
 /* Mesh: vertices (vx, vy), counter-clockwise triangles etov[K][3] (vertex 0 ->

@@ -212,7 +212,10 @@ inline double dmax2(double a, double b) { return a > b ? a : b; }
 inline double dmax3(double a, double b, double c) { double m1 = a > b ? a : b; return m1 > c ? m1 : c; }
 
 enum { EQ_ADVECTION = 0, EQ_EULER = 1, EQ_MAXWELL = 2 };
-enum { BC_FIXED = 0, BC_VORTEX = 1, BC_TM = 2, BC_PEC = 3 };
+enum { BC_FIXED = 0, BC_VORTEX = 1, BC_TM = 2, BC_PEC = 3, BC_EULER_WALL = 4, BC_EULER_INFLOW = 5,
+       BC_EULER_ZEROGRAD = 6, BC_EULER_DIRICHLET = 7 };
+// Euler Numerical_Flux codes (wxeulereqn.cc:10-15), held in eqp[3]
+enum { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4 };
 enum { ERR_NONPHYS = 1, ERR_NAN = 2, ERR_JAC = 4 };
 
 typedef void (*flux_fn)(void* ctx, int d, const double* q, double* f);
@@ -296,12 +299,132 @@ void eq_flux(Oracle& o, int d, const double* q, double* f) {
   else maxwell_flux(o, d, q, f);
 }
 
+// Euler fluxes other than LF, following wxeulereqn.cc:1121-1322 step by step.
+// Momentum to the face's normal-tangent frame, in place.
+void euler_rotate(const double* n, double* q) {
+  double ru = q[1], rv = q[2];
+  q[1] = n[0] * ru + n[1] * rv;
+  q[2] = -n[1] * ru + n[0] * rv;
+}
+double euler_speed(const Oracle& o, const double* pM, const double* pP) {
+  double gamma = o.eqp[0];
+  double c0M = std::sqrt(pM[1] * pM[1] + pM[2] * pM[2] + pM[3] * pM[3]) + std::sqrt(gamma * pM[4] / pM[0]);
+  double c0P = std::sqrt(pP[1] * pP[1] + pP[2] * pP[2] + pP[3] * pP[3]) + std::sqrt(gamma * pP[4] / pP[0]);
+  return dmax2(c0M, c0P);
+}
+// HLL, :1121-1202.  abs(SR) there is int abs(int) (only <cmath> and the C
+// library's int abs are in scope), so SR enters truncated toward zero.
+double euler_hll(Oracle& o, const double* n, double* qM, double* qP, double* nf) {
+  double fM[5], fP[5], gM[5], gP[5], pM[5], pP[5], fx[5];
+  double gamma = o.eqp[0];
+  euler_rotate(n, qM);
+  euler_rotate(n, qP);
+  euler_flux(o, 0, qM, fM); euler_flux(o, 0, qP, fP); euler_flux(o, 1, qM, gM); euler_flux(o, 1, qP, gP);
+  euler_prim(o, qM, pM); euler_prim(o, qP, pP);
+  double HM = (qM[4] + pM[4]) / pM[0], cM = std::sqrt(gamma * pM[4] / pM[0]);
+  double HP = (qP[4] + pP[4]) / pP[0], cP = std::sqrt(gamma * pP[4] / pP[0]);
+  double rMs = std::sqrt(pM[0]), rPs = std::sqrt(pP[0]);
+  double u = (rMs * pM[1] + rPs * pP[1]) / (rMs + rPs);
+  double v = (rMs * pM[2] + rPs * pP[2]) / (rMs + rPs);
+  double w = (rMs * pM[3] + rPs * pP[3]) / (rMs + rPs);
+  double H = (rMs * HM + rPs * HP) / (rMs + rPs);
+  double c2 = (gamma - 1.) * (H - 0.5 * (u * u + v * v + w * w)), c = std::sqrt(c2);
+  double a = pM[1] - cM, b = u - c;
+  double SL = a < b ? a : b;
+  a = pP[1] + cP;
+  b = u + c;
+  double SR = a > b ? a : b;
+  double zero = 0.0;
+  double t1 = ((SR < zero ? SR : zero) - (zero < SL ? zero : SL)) / (SR - SL);
+  double t2 = 1. - t1;
+  double t3 = (SR * std::fabs(SL) - SL * (double)std::abs((int)SR)) / (2. * (SR - SL));
+  for (int i = 0; i < 5; ++i) fx[i] = t1 * fP[i] + t2 * fM[i] - t3 * (qP[i] - qM[i]);
+  nf[0] = fx[0];
+  nf[1] = n[0] * fx[1] - n[1] * fx[2];
+  nf[2] = n[1] * fx[1] + n[0] * fx[2];
+  nf[3] = 0.0;
+  nf[4] = fx[4];
+  return euler_speed(o, pM, pP);
+}
+// Roe, :1206-1275: nflux[1] is assigned twice (the second, y-momentum, value
+// stays) and nflux[2] is never set, so it keeps the caller's buffer, which is
+// Apollo's zero-initialised flux array (wxnodaldg2dmethod.cc:98).
+double euler_roe(Oracle& o, const double* n, double* qM, double* qP, double* nf) {
+  double fM[5], fP[5], pM[5], pP[5], fx[5];
+  double gamma = o.eqp[0];
+  euler_rotate(n, qM);
+  euler_rotate(n, qP);
+  euler_prim(o, qM, pM); euler_prim(o, qP, pP);
+  double HM = (qM[4] + pM[4]) / pM[0];
+  double HP = (qP[4] + pP[4]) / pP[0];
+  double rMs = std::sqrt(pM[0]), rPs = std::sqrt(pP[0]);
+  double rho = rMs * rPs;
+  double u = (rMs * pM[1] + rPs * pP[1]) / (rMs + rPs);
+  double v = (rMs * pM[2] + rPs * pP[2]) / (rMs + rPs);
+  double w = (rMs * pM[3] + rPs * pP[3]) / (rMs + rPs);
+  double H = (rMs * HM + rPs * HP) / (rMs + rPs);
+  double c2 = (gamma - 1.) * (H - 0.5 * (u * u + v * v + w * w)), c = std::sqrt(c2);
+  double dw1 = -0.5 * rho * (pP[1] - pM[1]) / c + 0.5 * (pP[4] - pM[4]) / c2;
+  double dw2 = (pP[0] - pM[0]) - (pP[4] - pM[4]) / c2;
+  double dw3 = rho * (pP[2] - pM[2]);
+  double dw4 = 0.5 * rho * (pP[1] - pM[1]) / c + 0.5 * (pP[4] - pM[4]) / c2;
+  dw1 = std::fabs(u - c) * dw1;
+  dw2 = std::fabs(u) * dw2;
+  dw3 = std::fabs(u) * dw3;
+  dw4 = std::fabs(u + c) * dw4;
+  euler_flux(o, 0, qM, fM);
+  euler_flux(o, 0, qP, fP);
+  for (int i = 0; i < 5; ++i) fx[i] = 0.5 * (fM[i] + fP[i]);
+  fx[0] -= 0.5 * (dw1 * 1. + dw2 * 1. + dw3 * 0. + dw4 * 1.);
+  fx[1] -= 0.5 * (dw1 * (u - c) + dw2 * u + dw3 * 0. + dw4 * (u + c));
+  fx[2] -= 0.5 * (dw1 * v + dw2 * v + dw3 * 1. + dw4 * v);
+  fx[3] = 0.0;
+  fx[4] -= 0.5 * (dw1 * (H - u * c) + dw2 * (u * u + v * v) / 2. + dw3 * v + dw4 * (H + u * c));
+  nf[0] = fx[0];
+  nf[1] = n[1] * fx[1] + n[0] * fx[2];
+  nf[2] = 0.0;
+  nf[3] = 0.0;
+  nf[4] = fx[4];
+  return euler_speed(o, pM, pP);
+}
+// Wave, :1279-1322 then the switch's fall-through into LF (:888-892): the
+// traces are rotated in place and pass the Riemann solver rp(0, qP, qM)
+// (:94-199), whose checks may fail and whose pressure floor may rewrite the
+// energies; the wave flux itself is overwritten by the LF flux that follows.
+void euler_wave_prelude(Oracle& o, const double* n, double* qM, double* qP) {
+  double fM[5], fP[5];
+  euler_rotate(n, qM);
+  euler_rotate(n, qP);
+  euler_flux(o, 0, qM, fM);
+  euler_flux(o, 0, qP, fP);
+  double* ql = qP;
+  double* qr = qM;
+  double g1 = o.eqp[0] - 1, minP = o.eqp[1];
+  if (ql[0] < 0 || qr[0] < 0) { o.err |= ERR_NONPHYS; return; }
+  double rl = std::sqrt(ql[0]), rr = std::sqrt(qr[0]);
+  double pl = g1 * (ql[4] - 0.5 * (ql[1] * ql[1] + ql[2] * ql[2] + ql[3] * ql[3]) / ql[0]);
+  double pr = g1 * (qr[4] - 0.5 * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]) / qr[0]);
+  if (minP == 0.0 && (pl < 0 || pr < 0)) o.err |= ERR_NONPHYS;
+  if (pl < minP) { ql[4] = minP / (o.eqp[0] - 1) + 0.5 * (ql[1] * ql[1] + ql[2] * ql[2] + ql[3] * ql[3]) / ql[0]; pl = minP; }
+  if (pr < minP) { qr[4] = minP / (o.eqp[0] - 1) + 0.5 * (qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]) / qr[0]; pr = minP; }
+  double rsq2 = rl + rr;
+  double u = (ql[1] / rl + qr[1] / rr) / rsq2, v = (ql[2] / rl + qr[2] / rr) / rsq2, w = (ql[3] / rl + qr[3] / rr) / rsq2;
+  double enth = ((ql[4] + pl) / rl + (qr[4] + pr) / rr) / rsq2;
+  if (g1 * (enth - 0.5 * (u * u + v * v + w * w)) < 0) o.err |= ERR_NONPHYS;
+}
+
 // DGnumericalFlux (qM/qP may be modified by the Euler primitive clamp, as in
 // the reference).
 void eq_numflux(Oracle& o, const double* n, double* qM, double* qP, double* nf, double* lam) {
   if (o.ref_numflux) { o.ref_numflux(o.ref_ctx, n, qM, qP, nf, lam); return; }
   double fM[8], fP[8], gM[8], gP[8], lambda;
   int m = o.meqn;
+  if (o.eq == EQ_EULER) {
+    const int kind = (int)o.eqp[3];
+    if (kind == NF_HLL) { *lam = euler_hll(o, n, qM, qP, nf); return; }
+    if (kind == NF_ROE) { *lam = euler_roe(o, n, qM, qP, nf); return; }
+    if (kind == NF_WAVE) euler_wave_prelude(o, n, qM, qP);
+  }
   if (o.eq == EQ_ADVECTION) {
     adv_flux(o, 0, qM, fM); adv_flux(o, 0, qP, fP); adv_flux(o, 1, qM, gM); adv_flux(o, 1, qP, gP);
     lambda = dmax2(std::fabs(o.eqp[0]), std::fabs(o.eqp[1]));
@@ -379,6 +502,29 @@ void apply_bc(const Oracle& o, int tag, const double* xc, const double* nx, cons
     double p1 = std::pow(rho1, gamma);
     qb[0] = rho1; qb[1] = rho1 * u; qb[2] = rho1 * v; qb[3] = 0.0;
     qb[4] = p1 / (gamma - 1) + 0.5 * rho1 * (u * u + v * v);
+  } else if (kind == BC_EULER_WALL) {
+    // wxeulerwallbc.cc
+    qb[0] = q[0];
+    qb[1] = q[1] - 2. * (nx[0] * q[1] + nx[1] * q[2]) * nx[0];
+    qb[2] = q[2] - 2. * (nx[0] * q[1] + nx[1] * q[2]) * nx[1];
+    qb[3] = 0.0;
+    qb[4] = q[4];
+  } else if (kind == BC_EULER_INFLOW) {
+    // wxeulerinflowbc.cc: Mach_number, Flow_angle, gas_gamma, Pressure, density
+    double mach = p[0], angle = p[1], gamma = p[2], pres = p[3], rho = p[4];
+    double pi = 3.141592653589793;
+    double sound = std::sqrt(gamma * pres / rho);
+    double u = mach * sound * std::cos(angle * pi / 180.), v = mach * sound * std::sin(angle * pi / 180.);
+    qb[0] = rho; qb[1] = rho * u; qb[2] = rho * v; qb[3] = 0.0;
+    qb[4] = pres / (gamma - 1) + 0.5 * rho * (u * u + v * v);
+  } else if (kind == BC_EULER_ZEROGRAD) {
+    // wxeulerzerogradientbc.cc
+    for (int c = 0; c < 5; ++c) qb[c] = q[c];
+  } else if (kind == BC_EULER_DIRICHLET) {
+    // wxeulerdirichletbc.cc: density, xvelocity, yvelocity, zvelocity, gas_gamma, pressure
+    double rho = p[0], u = p[1], v = p[2], w = p[3], gamma = p[4], pres = p[5];
+    qb[0] = rho; qb[1] = rho * u; qb[2] = rho * v; qb[3] = rho * w;
+    qb[4] = pres / (gamma - 1) + 0.5 * rho * (u * u + v * v + w * w);
   } else if (kind == BC_TM) {
     for (int c = 0; c < m; ++c) qb[c] = q[c];
     qb[2] = -q[2];

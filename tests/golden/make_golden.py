@@ -37,6 +37,30 @@ def gmsh_vortex(N: int = 3):
     return problems.Problem("gmsh_vortex", N, 0.5, "eulerEqn", (1.4, 0.0, 0.0), mesh, (), 0,
                             ic=lambda x, y: problems.vortex_ic(x, y, 5, beta=5.0))
 
+def channel(N: int = 3, n: int = 7, seed: int = 2):
+    """Euler flow through [0,2] x [0,1] (5 fields): bottom wall (tag 1), right
+    zero-gradient outflow (2), top inflow (3), left Dirichlet state (4); a
+    density bump and a transverse velocity wave on a uniform stream."""
+    from apollo_b200.mesh import jittered_square
+    mesh = jittered_square(n, (0.0, 0.0), (2.0, 1.0), seed=seed, periodic=False, wall_tag=1)
+    for f, (i, j) in enumerate(((0, 1), (1, 2), (2, 0))):
+        xa, ya = mesh.vx[mesh.etov[:, i]], mesh.vy[mesh.etov[:, i]]
+        xb, yb = mesh.vx[mesh.etov[:, j]], mesh.vy[mesh.etov[:, j]]
+        mesh.face_tag[:, f] = np.select([(ya == 0) & (yb == 0), (xa == 2) & (xb == 2), (ya == 1) & (yb == 1),
+                                         (xa == 0) & (xb == 0)], [1, 2, 3, 4], 0)
+
+    def ic(x, y):
+        rho = 1.0 + 0.2 * np.exp(-((x - 1.0) ** 2 + (y - 0.5) ** 2) / 0.05)
+        u, v, p = 0.5 + 0 * x, 0.1 * np.sin(np.pi * x), 1.0 + 0 * x
+        return np.stack([rho, rho * u, rho * v, 0 * x, p / 0.4 + 0.5 * rho * (u * u + v * v)], axis=-1)
+
+    return problems.Problem("channel", N, 0.5, "eulerEqn", (1.4, 0.0, 0.0), mesh, (), 0, ic=ic)
+
+
+CHANNEL_BCS = ((orc.BC_EULER_WALL, ()), (orc.BC_EULER_ZEROGRAD, ()),
+               (orc.BC_EULER_INFLOW, (0.4, -60.0, 1.4, 1.0, 1.0)),
+               (orc.BC_EULER_DIRICHLET, (1.0, 0.5, 0.0, 0.0, 1.4, 1.0)))
+
 CASES = [
     # name, builder, kwargs, oracle eq, eq params, ref kind, ref params, bcs, steps
     ("adv_N3", problems.advection, dict(n=8, N=3), orc.EQ_ADVECTION, (1.0, 0.5, 0.0), "advectionEqn",
@@ -53,7 +77,15 @@ CASES = [
      "phMaxwellEqn", dict(c0=1.0), ((orc.BC_TM, ()),), 3),
     ("euler_gmsh_N3", gmsh_vortex, dict(N=3), orc.EQ_EULER, (1.4, 0.0, 0.0), "eulerEqn", dict(gas_gamma=1.4),
      ((orc.BC_VORTEX, VORTEX_BC), (orc.BC_VORTEX, VORTEX_BC)), 3),
+    ("euler_hll_N3", channel, dict(N=3), orc.EQ_EULER, (1.4, 0.0, 0.0, orc.NF_HLL), "eulerEqn",
+     dict(gas_gamma=1.4, Numerical_Flux="HLL"), CHANNEL_BCS, 3),
+    ("euler_roe_N4", channel, dict(N=4, seed=3), orc.EQ_EULER, (1.4, 0.0, 0.0, orc.NF_ROE), "eulerEqn",
+     dict(gas_gamma=1.4, Numerical_Flux="Roe"), CHANNEL_BCS, 0),  # Apollo's Roe flux is non-physical within a step
+    ("euler_wave_N2", channel, dict(N=2, n=8), orc.EQ_EULER, (1.4, 0.0, 0.0, orc.NF_WAVE), "eulerEqn",
+     dict(gas_gamma=1.4, Numerical_Flux="Wave"), CHANNEL_BCS, 1),  # non-physical from the second step
 ]
+
+FLUX_NAMES = {orc.NF_LF: "LF", orc.NF_HLL: "HLL", orc.NF_ROE: "Roe", orc.NF_WAVE: "Wave"}
 
 
 def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref):
@@ -72,7 +104,8 @@ def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref)
     np.savez_compressed(
         os.path.join(HERE, f"{name}.npz"),
         vx=mesh.vx, vy=mesh.vy, etov=mesh.etov, face_tag=mesh.face_tag, vert_canon=mesh.vert_canon,
-        N=prob.N, cfl=prob.cfl, eq=eq, eqp=np.asarray(eqp, dtype=np.float64), equation=ref_kind,
+        N=prob.N, cfl=prob.cfl, eq=eq, eqp=np.asarray(list(eqp) + [0.0] * (4 - len(eqp)), dtype=np.float64),
+        equation=ref_kind, numflux=FLUX_NAMES[int(eqp[3]) if len(eqp) > 3 else 0],
         bc_kinds=np.asarray([b[0] for b in bcs], dtype=np.int32),
         bc_params=np.asarray([list(b[1]) + [0.0] * (8 - len(b[1])) for b in bcs], dtype=np.float64).reshape(-1, 8),
         x=x, y=y, U0=U0, rhs=rhs, sugg=sugg, dt0=dt0,

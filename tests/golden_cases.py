@@ -9,7 +9,10 @@ from apollo_b200.mesh import Mesh
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 NAMES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "*.npz")))
 
-BC_NAMES = {0: "gridFixedBC", 1: "isentropicVortexBC", 2: "maxwellTransverseMagneticBC", 3: "phmConductingWallBC"}
+BC_NAMES = {0: "gridFixedBC", 1: "isentropicVortexBC", 2: "maxwellTransverseMagneticBC", 3: "phmConductingWallBC",
+            4: "eulerWallBC", 5: "eulerInflowBC", 6: "eulerZeroGradientBC", 7: "eulerDirichletBC"}
+# the parameters each kind takes, of the 8 stored per condition
+BC_NPARAMS = {0: 1, 1: 6, 2: 0, 3: 0, 4: 0, 5: 5, 6: 0, 7: 6}
 
 
 def load(name):
@@ -19,8 +22,9 @@ def load(name):
                 lo=(0, 0), hi=(1, 1), periodic=False)
     d["mesh"] = mesh
     d["equation"] = str(d["equation"])
-    par = d.get("bc_params", np.zeros((len(d["bc_kinds"]), 0)))
-    d["bcs"] = tuple((BC_NAMES[int(k)], tuple(par[i]) if par.shape[1] else ()) for i, k in enumerate(d["bc_kinds"]))
+    par = d.get("bc_params", np.zeros((len(d["bc_kinds"]), 8)))
+    d["bcs"] = tuple((BC_NAMES[int(k)], tuple(par[i][:BC_NPARAMS[int(k)]])) for i, k in enumerate(d["bc_kinds"]))
+    d["numflux"] = str(d["numflux"]) if "numflux" in d else "LF"
     return d
 
 
@@ -29,3 +33,11 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.float64)
     den = np.linalg.norm(b.ravel())
     return np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0)
+
+
+def is_lf(name):
+    """Fixtures with the Lax-Friedrichs flux (the mixed and adjoint forms' flux)."""
+    return load(name)["numflux"] == "LF"
+
+
+LF_NAMES = [n for n in NAMES if is_lf(n)]

@@ -11,13 +11,14 @@ import numpy as np
 import pytest
 
 from apollo_b200 import NodalDG2d, problems
-from golden_cases import NAMES, load
+from golden_cases import LF_NAMES as NAMES, load
 
 pytestmark = pytest.mark.gpu
 
 
 def _fixture_solver(g):
-    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"])
+    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
+                     numerical_flux=g["numflux"])
 
 
 @pytest.mark.parametrize("name", NAMES)

@@ -3,13 +3,14 @@ import numpy as np
 import pytest
 
 from apollo_b200 import ApolloError, NodalDG2d, problems
-from golden_cases import NAMES, load, rel_l2
+from golden_cases import LF_NAMES as NAMES, load, rel_l2
 
 pytestmark = pytest.mark.gpu
 
 
 def _solver(g):
-    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"])
+    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
+                     numerical_flux=g["numflux"])
 
 
 @pytest.mark.parametrize("name", NAMES)

@@ -16,7 +16,8 @@ RHS_TOL_CANCELLING = 1e-11
 
 
 def _solver(g):
-    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"])
+    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
+                     numerical_flux=g["numflux"])
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -167,3 +168,59 @@ def test_negative_density_reports_error():
     with pytest.raises(ApolloError) as e:
         s.step(0.0, 0.0, U)
     assert e.value.code == 3
+
+
+def _channel_solver(g, kind="eulerEqn", fields=5, flux=None):
+    bcs = g["bcs"]
+    return NodalDG2d(int(g["N"]), float(g["cfl"]), kind, g["eqp"][:3], g["mesh"], bcs=bcs,
+                     numerical_flux=flux or g["numflux"])
+
+
+@pytest.mark.parametrize("name", ["euler_hll_N3", "euler_roe_N4", "euler_wave_N2"])
+def test_planar_euler_equals_full_with_new_fluxes_and_bcs(name):
+    """eulerEqn2d equals eulerEqn with rho w = 0 under HLL, Roe and Wave and the
+    wall, inflow, zero-gradient and Dirichlet conditions."""
+    g = load(name)
+    s5 = _channel_solver(g)
+    s4 = _channel_solver(g, "eulerEqn2d")
+    r5, a5 = s5.step(0.2, 0.01, g["U0"])
+    r4, a4 = s4.step(0.2, 0.01, np.ascontiguousarray(g["U0"][..., [0, 1, 2, 4]]))
+    assert np.abs(r5[..., 3]).max() == 0.0
+    assert rel_l2(r4, r5[..., [0, 1, 2, 4]]) <= 1e-14
+    assert a4 == a5
+
+
+def test_unknown_flux_name_is_lax_friedrichs():
+    g = load("euler_hll_N3")
+    lf, _ = _channel_solver(g, flux="LF").step(0.0, 0.0, g["U0"])
+    other, _ = _channel_solver(g, flux="HLLC").step(0.0, 0.0, g["U0"])
+    np.testing.assert_array_equal(other, lf)
+    hll, _ = _channel_solver(g).step(0.0, 0.0, g["U0"])
+    assert rel_l2(hll, lf) > 1e-3
+
+
+def test_non_lf_fluxes_refused_by_mixed_and_adjoint():
+    from apollo_b200 import ApolloError
+    g = load("euler_hll_N3")
+    s = _channel_solver(g)
+    with pytest.raises(ApolloError) as e:
+        s.step(0.0, 0.0, g["U0"], precision="mixed")
+    assert e.value.code == 1
+    with pytest.raises(ApolloError) as e:
+        s.rhs_vjp(0.0, g["U0"], np.ones_like(g["U0"]))
+    assert e.value.code == 1
+
+
+def test_hll_tangent_matches_finite_differences():
+    """The forward-mode derivative runs through the same templated HLL flux."""
+    g = load("euler_hll_N3")
+    s = _channel_solver(g)
+    U = g["U0"]
+    v = np.random.default_rng(5).standard_normal(U.shape)
+    v[..., 3] = 0.0
+    jv = s.rhs_jvp(0.1, U, v)
+    eps = 1e-6
+    rp, _ = s.step(0.1, 0.0, U + eps * v)
+    rm, _ = s.step(0.1, 0.0, U - eps * v)
+    fd = (rp - rm) / (2 * eps)
+    assert rel_l2(jv, fd) <= 1e-6

@@ -116,6 +116,47 @@ def test_rhs_random_states_bitexact(oracle_lib):
         assert sa == sb
 
 
+@pytest.mark.parametrize("flux", ["HLL", "Roe", "Wave", "LF"])
+def test_euler_fluxes_and_bcs_bitexact(oracle_lib, flux):
+    """HLL, Roe and Wave restated in the oracle equal Apollo's compiled
+    fluxes bit for bit through a full RHS of random states, on a walled mesh
+    carrying every Euler boundary condition (wall, inflow, zero gradient,
+    Dirichlet)."""
+    orc = oracle_lib
+    ref = _ref(orc)
+    code = {"LF": orc.NF_LF, "HLL": orc.NF_HLL, "Roe": orc.NF_ROE, "Wave": orc.NF_WAVE}[flux]
+    rng = np.random.default_rng(23)
+    mesh = jittered_square(7, (0, 0), (2, 1), periodic=False, wall_tag=1)
+    # tags 1..4 by side: bottom wall, right outflow, top inflow, left Dirichlet
+    vn = ((0, 1), (1, 2), (2, 0))
+    for f, (i, j) in enumerate(vn):
+        ya, yb = mesh.vy[mesh.etov[:, i]], mesh.vy[mesh.etov[:, j]]
+        xa, xb = mesh.vx[mesh.etov[:, i]], mesh.vx[mesh.etov[:, j]]
+        mesh.face_tag[:, f] = np.select([(ya == 0) & (yb == 0), (xa == 2) & (xb == 2), (ya == 1) & (yb == 1),
+                                         (xa == 0) & (xb == 0)], [1, 2, 3, 4], 0)
+    bcs = ((orc.BC_EULER_WALL, ()), (orc.BC_EULER_ZEROGRAD, ()), (orc.BC_EULER_INFLOW, (0.8, 30.0, 1.4, 1.0, 1.2)),
+           (orc.BC_EULER_DIRICHLET, (0.9, 0.5, -0.2, 0.0, 1.4, 0.8)))
+    h = ref.equation("eulerEqn", gas_gamma=1.4, Numerical_Flux=flux)
+    eqp = (1.4, 0.0, 0.0, code)
+    for trial in range(3):
+        U = rng.uniform(-1, 1, (mesh.K, 10, 5))
+        U[..., 0] = rng.uniform(0.5, 2.0, U.shape[:2])
+        U[..., 3] = 0.0
+        U[..., 4] = 0.5 * (U[..., 1] ** 2 + U[..., 2] ** 2) / U[..., 0] + rng.uniform(1.0, 3.0, U.shape[:2])
+        a = orc.Oracle(mesh, 3, orc.EQ_EULER, eqp, bcs=bcs)
+        b = orc.Oracle(mesh, 3, orc.EQ_EULER, eqp, bcs=bcs)
+        b.use_ref_plugins(ref, h)
+        ra, sa = a.rhs(U, 0.3, 0.01)
+        rb, sb = b.rhs(U, 0.3, 0.01)
+        assert a.error == 0 and b.error == 0
+        np.testing.assert_array_equal(ra, rb)
+        assert sa == sb
+    if flux == "Roe":
+        # Apollo's Roe flux leaves the y-momentum component at zero
+        f, _ = ref.numflux(h, np.array([0.6, 0.8]), U[0, 0], U[1, 0])
+        assert f[2] == 0.0 and f[3] == 0.0
+
+
 @pytest.mark.parametrize("prob,text,fields", [
     ("vortex", """<ic>
  xo = 5.
