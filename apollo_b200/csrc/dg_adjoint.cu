@@ -205,7 +205,21 @@ __global__ void __launch_bounds__(kDThreads) k_tan_face(DgDev d, const double* _
     const double w = d.gw[gq] * sJ;
 #pragma unroll
     for (int f = 0; f < M; ++f) dflux[om + f] = nf[f].d[0] * w;
-    if (fr.k2 >= 0) {
+    if (fr.k2 >= 0 && flux_two_sided<EQ>(d.eqp)) {
+      // the partner's own evaluation (its normal, weight and trace as "-")
+      const ElemGeo& h2 = d.geo[fr.k2];
+#pragma unroll
+      for (int f = 0; f < M; ++f) {
+        qM[f].v = d.trace[op + f];
+        qM[f].d[0] = dtrace[op + f];
+        qP[f].v = d.trace[om + f];
+        qP[f].d[0] = dtrace[om + f];
+      }
+      P::numflux(d.eqp, Dual<1>(h2.nx[fr.f2]), Dual<1>(h2.ny[fr.f2]), qM, qP, nf, &err);
+      const double w2 = d.gw[NG - 1 - gq] * h2.sJ[fr.f2];
+#pragma unroll
+      for (int f = 0; f < M; ++f) dflux[op + f] = nf[f].d[0] * w2;
+    } else if (fr.k2 >= 0) {
 #pragma unroll
       for (int f = 0; f < M; ++f) dflux[op + f] = -(nf[f].d[0] * w);
     }

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
   LamAcc lam_acc;
   // each block takes a contiguous range of face points, so a thread's points
   // stay within one instance of a batched ensemble
+  const bool two_sided = flux_two_sided<EQ>(d.eqp);
   const int total = d.nfaces * NG;
   const int per_block = (total + gridDim.x - 1) / gridDim.x;
   const int i0 = blockIdx.x * per_block, i1 = min(total, i0 + per_block);
@@ -180,9 +181,23 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
 #pragma unroll
     for (int f = 0; f < M; ++f) om[f] = nf[f] * w;
     if (fr.k2 >= 0) {
-      double* op = d.flux + ((size_t)fr.k2 * NF + fr.f2 * NG + (NG - 1 - gq)) * M;
+      const int g2 = NG - 1 - gq;
+      double* op = d.flux + ((size_t)fr.k2 * NF + fr.f2 * NG + g2) * M;
+      if (two_sided) {
+        // the partner's own evaluation: its normal, weight and trace as "-"
+        const ElemGeo& h2 = d.geo[fr.k2];
+        const double* t2 = d.trace + ((size_t)fr.k2 * NF + fr.f2 * NG + g2) * M;
 #pragma unroll
-      for (int f = 0; f < M; ++f) op[f] = -(nf[f] * w);
+        for (int f = 0; f < M; ++f) { qM[f] = t2[f]; qP[f] = tm[f]; }
+        const double lam2 = P::numflux(d.eqp, h2.nx[fr.f2], h2.ny[fr.f2], qM, qP, nf, &err);
+        lam_acc.add(d.st, inst, fabs(lam2));
+        const double w2 = d.gw[g2] * h2.sJ[fr.f2];
+#pragma unroll
+        for (int f = 0; f < M; ++f) op[f] = nf[f] * w2;
+      } else {
+#pragma unroll
+        for (int f = 0; f < M; ++f) op[f] = -(nf[f] * w);
+      }
     }
   }
   lam_acc.flush_warp(d.st);

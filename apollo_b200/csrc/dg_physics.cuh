@@ -428,6 +428,19 @@ template <> struct Eq<EQ_MAXWELL_TM> {
   }
 };
 
+// Whether the face flux is evaluated from each side of an interior face.
+// Apollo computes every element's faces from that element's side; the
+// kernels compute a face once and negate it for the partner where
+// f*(n, a, b) = -f*(-n, b, a), which holds for Lax-Friedrichs and for
+// Apollo's Roe flux but not for its HLL (the truncated bound |S_R| differs
+// between the sides) nor for Wave (traces rotated against an unrotated normal).
+template <int EQ>
+APOLLO_HD bool flux_two_sided(const EqParams& P) {
+  if (EQ != EQ_EULER && EQ != EQ_EULER2D) return false;
+  const int kind = (int)P.p[3];
+  return kind == NF_HLL || kind == NF_WAVE;
+}
+
 // ---------------------------------------------------- boundary conditions ----
 // WxGridFixedBC::applyBC (wxgridfixedbc.cc:17-20): field 0 set to `value`; the
 // other fields (for systems) are copied from the interior trace.
