@@ -163,8 +163,10 @@ def dist_env():
 
 
 # --------------------------------------------------------------- CPU arm ----
-def cpu_sample(n_sample: int = 128, steps: int = 2, threads: int | None = None):
-    """Time the CPU oracle (all host threads) on a bounded sample of the workload."""
+def cpu_sample(n_sample: int = 256, steps: int = 8, threads: int | None = None):
+    """Time the CPU oracle (all host threads) on a bounded sample of the workload: the
+    benchmark mesh itself (256 x 256 vertex grid, K = 130,050) for a few steps (about
+    10 s of CPU work on 16 threads)."""
     from apollo_b200 import problems
     from oracle import oracle as orc
     threads = threads or os.cpu_count() or 1
