@@ -145,6 +145,20 @@ cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStrea
 cudaError_t launch_finalize(const DgDev& d, cudaStream_t s);
 // st[i].lam_bits = 0 for every instance
 cudaError_t launch_reset_lambda(const DgDev& d, cudaStream_t s);
+// Apollo's Euler limiter "eulerLimiterHW" (dg_limiter.cu), orders 2..4: the
+// averaging weights of the nodal basis (half the reference mass matrix's
+// column sums), the face-node mask, and the limiter's own gas_gamma,
+// min_pressure and min_density
+struct LimArgs {
+  double ave[15];
+  int fmask[15];
+  double gamma, minP, minD;
+};
+size_t limiter_work_doubles(int K);
+// limits x into out (may be x), scratch work[limiter_work_doubles(K)]; xn, yn
+// are the node coordinates [K][Np]
+cudaError_t launch_limiter(int eq, const DgDev& d, const LimArgs& L, const double* x, double* out, const double* xn,
+                           const double* yn, double* work, cudaStream_t s);
 // Halo trace blocks (dg_halo.cu): gather (dst[j] = src[idx[j]]) or scatter
 // (dst[idx[j]] = src[j]) of n blocks of block_bytes (a multiple of 16) each
 cudaError_t launch_halo_blocks(const void* src, void* dst, const int* idx, int n, int block_bytes, bool scatter,

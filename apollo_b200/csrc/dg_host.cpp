@@ -78,6 +78,10 @@ struct apollo_dg {
   int *halo_src_d = nullptr, *halo_dst_d = nullptr;
   void *hsend = nullptr, *hrecv = nullptr, *hlam = nullptr;
   size_t hsend_bytes = 0, hrecv_bytes = 0;
+  // Euler limiter (apollo_dg_set_limiter): applied to every stage input
+  bool lim_on = false;
+  LimArgs lim{};
+  double *lim_work_d = nullptr, *xn_d = nullptr, *yn_d = nullptr;
 };
 
 namespace {
@@ -142,6 +146,8 @@ void free_mesh(apollo_dg* h) {
   h->n_send = h->n_recv = 0;
   h->hsend = h->hrecv = h->hlam = nullptr;
   h->hsend_bytes = h->hrecv_bytes = 0;
+  dfree(h->lim_work_d); dfree(h->xn_d); dfree(h->yn_d);
+  h->lim_on = false;
 }
 
 template <class T>
@@ -179,17 +185,28 @@ apollo_status check_ready(apollo_dg* h) {
   return APOLLO_OK;
 }
 
-// the mixed stage's fp32 face flux is the Lax-Friedrichs flux
+// the mixed stage's fp32 face flux is the Lax-Friedrichs flux, and its
+// stage inputs are never limited
 apollo_status check_mixed_flux(apollo_dg* h) {
   if ((h->eq == EQ_EULER || h->eq == EQ_EULER2D) && (int)h->eqp.p[3] != NF_LF)
     return fail(h, APOLLO_ERR_CONFIG, "mixed precision supports the Lax-Friedrichs flux only");
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "mixed precision does not support the limiter");
   return APOLLO_OK;
 }
 
-// the adjoint's face terms are written for the Lax-Friedrichs flux
+// the adjoint's face terms are written for the Lax-Friedrichs flux, and the
+// derivatives do not differentiate the limiter
 apollo_status check_adjoint_flux(apollo_dg* h) {
   if ((h->eq == EQ_EULER || h->eq == EQ_EULER2D) && (int)h->eqp.p[3] != NF_LF)
     return fail(h, APOLLO_ERR_CONFIG, "the adjoint supports the Lax-Friedrichs flux only");
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "the derivatives do not support the limiter");
+  return APOLLO_OK;
+}
+
+// the limiter into out from x (x may be out)
+apollo_status enqueue_limiter(apollo_dg* h, const double* x, double* out) {
+  DgDev d = make_dev(h);
+  CK(launch_limiter(h->eq, d, h->lim, x, out, h->xn_d, h->yn_d, h->lim_work_d, h->stream), "limiter launch");
   return APOLLO_OK;
 }
 
@@ -256,7 +273,14 @@ StageArgs stage_args(const apollo_dg* h, int i) {
 
 apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
   for (int i = 0; i < 5; ++i) {
-    const StageArgs a = stage_args(h, i);
+    StageArgs a = stage_args(h, i);
+    if (h->lim_on) {
+      // PETSc's SSP stepper hands the right-hand side its work vector, which
+      // Apollo's step limits in place: stage 0 limits a copy of U into W
+      apollo_status rl = enqueue_limiter(h, a.x, h->W_d);
+      if (rl) return rl;
+      a.x = h->W_d;
+    }
     apollo_status r = enqueue_stage(h, a, prec);
     if (r != APOLLO_OK) return r;
   }
@@ -410,6 +434,44 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name) {
   // captured graphs hold the equation parameters
   for (auto& g : h->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double* params, int nparams) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (!kind || !*kind) {
+    h->lim_on = false;
+    return APOLLO_OK;
+  }
+  if (std::string(kind) != "eulerLimiterHW") return fail(h, APOLLO_ERR_CONFIG, std::string("unknown limiter ") + kind);
+  if (h->eq != EQ_EULER && h->eq != EQ_EULER2D) return fail(h, APOLLO_ERR_CONFIG, "eulerLimiterHW needs an Euler equation");
+  if (h->ops.N > 4) return fail(h, APOLLO_ERR_CONFIG, "eulerLimiterHW supports orders up to 4");
+  if (nparams != 3 || !params) return fail(h, APOLLO_ERR_ARG, "eulerLimiterHW takes gas_gamma, min_pressure, min_density");
+  if (!h->peers.empty()) return fail(h, APOLLO_ERR_CONFIG, "partitioned meshes do not support the limiter");
+  // Apollo's limiter hands its boundary conditions two coordinates where they
+  // read (t, x, y): only conditions that read none are accepted
+  for (int i = 0; i < h->bcs.n; ++i) {
+    const int k = h->bcs.kind[i];
+    if (k != BC_FIXED && k != BC_EULER_WALL && k != BC_EULER_ZEROGRAD && k != BC_EULER_STATE)
+      return fail(h, APOLLO_ERR_CONFIG, "the limiter supports wall, zero-gradient, inflow, Dirichlet and fixed boundaries");
+  }
+  const RefOps& o = h->ops;
+  LimArgs L{};
+  for (int k = 0; k < o.Np; ++k) L.ave[k] = 0.5 * o.mass_colsum[k];
+  for (int i = 0; i < 3 * (o.N + 1); ++i) L.fmask[i] = o.fmask[i];
+  L.gamma = params[0];
+  L.minP = params[1];
+  L.minD = params[2];
+  if (!h->lim_work_d) {
+    CK(cudaMalloc((void**)&h->lim_work_d, limiter_work_doubles(h->K) * sizeof(double)), "limiter alloc");
+    CK(upload(&h->xn_d, h->xn.data(), h->xn.size()), "limiter coordinates");
+    CK(upload(&h->yn_d, h->yn.data(), h->yn.size()), "limiter coordinates");
+  }
+  h->lim = L;
+  h->lim_on = true;
   return APOLLO_OK;
 }
 
@@ -667,6 +729,12 @@ apollo_status apollo_dg_rhs(apollo_dg* h, double t, double dt, const double* in,
     o = h->out_d;
   }
   CK(cudaMemsetAsync(&h->st_d->err, 0, sizeof(int), h->stream), "rhs");
+  if (h->lim_on) {
+    // the limited input, in the handle's input buffer (the caller's array is unchanged)
+    r = enqueue_limiter(h, x, h->in_d);
+    if (r) return r;
+    x = h->in_d;
+  }
   StageArgs a{};
   a.x = x;
   a.out = o;
@@ -1041,6 +1109,7 @@ const char* apollo_dg_last_error(const apollo_dg* h) { return h ? h->err.c_str()
 apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, double dt, int checkpoint_every) {
   apollo_status r = check_whole(h);
   if (r) return r;
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "the derivatives do not support the limiter");
   if (nsteps < 1 || checkpoint_every < 1 || !(dt > 0.0)) return fail(h, APOLLO_ERR_ARG, "nsteps, checkpoint_every >= 1, dt > 0");
   if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
   r = ensure_deriv_buffers(h);
@@ -1129,6 +1198,7 @@ apollo_status apollo_dg_tangent(apollo_dg* h, int nsteps, double t0, double dt, 
                                 int where) {
   apollo_status r = check_whole(h);
   if (r) return r;
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "the derivatives do not support the limiter");
   if (nsteps < 0 || !(dt > 0.0) || !du0 || !duT) return APOLLO_ERR_ARG;
   if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
   r = ensure_deriv_buffers(h);
@@ -1158,6 +1228,7 @@ apollo_status apollo_dg_tangent(apollo_dg* h, int nsteps, double t0, double dt, 
 apollo_status apollo_dg_rhs_jvp(apollo_dg* h, double t, const double* x, const double* v, double* out, int where) {
   apollo_status r = check_whole(h);
   if (r) return r;
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "the derivatives do not support the limiter");
   if (!x || !v || !out) return APOLLO_ERR_ARG;
   r = ensure_deriv_buffers(h);
   if (r) return r;
@@ -1295,6 +1366,7 @@ apollo_status apollo_dg_dist_start(apollo_dg* h, double t, double dt, apollo_pre
 apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision prec) {
   apollo_status r = check_ready(h);
   if (r) return r;
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "partitioned meshes do not support the limiter");
   if (prec == APOLLO_PREC_MIXED && (r = check_mixed_flux(h))) return r;
   if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
   if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");
@@ -1317,6 +1389,7 @@ apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision pr
 apollo_status apollo_dg_stage_end(apollo_dg* h, int stage, apollo_precision prec) {
   apollo_status r = check_ready(h);
   if (r) return r;
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "partitioned meshes do not support the limiter");
   if (prec == APOLLO_PREC_MIXED && (r = check_mixed_flux(h))) return r;
   if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
   if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");

@@ -71,20 +71,24 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 
+// One poll of an mbarrier phase.  The thread may be suspended until the phase
+// completes or kSuspendNs nanoseconds pass, so a waiting warp issues one poll
+// per interval instead of spinning on the scheduler its working warps share.
+constexpr uint32_t kSuspendNs = 500;
 __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.b32 %0, 1, 0, p;\n\t}\n"
       : "=r"(ok)
-      : "r"(mbar), "r"(parity)
+      : "r"(mbar), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
 
 // Bounded wait on an mbarrier phase: gives up after `limit` polls (each poll
-// may suspend for a hardware-chosen time) and returns false.
+// suspends for at most kSuspendNs: about 2 s in all) and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, uint32_t limit = (1u << 22)) {
   for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(mbar, parity)) return true;

@@ -67,6 +67,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_set_equation": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_add_bc": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_set_numerical_flux": (C.c_int, [H, C.c_char_p]),
+        "apollo_dg_set_limiter": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_set_mesh": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip]),
         "apollo_dg_num_fields": (C.c_int, [H]),
         "apollo_dg_num_nodes": (C.c_int, [H]),
@@ -204,6 +205,13 @@ class NodalDG2d:
             self.close()
         except Exception:
             pass
+
+    def set_limiter(self, kind: str | None, params=()):
+        """Apollo's limiter on every stage input (kind "eulerLimiterHW", params
+        gas_gamma, min_pressure, min_density); None removes it."""
+        p = np.asarray(list(params), dtype=np.float64)
+        self._check(self.lib.apollo_dg_set_limiter(self.h, kind.encode() if kind else None,
+                                                   p.ctypes.data_as(_dp) if len(p) else None, len(p)))
 
     @property
     def shape(self):

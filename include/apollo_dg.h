@@ -78,7 +78,7 @@ apollo_status apollo_dg_create(const apollo_dg_config* cfg, apollo_dg** out);
  * arithmetic when the dropped fields are zero):
  *   "eulerEqn2d"    gas_gamma, minPressure, minDensity   (4 fields: rho, rhou, rhov, E)
  *   "maxwellTM"     c0                             (3 fields: Ez, Bx, By)
- * Numerical flux: Lax-Friedrichs ("Numerical_Flux = LF"). */
+ * Numerical flux: Lax-Friedrichs unless apollo_dg_set_numerical_flux says otherwise. */
 apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const double* params, int nparams);
 
 /* Euler numerical flux by Apollo's "Numerical_Flux" name (WxEulerEqn::setup,
@@ -91,6 +91,21 @@ apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const doubl
  * equations have only LF (the name is ignored).  Mixed precision and the
  * adjoint support LF only (APOLLO_ERR_CONFIG otherwise). */
 apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
+
+/* Limiter applied to every stage input before its right-hand side, as
+ * WxNodalDG2dMethod::step does (src/subsolvers/wxnodaldg2dmethod.cc:243-247,
+ * "Limiter = [...]").  kind "eulerLimiterHW" (WxHestavenWarburtonEulerLimiter,
+ * src/hyperapps/euler/wxhesthavenwarburtoneulerlimiter.cc) with params
+ * gas_gamma, min_pressure, min_density; NULL or "" removes the limiter.  Call
+ * after apollo_dg_set_mesh and the boundary conditions.  Euler kinds, orders
+ * 2..4 (at order 5 Apollo reads past its face-average array); boundary
+ * conditions that read no time or position (wall, zero gradient, inflow,
+ * Dirichlet, fixed), since Apollo's limiter hands them none.  apollo_dg_step
+ * limits each stage's work state (the step's solution is combined unlimited,
+ * as in PETSc's SSP stepper); apollo_dg_rhs limits a copy of its input.
+ * Mixed precision, partitioned meshes and the derivatives refuse it
+ * (APOLLO_ERR_CONFIG). */
+apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double* params, int nparams);
 
 /* Boundary-condition plugin, appended to the list; a face tagged t uses the
  * t-th condition added (Apollo's boundaryConditions[t-1]).  Kinds and params:

@@ -236,6 +236,10 @@ struct Oracle {
   flux_fn ref_flux = nullptr; numflux_fn ref_numflux = nullptr; void* ref_ctx = nullptr;
   int nthreads = 1;
   std::vector<double> area_total; // per-field area integrals of the last RHS
+  // Euler limiter eulerLimiterHW (orc_set_limiter)
+  bool lim_on = false;
+  double lim_gamma = 1.4, lim_minP = 0.0, lim_minD = 0.0;
+  std::vector<double> lim_ave;
 };
 
 // ----------------------------------------------------------- plugins ----
@@ -824,6 +828,232 @@ double orc_init_dt(void* h, const double* u) {
   return 2. / 3. * o.cfl * o.dtscale * (o.rmin / maxSpeed);
 }
 
+// ---- Euler limiter "eulerLimiterHW": WxHestavenWarburtonEulerLimiter::applyLimiter
+// (src/hyperapps/euler/wxhesthavenwarburtoneulerlimiter.cc:44-330), with
+// LimiterElementAVE (wxnodaldggeometry2d.h:84-98) and the limiter's own
+// primitiveVariables (:354-362).  5 Euler fields; orders up to 4 (at order 5
+// the reference reads past its face-average array).
+static void lim_prim(const Oracle& o, const double* qc, double* qp) {
+  qp[0] = qc[0];
+  qp[1] = qc[1] / qc[0];
+  qp[2] = qc[2] / qc[0];
+  qp[3] = qc[3] / qc[0];
+  qp[4] = (o.lim_gamma - 1.) * (qc[4] - 0.5 * (qc[1] * qc[1] + qc[2] * qc[2] + qc[3] * qc[3]) / qc[0]);
+}
+
+static void apply_limiter(Oracle& o, double* u) {
+  const int K = o.K, Np = o.Np, NpF = o.N + 1, meqn = 5;
+  const std::vector<double>& AVE = o.lim_ave;
+  std::vector<double> dropAVE((size_t)Np * Np);
+  {
+    int sk = 0;
+    for (int k = 0; k < Np; ++k)
+      for (int m = 0; m < Np; ++m) dropAVE[sk++] = -AVE[m];
+    for (int m = 0; m < Np; ++m) dropAVE[m * Np + m] += 1.;
+  }
+  // GeometricFactors2d J and Normals2d (nx, ny, len/2) of every element
+  std::vector<double> Jel(K), nrm((size_t)K * 9);
+  for (int k = 0; k < K; ++k) {
+    const double* xk = &o.x[(size_t)k * Np];
+    const double* yk = &o.y[(size_t)k * Np];
+    double x1 = xk[o.fmask[0]], y1 = yk[o.fmask[0]], x2 = xk[o.fmask[NpF]], y2 = yk[o.fmask[NpF]],
+           x3 = xk[o.fmask[2 * NpF]], y3 = yk[o.fmask[2 * NpF]];
+    double dxdr = (x2 - x1) / 2, dxds = (x3 - x1) / 2, dydr = (y2 - y1) / 2, dyds = (y3 - y1) / 2;
+    Jel[k] = -dxds * dydr + dxdr * dyds;
+    double n9[9] = {(y2 - y1), -(x2 - x1), 0, (y3 - y2), -(x3 - x2), 0, (y1 - y3), -(x1 - x3), 0};
+    for (int f = 0; f < 3; ++f) {
+      double sJ = std::sqrt(n9[3 * f] * n9[3 * f] + n9[3 * f + 1] * n9[3 * f + 1]);
+      n9[3 * f] /= sJ; n9[3 * f + 1] /= sJ; n9[3 * f + 2] = sJ / 2.;
+    }
+    for (int i = 0; i < 9; ++i) nrm[(size_t)k * 9 + i] = n9[i];
+  }
+  auto X = [&](int k, int node) { return o.x[(size_t)k * Np + node]; };
+  auto Y = [&](int k, int node) { return o.y[(size_t)k * Np + node]; };
+  auto averages = [&](const double* qIn, double* qCons, double* qPrim) {
+    double c[5] = {0., 0., 0., 0., 0.};
+    for (int n = 0; n < Np; ++n)
+      for (int f = 0; f < 5; ++f) c[f] += AVE[n] * qIn[n * 5 + f];
+    for (int f = 0; f < 5; ++f) qCons[f] = c[f];
+    lim_prim(o, qCons, qPrim);
+  };
+  // the reference hands the boundary conditions two coordinates where they
+  // read (t, x, y); only conditions that read none are accepted with the limiter
+  auto bc = [&](int tag, double xa, double ya, const double* nx, const double* q, double* qb) {
+    double xc[5] = {xa, ya, 0.0, 0.0, 0.0};
+    apply_bc(o, tag, xc, nx, q, qb);
+  };
+  std::vector<double> dVdxE1((size_t)5 * K), dVdyE1((size_t)5 * K), dVdxE2((size_t)5 * K), dVdyE2((size_t)5 * K),
+      dVdxE3((size_t)5 * K), dVdyE3((size_t)5 * K), dVdxC0((size_t)5 * K), dVdyC0((size_t)5 * K);
+  std::vector<double> cellAVEcons((size_t)meqn * K), cellAVEprim((size_t)meqn * K);
+  std::vector<double> QM(3 * NpF * meqn), QP(3 * NpF * meqn), fConsA(3 * NpF * meqn);
+  for (int e = 0; e < K; ++e) {
+    const int* connect = &o.conn[(size_t)e * 6];
+    const double* normals = &nrm[(size_t)e * 9];
+    double xc[4] = {0, 0, 0, 0}, yc[4] = {0, 0, 0, 0}, A0[4] = {0, 0, 0, 0};
+    for (int kk = 0; kk < 3; ++kk) {
+      xc[0] += AVE[kk] * X(e, o.fmask[kk * NpF]);
+      yc[0] += AVE[kk] * Y(e, o.fmask[kk * NpF]);
+      A0[0] += 2. / 3. * AVE[kk] * Jel[e];
+    }
+    for (int face = 0; face < 3; ++face) {
+      if (connect[2 * face] < 0) {
+        double H1 = 2.0 * A0[0] / normals[3 * face + 2];
+        xc[face + 1] = xc[0] + 2.0 * normals[3 * face] * H1;
+        yc[face + 1] = yc[0] + 2.0 * normals[3 * face + 1] * H1;
+      } else {
+        int nb = connect[2 * face];
+        for (int node = 0; node < 3; ++node) {
+          xc[face + 1] += AVE[node] * X(nb, o.fmask[node * NpF]);
+          yc[face + 1] += AVE[node] * Y(nb, o.fmask[node * NpF]);
+          A0[face + 1] += 2. / 3. * AVE[node] * Jel[nb];
+        }
+      }
+    }
+    for (int face = 0; face < 3; ++face) A0[face + 1] += A0[0];
+    double ConsAve[5][4], PrimAve[5][4], qCons[5], qPrim[5], qBC[5];
+    const double* qIn = &u[(size_t)e * Np * meqn];
+    averages(qIn, qCons, qPrim);
+    for (int c = 0; c < meqn; ++c) {
+      ConsAve[c][0] = qCons[c];
+      PrimAve[c][0] = qPrim[c];
+      cellAVEprim[(size_t)e * meqn + c] = qPrim[c];
+      cellAVEcons[(size_t)e * meqn + c] = qCons[c];
+    }
+    for (int edge = 0; edge < 3; ++edge)
+      for (int n = 0; n < NpF; ++n)
+        for (int c = 0; c < meqn; ++c) QM[(edge * NpF + n) * meqn + c] = qIn[o.fmask[edge * NpF + n] * meqn + c];
+    for (int el = 0; el < 3; ++el) {
+      if (connect[2 * el] < 0) {
+        double NX[2] = {normals[3 * el], normals[3 * el + 1]};
+        for (int c = 0; c < meqn; ++c) qCons[c] = ConsAve[c][0];
+        bc(-connect[2 * el], xc[el + 1], yc[el + 1], NX, qCons, qBC);
+        lim_prim(o, qBC, qPrim);
+        for (int c = 0; c < meqn; ++c) {
+          ConsAve[c][el + 1] = qBC[c];
+          PrimAve[c][el + 1] = qPrim[c];
+        }
+        for (int n = 0; n < NpF; ++n) {
+          int node = o.fmask[el * NpF + n];
+          for (int c = 0; c < meqn; ++c) qCons[c] = qIn[node * meqn + c];
+          bc(-connect[2 * el], X(e, node), Y(e, node), NX, qCons, qBC);
+          for (int c = 0; c < meqn; ++c) QP[(el * NpF + n) * meqn + c] = qBC[c];
+        }
+      } else {
+        const double* qn = &u[(size_t)connect[2 * el] * Np * meqn];
+        averages(qn, qCons, qPrim);
+        for (int c = 0; c < meqn; ++c) {
+          ConsAve[c][el + 1] = qCons[c];
+          PrimAve[c][el + 1] = qPrim[c];
+        }
+        int faceNum = connect[2 * el + 1];
+        for (int n = 0; n < NpF; ++n)
+          for (int c = 0; c < meqn; ++c) QP[(el * NpF + n) * meqn + c] = qn[o.fmask[faceNum * NpF + NpF - 1 - n] * meqn + c];
+      }
+    }
+    for (int i = 0; i < 3 * NpF * meqn; ++i) fConsA[i] = 0.5 * (QP[i] + QM[i]);
+    int endIDs[6] = {o.fmask[0], o.fmask[NpF - 1], o.fmask[NpF], o.fmask[2 * NpF - 1], o.fmask[2 * NpF], o.fmask[3 * NpF - 1]};
+    double fPrimA[6 * 5];
+    for (int n = 0; n < 6; ++n) {
+      double rho = fConsA[endIDs[n] * meqn + 0], rhou = fConsA[endIDs[n] * meqn + 1],
+             rhov = fConsA[endIDs[n] * meqn + 2], rhow = fConsA[endIDs[n] * meqn + 3],
+             Ener = fConsA[endIDs[n] * meqn + 4];
+      fPrimA[n * meqn + 0] = rho;
+      fPrimA[n * meqn + 1] = rhou / rho;
+      fPrimA[n * meqn + 2] = rhov / rho;
+      fPrimA[n * meqn + 3] = rhow / rho;
+      fPrimA[n * meqn + 4] = (o.lim_gamma - 1.) * (Ener - 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho);
+    }
+    double xv1 = X(e, endIDs[0]), yv1 = Y(e, endIDs[0]);
+    double xv2 = X(e, endIDs[2]), yv2 = Y(e, endIDs[2]);
+    double xv3 = X(e, endIDs[4]), yv3 = Y(e, endIDs[4]);
+    for (int c = 0; c < meqn; ++c) {
+      size_t i = (size_t)meqn * e + c;
+      dVdxE1[i] = 0.5 * ((PrimAve[c][1] - PrimAve[c][0]) * (yv2 - yv1) + (fPrimA[0 * meqn + c] - fPrimA[1 * meqn + c]) * (yc[1] - yc[0])) / A0[1];
+      dVdyE1[i] = -0.5 * ((PrimAve[c][1] - PrimAve[c][0]) * (xv2 - xv1) + (fPrimA[0 * meqn + c] - fPrimA[1 * meqn + c]) * (xc[1] - xc[0])) / A0[1];
+      dVdxE2[i] = 0.5 * ((PrimAve[c][2] - PrimAve[c][0]) * (yv3 - yv2) + (fPrimA[2 * meqn + c] - fPrimA[3 * meqn + c]) * (yc[2] - yc[0])) / A0[2];
+      dVdyE2[i] = -0.5 * ((PrimAve[c][2] - PrimAve[c][0]) * (xv3 - xv2) + (fPrimA[2 * meqn + c] - fPrimA[3 * meqn + c]) * (xc[2] - xc[0])) / A0[2];
+      dVdxE3[i] = 0.5 * ((PrimAve[c][3] - PrimAve[c][0]) * (yv3 - yv2) + (fPrimA[4 * meqn + c] - fPrimA[5 * meqn + c]) * (yc[3] - yc[0])) / A0[3];
+      dVdyE3[i] = -0.5 * ((PrimAve[c][3] - PrimAve[c][0]) * (xv3 - xv2) + (fPrimA[4 * meqn + c] - fPrimA[5 * meqn + c]) * (xc[3] - xc[0])) / A0[3];
+      dVdxC0[i] = (A0[1] * dVdxE1[i] + A0[2] * dVdxE2[i] + A0[3] * dVdxE3[i]) / (A0[1] + A0[2] + A0[3]);
+      dVdyC0[i] = (A0[1] * dVdyE1[i] + A0[2] * dVdyE2[i] + A0[3] * dVdyE3[i]) / (A0[1] + A0[2] + A0[3]);
+    }
+  }
+  std::vector<double> lim_dx(Np), lim_dy(Np), qdv((size_t)meqn * Np);
+  for (int e = 0; e < K; ++e) {
+    const int* connect = &o.conn[(size_t)e * 6];
+    for (int i = 0; i < Np; ++i) { lim_dx[i] = 0.0; lim_dy[i] = 0.0; }
+    for (int i = 0; i < Np; ++i)
+      for (int j = 0; j < Np; ++j) {
+        lim_dx[i] += dropAVE[i * Np + j] * X(e, j);
+        lim_dy[i] += dropAVE[i * Np + j] * Y(e, j);
+      }
+    for (int c = 0; c < meqn; ++c) {
+      double gx[3], gy[3];
+      for (int edge = 0; edge < 3; ++edge) {
+        size_t i = (size_t)e * meqn + c;
+        if (connect[2 * edge] < 0) {
+          gx[edge] = edge == 0 ? dVdxE1[i] : edge == 1 ? dVdxE2[i] : dVdxE3[i];
+          gy[edge] = edge == 0 ? dVdyE1[i] : edge == 1 ? dVdyE2[i] : dVdyE3[i];
+        } else {
+          size_t a = (size_t)connect[2 * edge] * meqn + c;
+          gx[edge] = dVdxC0[a];
+          gy[edge] = dVdyC0[a];
+        }
+      }
+      double g1 = (gx[0] * gx[0] + gy[0] * gy[0]);
+      double g2 = (gx[1] * gx[1] + gy[1] * gy[1]);
+      double g3 = (gx[2] * gx[2] + gy[2] * gy[2]);
+      double fac = g1 * g1 + g2 * g2 + g3 * g3;
+      double epse = 1.e-14;
+      double fac3e = fac + 3.0 * epse;
+      double w1 = (g2 * g3 + epse) / fac3e, w2 = (g1 * g3 + epse) / fac3e, w3 = (g1 * g2 + epse) / fac3e;
+      double Lx = w1 * gx[0] + w2 * gx[1] + w3 * gx[2];
+      double Ly = w1 * gy[0] + w2 * gy[1] + w3 * gy[2];
+      for (int n = 0; n < Np; ++n) qdv[n * meqn + c] = lim_dx[n] * Lx + lim_dy[n] * Ly;
+    }
+    double* qOut = &u[(size_t)e * Np * meqn];
+    const double* cp = &cellAVEprim[(size_t)e * meqn];
+    const double* cc = &cellAVEcons[(size_t)e * meqn];
+    const double g = o.lim_gamma;
+    for (int n = 0; n < Np; ++n) {
+      double averho = cp[0], aveu = cp[1], avev = cp[2], avew = cp[3], avep = cp[4];
+      double drho = qdv[n * meqn + 0], du = qdv[n * meqn + 1], dv = qdv[n * meqn + 2], dw = qdv[n * meqn + 3],
+             dp = qdv[n * meqn + 4];
+      double Lrho = averho + drho;
+      if (Lrho < o.lim_minD) {
+        for (int r = 0; r < 4; ++r) {
+          drho *= 0.5;
+          Lrho = averho + drho;
+          if (Lrho > o.lim_minD) break;
+          else if (r == 3) Lrho = cc[0];
+        }
+      }
+      double Lrhou = cc[1] + averho * du + drho * aveu;
+      double Lrhov = cc[2] + averho * dv + drho * avev;
+      double Lrhow = cc[3] + averho * dw + drho * avew;
+      double dEner = dp / (g - 1.) + 0.5 * drho * (aveu * aveu + avev * avev + avew * avew) + averho * (aveu * du + avev * dv + avew * dw);
+      double LEner = cc[4] + dEner;
+      double Lp = (g - 1.) * (LEner - 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho);
+      if (Lp < o.lim_minP) {
+        for (int r = 0; r < 4; ++r) {
+          dp *= 0.5;
+          dEner = dp / (g - 1.) + 0.5 * drho * (aveu * aveu + avev * avev + avew * avew) + averho * (aveu * du + avev * dv + avew * dw);
+          LEner = cc[4] + dEner;
+          Lp = (g - 1.) * (LEner - 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho);
+          if (Lp > o.lim_minP) break;
+          else if (r == 3) LEner = avep / (g - 1.) + 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho;
+        }
+      }
+      qOut[n * meqn + 0] = Lrho;
+      qOut[n * meqn + 1] = Lrhou;
+      qOut[n * meqn + 2] = Lrhov;
+      qOut[n * meqn + 3] = Lrhow;
+      qOut[n * meqn + 4] = LEner;
+      if (!std::isfinite(Lrho) || !std::isfinite(LEner)) o.err |= ERR_NAN;
+    }
+  }
+}
+
 // One SSPRK(5,2) step, PETSc TSSSP default "rks2" with 5 stages
 // (TSSSPStep_RK_2): w = u; 4x { w += dt/4 L(w) } at t0 + dt*i/4;
 // u = 4/5 w + dt/5 L(w) + 1/5 u.  Returns the suggested dt of the last stage
@@ -834,17 +1064,42 @@ double orc_ssp_step(void* h, double* u, double t0, double dt) {
   std::vector<double> w(u, u + n), F(n);
   const int s = 5;
   double sugg = 0.0;
+  Oracle& oo = *(Oracle*)h;
   for (int i = 0; i < s - 1; ++i) {
     double st = t0 + dt * (i / (s - 1.));
+    // the limiter rewrites the stage vector the right-hand side receives
+    // (WxNodalDG2dMethod::step, wxnodaldg2dmethod.cc:243-247)
+    if (oo.lim_on) apply_limiter(oo, w.data());
     orc_rhs(h, st, dt, w.data(), F.data());
     double a = dt / (s - 1.);
     for (size_t j = 0; j < n; ++j) w[j] += a * F[j];
   }
+  if (oo.lim_on) apply_limiter(oo, w.data());
   sugg = orc_rhs(h, t0 + dt, dt, w.data(), F.data());
   double al = (s - 1.) / s, be = dt / s, ga = 1. / s;
   for (size_t j = 0; j < n; ++j) u[j] = al * w[j] + be * F[j] + ga * u[j];
   return sugg;
 }
+
+// Enables the Euler limiter (5 fields, N <= 4) with its gas_gamma,
+// min_pressure and min_density; returns 0, or -1 if not applicable.
+int orc_set_limiter(void* h, double gamma, double minP, double minD) {
+  Oracle& o = *(Oracle*)h;
+  if (o.eq != EQ_EULER || o.N > 4) return -1;
+  o.lim_on = true;
+  o.lim_gamma = gamma;
+  o.lim_minP = minP;
+  o.lim_minD = minD;
+  // LimiterElementAVE: half the column sums of the mass matrix inv(V V^T)
+  std::vector<double> Mass = invert(o.VVT, o.Np);
+  o.lim_ave.assign(o.Np, 0.0);
+  for (int k = 0; k < o.Np; ++k)
+    for (int m = 0; m < o.Np; ++m) o.lim_ave[k] += 0.5 * Mass[k + m * o.Np];
+  return 0;
+}
+
+// The limiter applied in place to a state u [K][Np][5].
+void orc_limit(void* h, double* u) { apply_limiter(*(Oracle*)h, u); }
 
 // Run nsteps steps (stopping early at tend) with Apollo's dt policy: the
 // step's dt is min(current dt, the last stage's suggestion) for the next

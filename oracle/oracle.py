@@ -67,6 +67,10 @@ def _lib():
     lib.orc_ssp_step.restype = C.c_double
     lib.orc_run.argtypes = [C.c_void_p, _dp, C.c_int, _dp, _dp, C.c_double]
     lib.orc_run.restype = C.c_int
+    lib.orc_set_limiter.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+    lib.orc_set_limiter.restype = C.c_int
+    lib.orc_limit.argtypes = [C.c_void_p, _dp]
+    lib.orc_limit.restype = None
     return lib
 
 
@@ -156,6 +160,17 @@ class Oracle:
     def ssp_step(self, u, t0: float, dt: float) -> float:
         assert u.flags.c_contiguous and u.dtype == np.float64
         return self.lib.orc_ssp_step(self.h, _p(u), t0, dt)
+
+    def set_limiter(self, gamma: float, min_pressure: float, min_density: float) -> None:
+        """Apollo's eulerLimiterHW on every stage input (5 fields, N <= 4)."""
+        if self.lib.orc_set_limiter(self.h, gamma, min_pressure, min_density) != 0:
+            raise ValueError("the limiter needs eulerEqn at order <= 4")
+
+    def limit(self, u):
+        """The limiter applied to a copy of u."""
+        v = np.array(u, dtype=np.float64, order="C", copy=True)
+        self.lib.orc_limit(self.h, _p(v))
+        return v
 
     def run(self, u, nsteps: int, t: float, dt: float, tend: float = -1.0):
         """Advance u in place; returns (steps taken, t, dt for the next step)."""

@@ -83,7 +83,12 @@ CASES = [
      dict(gas_gamma=1.4, Numerical_Flux="Roe"), CHANNEL_BCS, 0),  # Apollo's Roe flux is non-physical within a step
     ("euler_wave_N2", channel, dict(N=2, n=8), orc.EQ_EULER, (1.4, 0.0, 0.0, orc.NF_WAVE), "eulerEqn",
      dict(gas_gamma=1.4, Numerical_Flux="Wave"), CHANNEL_BCS, 1),  # non-physical from the second step
+    ("euler_hll_limiter_N3", channel, dict(N=3, n=9, seed=4), orc.EQ_EULER, (1.4, 0.0, 0.0, orc.NF_HLL), "eulerEqn",
+     dict(gas_gamma=1.4, Numerical_Flux="HLL"), CHANNEL_BCS, 4),
 ]
+
+# the eulerLimiterHW parameters (gas_gamma, min_pressure, min_density) per case
+LIMITERS = {"euler_hll_limiter_N3": (1.4, 1e-6, 1e-6)}
 
 FLUX_NAMES = {orc.NF_LF: "LF", orc.NF_HLL: "HLL", orc.NF_ROE: "Roe", orc.NF_WAVE: "Wave"}
 
@@ -96,7 +101,16 @@ def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref)
     o.use_ref_plugins(ref, eh)
     x, y = o.node_coords()
     U0 = np.ascontiguousarray(prob.ic(x, y), dtype=np.float64)
-    rhs, sugg = o.rhs(U0, 0.0, 0.0)
+    lim = LIMITERS.get(name)
+    extra = {}
+    if lim is not None:
+        # the limiter (restated in the oracle; Apollo's needs PETSc's DMPlex)
+        # acts on every stage input, and on the input of a single right-hand side
+        o.set_limiter(*lim)
+        extra["limiter"] = np.asarray(lim, dtype=np.float64)
+        rhs, sugg = o.rhs(o.limit(U0), 0.0, 0.0)
+    else:
+        rhs, sugg = o.rhs(U0, 0.0, 0.0)
     dt0 = o.init_dt(U0)
     U = U0.copy()
     n, t, dt = o.run(U, steps, 0.0, dt0)
@@ -109,7 +123,7 @@ def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref)
         bc_kinds=np.asarray([b[0] for b in bcs], dtype=np.int32),
         bc_params=np.asarray([list(b[1]) + [0.0] * (8 - len(b[1])) for b in bcs], dtype=np.float64).reshape(-1, 8),
         x=x, y=y, U0=U0, rhs=rhs, sugg=sugg, dt0=dt0,
-        steps=steps, U_end=U, t_end=t, dt_end=dt)
+        steps=steps, U_end=U, t_end=t, dt_end=dt, **extra)
     return name, U0.shape, float(np.abs(rhs).max())
 
 

@@ -16,8 +16,11 @@ RHS_TOL_CANCELLING = 1e-11
 
 
 def _solver(g):
-    return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
-                     numerical_flux=g["numflux"])
+    s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
+                  numerical_flux=g["numflux"])
+    if "limiter" in g:
+        s.set_limiter("eulerLimiterHW", g["limiter"])
+    return s
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -224,3 +227,27 @@ def test_hll_tangent_matches_finite_differences():
     rm, _ = s.step(0.1, 0.0, U - eps * v)
     fd = (rp - rm) / (2 * eps)
     assert rel_l2(jv, fd) <= 1e-6
+
+
+def test_limiter_refusals_and_removal():
+    """The limiter is refused where it is not supported, and removing it
+    restores the plain right-hand side."""
+    from apollo_b200 import ApolloError
+    g = load("euler_hll_limiter_N3")
+    s = _solver(g)
+    with pytest.raises(ApolloError) as e:
+        s.step(0.0, 0.0, g["U0"], precision="mixed")
+    assert e.value.code == 1
+    with pytest.raises(ApolloError):
+        s.rhs_jvp(0.0, g["U0"], g["U0"])
+    lim, _ = s.step(0.0, 0.0, g["U0"])
+    s.set_limiter(None)
+    plain, _ = s.step(0.0, 0.0, g["U0"])
+    ref, _ = _channel_solver(g).step(0.0, 0.0, g["U0"])
+    np.testing.assert_array_equal(plain, ref)
+    assert rel_l2(lim, plain) > 1e-3
+    # the vortex boundary condition reads (t, x, y), which the limiter cannot give it
+    v = load("euler_gmsh_N3")
+    sv = NodalDG2d(int(v["N"]), float(v["cfl"]), v["equation"], v["eqp"][:3], v["mesh"], bcs=v["bcs"])
+    with pytest.raises(ApolloError):
+        sv.set_limiter("eulerLimiterHW", (1.4, 1e-6, 1e-6))
