@@ -437,6 +437,12 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name) {
   return APOLLO_OK;
 }
 
+apollo_status apollo_dg_averaging_weights(const apollo_dg* h, double* w) {
+  if (!h || !w || h->ops.Np == 0) return APOLLO_ERR_ARG;
+  for (int k = 0; k < h->ops.Np; ++k) w[k] = 0.5 * h->ops.mass_colsum[k];
+  return APOLLO_OK;
+}
+
 apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double* params, int nparams) {
   apollo_status r = check_ready(h);
   if (r) return r;

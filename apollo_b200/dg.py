@@ -68,6 +68,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_add_bc": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_set_numerical_flux": (C.c_int, [H, C.c_char_p]),
         "apollo_dg_set_limiter": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
+        "apollo_dg_averaging_weights": (C.c_int, [H, _dp]),
         "apollo_dg_set_mesh": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip]),
         "apollo_dg_num_fields": (C.c_int, [H]),
         "apollo_dg_num_nodes": (C.c_int, [H]),
@@ -205,6 +206,17 @@ class NodalDG2d:
             self.close()
         except Exception:
             pass
+
+    def averaging_weights(self):
+        """w[Np]: an element's average of a nodal field is sum_n w[n] u[n]."""
+        w = np.empty(self.Np)
+        self._check(self.lib.apollo_dg_averaging_weights(self.h, w.ctypes.data_as(_dp)))
+        return w
+
+    def write_vtu(self, path: str, U=None, time: float | None = None):
+        """The resident state (or U) as a VTK file (apollo_b200.vtk.write_vtu)."""
+        from .vtk import write_vtu
+        write_vtu(path, self.mesh, self.get_state() if U is None else U, averages=self.averaging_weights(), time=time)
 
     def set_limiter(self, kind: str | None, params=()):
         """Apollo's limiter on every stage input (kind "eulerLimiterHW", params

@@ -107,6 +107,11 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
  * (APOLLO_ERR_CONFIG). */
 apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double* params, int nparams);
 
+/* The element average of a nodal field is sum_n w[n] u[n]: w[Np] receives the
+ * weights (half the column sums of the reference mass matrix, Apollo's
+ * LimiterElementAVE, src/lib/wxnodaldggeometry2d.h:84-98). */
+apollo_status apollo_dg_averaging_weights(const apollo_dg* h, double* w);
+
 /* Boundary-condition plugin, appended to the list; a face tagged t uses the
  * t-th condition added (Apollo's boundaryConditions[t-1]).  Kinds and params:
  *   "gridFixedBC"                   value

@@ -251,3 +251,23 @@ def test_limiter_refusals_and_removal():
     sv = NodalDG2d(int(v["N"]), float(v["cfl"]), v["equation"], v["eqp"][:3], v["mesh"], bcs=v["bcs"])
     with pytest.raises(ApolloError):
         sv.set_limiter("eulerLimiterHW", (1.4, 1e-6, 1e-6))
+
+
+def test_averaging_weights_and_vtu(tmp_path):
+    """The averaging weights sum to one and average a linear field to its
+    centroid value; the handle writes its state as a VTK frame."""
+    from apollo_b200.vtk import read_vtu
+    g = load(NAMES[0])
+    s = _solver(g)
+    w = s.averaging_weights()
+    assert abs(w.sum() - 1.0) < 1e-14
+    x, y = s.node_coords()
+    lin = 2.0 * x - 3.0 * y + 1.0
+    verts = g["mesh"].etov
+    cx = g["mesh"].vx[verts].mean(axis=1)
+    cy = g["mesh"].vy[verts].mean(axis=1)
+    np.testing.assert_allclose(lin @ w, 2.0 * cx - 3.0 * cy + 1.0, rtol=0, atol=1e-12)
+    s.set_state(g["U0"])
+    s.write_vtu(str(tmp_path / "s.vtu"), time=0.0)
+    a = read_vtu(str(tmp_path / "s.vtu"))
+    np.testing.assert_array_equal(a["solution"], g["U0"].reshape(g["U0"].shape[0], -1))
