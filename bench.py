@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--replicas", action="store_true",
                     help="N>1: independent replicas instead of one partitioned mesh")
+    ap.add_argument("--partitioned", action="store_true",
+                    help="run the partitioned (multi-GPU) arm even at N=1 (one part, no peers)")
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--adjoint-dirs", type=int, default=32,
                     help="random directions of the adjoint's finite-difference check")
@@ -502,7 +504,7 @@ def ours_arm(args):
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    if world > 1 and not args.replicas:
+    if (world > 1 and not args.replicas) or args.partitioned:
         return partitioned_arm(args, rank, world, local)
     dist = None
     if world > 1:
