@@ -702,6 +702,9 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       // element is wtid % E in every chunk (the rotation moves whole warps), so
       // its per-element volume constants stay in registers.
       constexpr bool ECONST = 32 % E == 0;
+      // ... and since the worker count is a multiple of E as well, the item
+      // loops can step over a worker's own element only
+      constexpr bool FIXED_E = ECONST && NW % E == 0 && (M == 4 || M == 8);
       const int e_me = wtid % E;
       float kQF[M], kG[4], kP[2 * M];
       if constexpr (ECONST) {
@@ -723,7 +726,45 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         if (cc >= NBUF && !umma::mbar_wait_bounded(mb_empty(b), ((cc / NBUF) - 1) & 1)) *abort_flag = 1;
         unsigned char* bh = RING + b * 2 * C::SZ_CH;
         unsigned char* bl = bh + C::SZ_CH;
-        if (ch < NV) {
+        if (ch < NV && FIXED_E) {
+          // volume, each worker on its own element e_me (see FIXED_E): the
+          // element's row block and the operand offsets are set up once
+          const int npts = min(VPC, NC - ch * VPC);
+          const int nfill = 4 * ((npts + 3) / 4);
+          if (e_me < ne) {
+            const int rowb = rowb_of(e_me);
+            const uint32_t obase = umma::kmajor_offset_sbo(rowb, 0, C::SBOC);
+            const float* stb = ST + rowb;
+            for (int cp = wid / E; cp < nfill; cp += NW / E) {
+              float R[M], S[M];
+              if (cp < npts) {
+                float qc[M];
+                load_fields<M>(stb + (ch * VPC + cp) * 128, qc);
+#pragma unroll
+                for (int f = 0; f < M; ++f) qc[f] += kQF[f];
+                Q::dirflux(d.eqp, qc, kG[0], kG[1], kG[2], kG[3], R, S, &err);
+#pragma unroll
+                for (int f = 0; f < M; ++f) {
+                  R[f] -= kP[f];
+                  S[f] -= kP[M + f];
+                }
+              } else {
+#pragma unroll
+                for (int f = 0; f < M; ++f) { R[f] = 0.f; S[f] = 0.f; }
+              }
+              // rows rowb + f share one 8-row group: offsets step by 16 bytes
+              const uint32_t oc = obase + ((2 * cp) >> 2) * umma::kLBO + ((2 * cp) & 3) * 4;
+#pragma unroll
+              for (int f = 0; f < M; ++f) {
+                float h0, l0, h1, l1;
+                split_tf32(R[f], h0, l0);
+                split_tf32(S[f], h1, l1);
+                *(float2*)(bh + oc + 16 * f) = make_float2(h0, h1);
+                *(float2*)(bl + oc + 16 * f) = make_float2(l0, l1);
+              }
+            }
+          }
+        } else if (ch < NV) {
           // volume: deviation of the fp32 flux from the flux of the mean, times the metric
           const int npts = min(VPC, NC - ch * VPC);
           const int nfill = 4 * ((npts + 3) / 4);
@@ -778,9 +819,11 @@ __global__ void __launch_bounds__(kMixThreads, 1)
           }
           const int col0 = (ch - NV) * KV;
           const int ncol = min(KV, C::NFK - col0);
-          for (int it = wid; it < ncol * E; it += NW) {
-            const int e = it % E, cl = it / E, col = col0 + cl;
-            if (e >= ne) continue;
+          // with FIXED_E every iteration of a worker has e = e_me
+          const int it0 = FIXED_E ? (e_me < ne ? (wid / E) * E + e_me : ncol * E) : wid;
+          for (int it = it0; it < ncol * E; it += NW) {
+            const int e = FIXED_E ? e_me : it % E, cl = it / E, col = col0 + cl;
+            if (!FIXED_E && e >= ne) continue;
             const int rowb = rowb_of(e), k = k0 + e;
             float dev[M];
             if (col < NF) {
@@ -812,11 +855,13 @@ __global__ void __launch_bounds__(kMixThreads, 1)
 #pragma unroll
               for (int f = 0; f < M; ++f) dev[f] = 0.f;
             }
+            const uint32_t oc = umma::kmajor_offset_sbo(rowb, cl, C::SBOC);
 #pragma unroll
             for (int f = 0; f < M; ++f) {
               float h, l;
               split_tf32(dev[f], h, l);
-              const uint32_t off = umma::kmajor_offset_sbo(rowb + f, cl, C::SBOC);
+              // rows rowb + f share one 8-row group (rowb is a multiple of M, M | 8)
+              const uint32_t off = (M == 4 || M == 8) ? oc + 16 * f : umma::kmajor_offset_sbo(rowb + f, cl, C::SBOC);
               *(float*)(bh + off) = h;
               *(float*)(bl + off) = l;
             }
