@@ -32,6 +32,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "DOF-updates/s"
 WORKLOAD = "euler_vortex_N4_K130050"
+
+
+def workload_name(N: int, K: int) -> str:
+    return f"euler_vortex_N{N}_K{K}"
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -43,6 +47,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--n", type=int, default=256, help="vertex grid size (256: K = 130,050)")
+    ap.add_argument("--order", type=int, default=4, help="polynomial order N of the vortex workload (2..5)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-l2-500", action="store_true", help="skip the 500-step mixed vs float64 comparison")
@@ -64,7 +69,7 @@ def rhs_only(args):
     """Set up the benchmark workload and evaluate the RHS a few times (for ncu)."""
     import torch
     from apollo_b200 import NodalDG2d, problems
-    p = problems.euler_vortex(n=args.n, fields=4)
+    p = problems.euler_vortex(n=args.n, N=args.order, fields=4)
     s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=0)
     x, y = s.node_coords()
     u = torch.from_numpy(np.ascontiguousarray(p.ic(x, y))).cuda()
@@ -514,7 +519,7 @@ def ours_arm(args):
         dist = dist_mod
     from apollo_b200 import NodalDG2d, problems
 
-    p = problems.euler_vortex(n=args.n, fields=4)
+    p = problems.euler_vortex(n=args.n, N=args.order, fields=4)
     stream = torch.cuda.Stream()
     s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=local, stream=stream.cuda_stream)
     x, y = s.node_coords()
@@ -613,7 +618,7 @@ def ours_arm(args):
     dom = int(np.argmax(kt))
     dname = names[dom]
     achieved = alg_bytes[dname] / (kt[dom] / 1000.0) / 1e9
-    traffic = profile_traffic().get(f"{prec}:{dname}:{WORKLOAD}")
+    traffic = profile_traffic().get(f"{prec}:{dname}:{workload_name(p.N, s.K)}")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": dname,
                 "peak_source": f"{peak_src} hbm_gbs",
@@ -683,7 +688,8 @@ def ours_arm(args):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "mixed(tf32x3 tensor, fp32 acc, f64 state)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "K": s.K, "N": N, "Np": Np, "fields": M, "flux": "LF", "cfl": p.cfl,
+            "config": {"workload": workload_name(p.N, s.K), "K": s.K, "N": N, "Np": Np, "fields": M, "flux": "LF",
+                       "cfl": p.cfl,
                        "precision": prec, "l2_flush": "inputs larger than L2 (state + stage + scratch "
                        f"{(dofs * 8 * 4 + 2 * K * Nf * M * 8) / 2**20:.0f} MiB > 126 MiB)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
