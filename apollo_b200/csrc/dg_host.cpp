@@ -1014,6 +1014,8 @@ void handle_set_error(apollo_dg* h, const char* msg) {
   if (h) h->err = msg;
 }
 
+bool handle_has_limiter(const apollo_dg* h) { return h && h->lim_on; }
+
 // ---- batched ensembles (dg_batch.cpp): one handle holds several independent
 // meshes of one order, element ranges by instance
 apollo_status handle_set_instances(apollo_dg* h, int ninst, const int* einst) {

@@ -20,6 +20,7 @@ namespace apollo {
 // Reads the discretisation of a handle (dg_host.cpp).
 bool handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size_t* nU, size_t* nT);
 void handle_set_error(apollo_dg* h, const char* msg);
+bool handle_has_limiter(const apollo_dg* h);
 
 }  // namespace apollo
 
@@ -64,6 +65,11 @@ extern "C" apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt
   DgDev d;
   int eq = 0, device = 0;
   size_t nU = 0, nT = 0;
+  if (handle_has_limiter(h)) {
+    // the limiter needs scratch of its own; apollo_dg_rhs applies it
+    handle_set_error(h, "apollo_dg_rhs_noalloc: the handle has a limiter; use apollo_dg_rhs");
+    return APOLLO_ERR_STATE;
+  }
   if (!handle_device_view(h, &d, &eq, &device, &nU, &nT)) return APOLLO_ERR_STATE;
   const size_t need = kHeader + align256(nU * sizeof(double)) + 2 * align256(nT * sizeof(double));
   if (need > kScratchBytes) {

@@ -202,7 +202,9 @@ apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int it
  * APOLLO_ERR_ARG.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress); make that first call before any stream
  * capture.  All calls share the one array: calls that overlap on the GPU, on
- * any handle or stream of the same device, race. */
+ * any handle or stream of the same device, race.  Handles with a limiter
+ * (apollo_dg_set_limiter) or a partitioned mesh with peers are refused
+ * (APOLLO_ERR_STATE). */
 apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt, const double* in, double* out,
                                     double* suggested_dt, void* stream);
 

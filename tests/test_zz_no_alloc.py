@@ -30,8 +30,15 @@ def _noalloc(s, t, dt, u, out, stream):
 def test_noalloc_matches_rhs_twice(name):
     torch = pytest.importorskip("torch")
     g = load(name)
-    s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"])
+    s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
+                  numerical_flux=g["numflux"])
     u = torch.from_numpy(g["U0"]).cuda()
+    if "limiter" in g:
+        # the limiter needs scratch of its own: such handles are refused
+        s.set_limiter("eulerLimiterHW", g["limiter"])
+        rc, _ = _noalloc(s, 0.25, 1e-3, u, torch.empty_like(u), torch.cuda.current_stream().cuda_stream)
+        assert rc == 7
+        return
     ref = torch.empty_like(u)
     _, sugg_ref = s.step(0.25, 1e-3, u, ref)
     stream = torch.cuda.current_stream().cuda_stream
