@@ -35,6 +35,7 @@ apollo_status handle_enqueue_step_raw(apollo_dg* h, apollo_precision prec);
 apollo_status handle_prepare_step(apollo_dg* h, apollo_precision prec);
 apollo_status handle_read_errors(apollo_dg* h);
 void handle_set_grid_div(apollo_dg* h, int div);
+void handle_set_tile_shape(apollo_dg* h, int shape);
 }  // namespace apollo
 
 using namespace apollo;
@@ -56,6 +57,7 @@ struct apollo_dg_batch {
     apollo_dg* h = nullptr;
     std::vector<int> insts;  // batch instance ids, in element order
     int div = 1;             // persistent-grid share picked by the autotuner
+    int shape = 0;           // mixed stage operand chunking picked by the autotuner
   };
   std::vector<Group> groups;
   struct Inst {
@@ -386,7 +388,7 @@ apollo_status apollo_dg_batch_step(apollo_dg_batch* b, int nsteps, double* t, do
   return APOLLO_OK;
 }
 
-apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec, int* choice) {
+apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec, int* share, int* shape) {
   if (!b || !b->finalized) return APOLLO_ERR_ARG;
   // keep the states: every trial starts from them
   const size_t ni = b->inst.size();
@@ -439,25 +441,32 @@ apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec
     BCK(cudaEventElapsedTime(ms, e0, e1), "autotune");
     return APOLLO_OK;
   };
-  // coordinate descent over the groups' persistent-grid shares
-  const int cands[3] = {1, 2, 4};
+  // coordinate descent over the groups' launch shapes: the persistent-grid
+  // share and, in mixed precision, the operand chunking of the stage kernel
+  const int divs[3] = {1, 2, 4};
+  const int nshape = prec == APOLLO_PREC_MIXED ? 2 : 1;
   apollo_status r = APOLLO_OK;
   for (size_t gi = 0; gi < b->groups.size() && !r; ++gi) {
     float best = 1e30f;
-    int best_div = b->groups[gi].div;
-    for (int c : cands) {
-      handle_set_grid_div(b->groups[gi].h, c);
-      drop_graphs(b);
-      float ms = 0.f;
-      r = trial(&ms);
-      if (r) break;
-      if (ms < best) {
-        best = ms;
-        best_div = c;
+    int best_div = b->groups[gi].div, best_shape = b->groups[gi].shape;
+    for (int sh = 0; sh < nshape && !r; ++sh)
+      for (int c : divs) {
+        handle_set_grid_div(b->groups[gi].h, c);
+        handle_set_tile_shape(b->groups[gi].h, sh);
+        drop_graphs(b);
+        float ms = 0.f;
+        r = trial(&ms);
+        if (r) break;
+        if (ms < best) {
+          best = ms;
+          best_div = c;
+          best_shape = sh;
+        }
       }
-    }
     b->groups[gi].div = best_div;
+    b->groups[gi].shape = best_shape;
     handle_set_grid_div(b->groups[gi].h, best_div);
+    handle_set_tile_shape(b->groups[gi].h, best_shape);
     drop_graphs(b);
   }
   // restore the states
@@ -473,9 +482,13 @@ apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (choice) {
-    for (int i = 0; i < 4; ++i) choice[i] = 0;
-    for (auto& G : b->groups) choice[G.N - 2] = G.div;
+  for (int i = 0; i < 4; ++i) {
+    if (share) share[i] = 0;
+    if (shape) shape[i] = -1;
+  }
+  for (auto& G : b->groups) {
+    if (share) share[G.N - 2] = G.div;
+    if (shape) shape[G.N - 2] = G.shape;
   }
   return r;
 }

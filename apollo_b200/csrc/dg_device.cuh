@@ -54,7 +54,8 @@ struct DgDev {
   // word of st[0] serves them all)
   const int* einst;
   int ninst;
-  int grid_div;  // launch shape: persistent grids use SMs / grid_div (>= 1; 0 means 1)
+  int grid_div;    // launch shape: persistent grids use SMs / grid_div (>= 1; 0 means 1)
+  int tile_shape;  // mixed stage operand chunking (0 or 1), picked by the batch autotuner
   const double *V, *Dr, *Ds, *I, *L, *gz, *gw;
   double *vol, *trace, *flux;  // scratch: [K][NP][M], [K][NF][M], [K][NF][M]
   DevState* st;

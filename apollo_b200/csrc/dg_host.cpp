@@ -43,7 +43,8 @@ struct apollo_dg {
   // st_h then hold one DevState per instance)
   int* einst_d = nullptr;
   int ninst = 1;
-  int grid_div = 1;  // launch shape picked by the batch autotuner
+  int grid_div = 1;    // launch shape picked by the batch autotuner
+  int tile_shape = 0;  // mixed stage operand chunking picked by the batch autotuner
   double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
          *gw_d = nullptr, *wmass_d = nullptr;
   double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
@@ -83,6 +84,12 @@ struct apollo_dg {
   LimArgs lim{};
   double *lim_work_d = nullptr, *xn_d = nullptr, *yn_d = nullptr;
 };
+
+namespace apollo {
+// launch and tile shapes (defined with the batch helpers below)
+void handle_set_grid_div(apollo_dg* h, int div);
+void handle_set_tile_shape(apollo_dg* h, int shape);
+}  // namespace apollo
 
 namespace {
 
@@ -171,6 +178,7 @@ DgDev make_dev(const apollo_dg* h) {
   d.einst = h->einst_d;
   d.ninst = h->ninst;
   d.grid_div = h->grid_div;
+  d.tile_shape = h->tile_shape;
   d.eqp = h->eqp;
   d.bcs = h->bcs;
   d.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
@@ -434,6 +442,13 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name) {
   // captured graphs hold the equation parameters
   for (auto& g : h->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_set_launch_shape(apollo_dg* h, int grid_share, int tile_shape) {
+  if (!h || grid_share < 1 || tile_shape < 0 || tile_shape > 1) return APOLLO_ERR_ARG;
+  handle_set_grid_div(h, grid_share);
+  handle_set_tile_shape(h, tile_shape);
   return APOLLO_OK;
 }
 
@@ -1099,6 +1114,14 @@ apollo_status handle_prepare_step(apollo_dg* h, apollo_precision prec) {
   return APOLLO_OK;
 }
 apollo_status handle_read_errors(apollo_dg* h) { return read_errors(h); }
+void handle_set_tile_shape(apollo_dg* h, int shape) {
+  shape = shape == 1 ? 1 : 0;
+  if (shape != h->tile_shape) {
+    h->tile_shape = shape;
+    for (auto& g : h->graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
+}
 void handle_set_grid_div(apollo_dg* h, int div) {
   if (div < 1) div = 1;
   if (div != h->grid_div) {

@@ -46,13 +46,18 @@ constexpr int tmem_cols(int x) { return x <= 32 ? 32 : x <= 64 ? 64 : x <= 128 ?
 // padded to 16 bytes so that every block can be moved by a bulk copy
 constexpr int trace_stride(int NG, int M) { return round_up_c(NG * M, 4); }
 
-template <int N, int M> struct MixCfg {
+// SH selects the operand chunking: 0 = chunks of 24 K columns (16 at N = 5)
+// through a two-buffer ring, 1 = chunks of 16 through a three-buffer ring.
+// Both issue the same MMAs in the same K order (chunks start on 8-column
+// boundaries), so they compute the same result bit for bit; the batch
+// autotuner picks the faster per order.
+template <int N, int M, int SH = 0> struct MixCfg {
   static constexpr int NP = Sizes<N>::NP, NC = Sizes<N>::NC, NG = Sizes<N>::NG, NF = Sizes<N>::NF;
   static constexpr int EPQ = 32 / M;  // elements per warp quadrant
   static constexpr int E = 4 * EPQ;   // elements per tile
   static constexpr int K1 = round_up_c(NP, 8);
   static constexpr int GA = K1 / 4 <= 2 ? 2 : K1 / 4 <= 4 ? 4 : 8;  // lanes per row in the operand build
-  static constexpr int KV = N >= 5 ? 16 : 24;         // K columns per chunk
+  static constexpr int KV = (SH == 1 || N >= 5) ? 16 : 24;  // K columns per chunk
   static constexpr int VPC = KV / 2;                  // cubature points per volume chunk (R, S each)
   static constexpr int NV = (NC + VPC - 1) / VPC;     // volume chunks
   static constexpr int NFK = round_up_c(NF, 8);       // face columns (fc NG + g, packed)
@@ -61,7 +66,7 @@ template <int N, int M> struct MixCfg {
   static constexpr int NC16 = round_up_c(NC, 16);
   static constexpr int NPN = round_up_c(NP, 16);
   static constexpr int KB2 = NCH * KV;
-  static constexpr int NBUF = 2;
+  static constexpr int NBUF = SH == 1 ? 3 : 2;
   static constexpr int NWORK = kMixThreads - 32;      // worker threads; the last warp issues MMAs and copies
   static constexpr int TS = trace_stride(NG, M);      // floats per (element, face) trace block
   static constexpr int IFS = round_up_c(NP, 4);       // padded row of the interpolation operator
@@ -317,13 +322,13 @@ __device__ __forceinline__ void cp_async_arrive(uint32_t mbar) {
 // ring (full/empty mbarriers), and finish with the float64 epilogue and the
 // result's face traces.  The next tile's operand build and GEMM-A overlap
 // this tile's epilogue; per-tile data live in two slots by tile parity.
-template <int EQ, int N>
+template <int EQ, int N, int SH>
 __global__ void __launch_bounds__(kMixThreads, 1)
     k_mixed_stage(DgDev d, StageArgs a, const double* __restrict__ rowsum, int flags) {
   using P = Eq<EQ>;
   using Q = MixPhys<EQ>;
   constexpr int M = P::M;
-  using C = MixCfg<N, M>;
+  using C = MixCfg<N, M, SH>;
   constexpr int NP = C::NP, NC = C::NC, NG = C::NG, NF = C::NF, EPQ = C::EPQ, E = C::E, K1 = C::K1;
   constexpr int KV = C::KV, VPC = C::VPC, NV = C::NV, NW = C::NWORK, NBUF = C::NBUF, TS = C::TS;
   constexpr int IFS = C::IFS, GA = C::GA;
@@ -1046,9 +1051,9 @@ cudaError_t launch_traces_t(const DgDev& d, const double* x, float* T, cudaStrea
   return cudaGetLastError();
 }
 
-template <int EQ, int N>
-cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a0, cudaStream_t s, cudaEvent_t* ev) {
-  using C = MixCfg<N, Eq<EQ>::M>;
+template <int EQ, int N, int SH>
+cudaError_t launch_mixed_sh(MixedPlan* p, const DgDev& d, const StageArgs& a0, cudaStream_t s, cudaEvent_t* ev) {
+  using C = MixCfg<N, Eq<EQ>::M, SH>;
   if constexpr (!C::FITS) {
     return cudaErrorNotSupported;
   } else {
@@ -1056,7 +1061,7 @@ cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a0, cu
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(configured & (1u << (dev & 31)))) {
-      cudaError_t e = cudaFuncSetAttribute(k_mixed_stage<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
+      cudaError_t e = cudaFuncSetAttribute(k_mixed_stage<EQ, N, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
       if (e != cudaSuccess) return e;
       configured |= 1u << (dev & 31);
     }
@@ -1085,13 +1090,22 @@ cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a0, cu
     // bit 0: the state is bulk-copied (16-byte aligned); bit 1: warm L2 with u0
     const int flags = (((uintptr_t)a.x & 15) == 0 ? 1 : 0) |
                       (a.mode == MODE_FINAL && ((uintptr_t)a.u0 & 15) == 0 ? 2 : 0);
-    k_mixed_stage<EQ, N><<<grid, kMixThreads, C::BYTES, s>>>(d, a, p->rowsum, flags);
+    k_mixed_stage<EQ, N, SH><<<grid, kMixThreads, C::BYTES, s>>>(d, a, p->rowsum, flags);
     if (ev) {
       cudaEventRecord(ev[2], s);
       cudaEventRecord(ev[3], s);
     }
     return cudaGetLastError();
   }
+}
+
+// the second chunk shape for the Euler kinds (the batched ensembles' equations)
+template <int EQ, int N>
+cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+  if constexpr ((EQ == EQ_EULER || EQ == EQ_EULER2D) && MixCfg<N, Eq<EQ>::M, 1>::FITS) {
+    if (d.tile_shape == 1) return launch_mixed_sh<EQ, N, 1>(p, d, a, s, ev);
+  }
+  return launch_mixed_sh<EQ, N, 0>(p, d, a, s, ev);
 }
 
 template <int EQ, int N> constexpr bool mixed_fits() { return MixCfg<N, Eq<EQ>::M>::FITS; }

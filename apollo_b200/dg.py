@@ -69,6 +69,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_set_numerical_flux": (C.c_int, [H, C.c_char_p]),
         "apollo_dg_set_limiter": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_averaging_weights": (C.c_int, [H, _dp]),
+        "apollo_dg_set_launch_shape": (C.c_int, [H, C.c_int, C.c_int]),
         "apollo_dg_set_mesh": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip]),
         "apollo_dg_num_fields": (C.c_int, [H]),
         "apollo_dg_num_nodes": (C.c_int, [H]),
@@ -104,7 +105,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_batch_get_state": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
         "apollo_dg_batch_init_dt": (C.c_int, [H, _dp]),
         "apollo_dg_batch_step": (C.c_int, [H, C.c_int, _dp, _dp, C.c_int]),
-        "apollo_dg_batch_autotune": (C.c_int, [H, C.c_int, _ip]),
+        "apollo_dg_batch_autotune": (C.c_int, [H, C.c_int, _ip, _ip]),
         "apollo_dg_batch_last_error": (C.c_char_p, [H]),
         "apollo_dg_batch_destroy": (C.c_int, [H]),
         "apollo_dg_mesh_read_gmsh": (C.c_int, [C.c_char_p, C.POINTER(H), C.c_char_p, C.c_int]),
@@ -206,6 +207,10 @@ class NodalDG2d:
             self.close()
         except Exception:
             pass
+
+    def set_launch_shape(self, grid_share: int = 1, tile_shape: int = 0):
+        """The persistent grids' share of the SMs and the mixed stage's operand chunking."""
+        self._check(self.lib.apollo_dg_set_launch_shape(self.h, grid_share, tile_shape))
 
     def averaging_weights(self):
         """w[Np]: an element's average of a nodal field is sum_n w[n] u[n]."""
@@ -426,10 +431,13 @@ class NodalDG2dBatch:
         return t, dt
 
     def autotune(self, precision: str = "mixed"):
-        """Pick each order group's persistent-grid share by timing; returns {order: share}."""
-        ch = np.zeros(4, dtype=np.int32)
-        self._check(self.lib.apollo_dg_batch_autotune(self.h, PREC[precision], ch.ctypes.data_as(_ip)))
-        return {N: int(ch[N - 2]) for N in range(2, 6) if ch[N - 2]}
+        """Pick each order group's launch and tile shape by timing; returns
+        {order: (grid share, tile shape)}."""
+        share = np.zeros(4, dtype=np.int32)
+        shape = np.zeros(4, dtype=np.int32)
+        self._check(self.lib.apollo_dg_batch_autotune(self.h, PREC[precision], share.ctypes.data_as(_ip),
+                                                      shape.ctypes.data_as(_ip)))
+        return {N: (int(share[N - 2]), int(shape[N - 2])) for N in range(2, 6) if share[N - 2]}
 
     def close(self):
         if getattr(self, "h", None):

@@ -370,7 +370,7 @@ def ensemble_measure(args, device: int):
                    "orders": dict(sorted(Counter(p.N for p in ps).items())),
                    "beta_range": [min(p.meta["beta"] for p in ps), max(p.meta["beta"] for p in ps)],
                    "dofs": dofs, "steps": steps, "seed": 0},
-        "unit": METRIC, "mixed": res["mixed"], "fp64": res["fp64"], "autotune_grid_share": tune,
+        "unit": METRIC, "mixed": res["mixed"], "fp64": res["fp64"], "autotune_share_and_shape": {str(k): list(v) for k, v in tune.items()},
         "per_instance": {"l2_mixed_vs_exact": e_exact, "l2_mixed_vs_fp64": e_mixed,
                          "max_l2_mixed_vs_fp64": max(e_mixed), "max_l2_mixed_vs_exact": max(e_exact)},
         "how": "wall clock around the synchronous C-ABI calls (apollo_dg_batch_step; apollo_dg_step per "

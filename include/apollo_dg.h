@@ -107,6 +107,13 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
  * (APOLLO_ERR_CONFIG). */
 apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double* params, int nparams);
 
+/* Launch and tile shape of this handle's kernels, as the batch autotuner
+ * picks them (apollo_dg_batch_autotune): the persistent grids use
+ * SMs / grid_share CTAs; tile_shape 0 or 1 selects the mixed stage kernel's
+ * operand chunking for the Euler kinds (the same arithmetic either way).
+ * No counterpart in Apollo. */
+apollo_status apollo_dg_set_launch_shape(apollo_dg* h, int grid_share, int tile_shape);
+
 /* The element average of a nodal field is sum_n w[n] u[n]: w[Np] receives the
  * weights (half the column sums of the reference mass matrix, Apollo's
  * LimiterElementAVE, src/lib/wxnodaldggeometry2d.h:84-98). */
@@ -266,10 +273,14 @@ apollo_status apollo_dg_batch_init_dt(apollo_dg_batch* b, double* dt);
 /* nsteps steps of every instance from its own (t[i], dt[i]); both arrays are
  * updated in place (dt policy of apollo_dg_step, no end time). */
 apollo_status apollo_dg_batch_step(apollo_dg_batch* b, int nsteps, double* t, double* dt, apollo_precision prec);
-/* Times the candidate launch shapes of each order group (persistent CTAs per
- * SM share) for this precision and keeps the fastest; choice[4] receives the
- * picked share per order 2..5 (0: order absent). */
-apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec, int* choice);
+/* Times the candidate launch and tile shapes of each order group for this
+ * precision and keeps the fastest: the persistent grid's share of the SMs
+ * (all, half, a quarter) and, in mixed precision, the stage kernel's operand
+ * chunking (0: 24-column chunks, 16 at order 5, in a two-buffer ring; 1:
+ * 16-column chunks in a three-buffer ring; the same arithmetic either way).
+ * share[4] and shape[4] (either may be NULL) receive the picks per order
+ * 2..5 (share 0 and shape -1: order absent). */
+apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec, int* share, int* shape);
 const char* apollo_dg_batch_last_error(const apollo_dg_batch* b);
 apollo_status apollo_dg_batch_destroy(apollo_dg_batch* b);
 

@@ -103,7 +103,7 @@ def test_batch_autotune_keeps_state():
         U0.append(u)
     choice = b.autotune("mixed")
     assert set(choice) == {p.N for p in ps}
-    assert all(v in (1, 2, 4) for v in choice.values())
+    assert all(share in (1, 2, 4) and shape in (0, 1) for share, shape in choice.values())
     for i in range(len(ps)):
         np.testing.assert_array_equal(b.get_state(i), U0[i])
     # stepping after tuning still matches a single handle

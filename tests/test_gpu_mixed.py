@@ -84,3 +84,24 @@ def test_mixed_nan_reports_error():
     with pytest.raises(ApolloError) as e:
         s.step(0.0, 0.0, U, precision="mixed")
     assert e.value.code == 4
+
+
+@pytest.mark.parametrize("N", [2, 3, 4, 5])
+def test_tile_shapes_compute_the_same_steps(N):
+    """Both operand chunkings of the mixed stage (and a reduced grid) give the
+    same steps bit for bit: the same MMAs in the same K order."""
+    p = problems.euler_vortex(n=17, N=N)
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh)
+    x, y = s.node_coords()
+    U0 = np.ascontiguousarray(p.ic(x, y))
+    s.set_state(U0)
+    dt0 = s.init_dt()
+    ends = []
+    for share, shape in ((1, 0), (1, 1), (2, 1), (4, 0)):
+        s.set_launch_shape(share, shape)
+        s.set_state(U0)
+        t, dt = s.advance(6, 0.0, dt0, precision="mixed")
+        ends.append((s.get_state(), t, dt))
+    for U, t, dt in ends[1:]:
+        np.testing.assert_array_equal(U, ends[0][0])
+        assert t == ends[0][1] and dt == ends[0][2]
