@@ -505,6 +505,52 @@ def partitioned_arm(args, rank: int, world: int, local: int):
     return 0
 
 
+def e2e_pipelined(s, U0, dt0, prec: str, ne: int) -> float:
+    """Seconds for ne independent steps streamed through the public API, each
+    one's input uploaded from and its result downloaded to pinned host memory
+    inside the timed region, the copies of neighbouring steps overlapping the
+    current step's compute (two device buffers each way)."""
+    import torch
+    shape = s.shape
+    hU = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    hU.numpy()[...] = U0
+    hO = [torch.empty(shape, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    dU = [torch.empty(shape, dtype=torch.float64, device="cuda") for _ in range(2)]
+    dO = [torch.empty(shape, dtype=torch.float64, device="cuda") for _ in range(2)]
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    ev_up = [torch.cuda.Event() for _ in range(2)]
+    ev_down = [torch.cuda.Event() for _ in range(2)]
+
+    def run(n):
+        t, dt = 0.0, dt0
+        for e in ev_down:
+            e.record(down)
+        with torch.cuda.stream(up):
+            dU[0].copy_(hU, non_blocking=True)
+            ev_up[0].record(up)
+        for i in range(n):
+            b = i % 2
+            if i + 1 < n:
+                with torch.cuda.stream(up):  # dU[1 - b] was consumed by step i - 1's set_state
+                    dU[1 - b].copy_(hU, non_blocking=True)
+                    ev_up[1 - b].record(up)
+            ev_up[b].synchronize()
+            s.set_state(dU[b])
+            s.advance_async(1, t, dt, precision=prec)
+            ev_down[b].synchronize()  # step i - 2's result has left dO[b]
+            s.get_state(dO[b])        # returns once step i is done
+            t, dt = s.time()
+            with torch.cuda.stream(down):
+                hO[b].copy_(dO[b], non_blocking=True)
+                ev_down[b].record(down)
+        torch.cuda.synchronize()
+
+    run(2)
+    t0 = time.perf_counter()
+    run(ne)
+    return time.perf_counter() - t0
+
+
 def ours_arm(args):
     import torch
     rank, world, local = dist_env()
@@ -655,9 +701,20 @@ def ours_arm(args):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             el = float(tt.item())
         nb = s.K * s.Np * s.m * 8
-        e2e = {"value": dofs * world * ne / el, "unit": METRIC, "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
-               "steps": ne, "how": "wall clock; per step apollo_dg_set_state (pinned H2D) + apollo_dg_step (1 step) "
-                                   "+ apollo_dg_get_state (pinned D2H)"}
+        serial = dofs * world * ne / el
+        el_p = e2e_pipelined(s, U0, dt0, prec, ne)
+        if dist:
+            tt = torch.tensor([el_p], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el_p = float(tt.item())
+        e2e = {"value": dofs * world * ne / el_p, "unit": METRIC, "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
+               "steps": ne, "serial_value": serial,
+               "how": "wall clock over independent steps streamed through the public API: each step's input "
+                      "copied from pinned host memory to a device buffer on an upload stream while the previous "
+                      "step computes, apollo_dg_set_state (device pointer), apollo_dg_step_async (1 step), "
+                      "apollo_dg_get_state (device pointer), and the result copied to pinned host memory on a "
+                      "download stream while the next step computes; serial_value: the same calls with host "
+                      "pointers, one step at a time"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
