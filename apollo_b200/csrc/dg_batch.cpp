@@ -393,7 +393,19 @@ apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec
   // keep the states: every trial starts from them
   const size_t ni = b->inst.size();
   std::vector<double> t0(ni), dt0(ni);
-  std::vector<double*> saved(b->groups.size(), nullptr);
+  // the saved states and the timing events, released on every return
+  struct Scratch {
+    std::vector<double*> saved;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~Scratch() {
+      for (double* p : saved)
+        if (p) cudaFree(p);
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    }
+  } sc;
+  sc.saved.assign(b->groups.size(), nullptr);
+  std::vector<double*>& saved = sc.saved;
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
     apollo_dg* h = b->groups[gi].h;
     const DevState* st = handle_states_host(h);
@@ -418,9 +430,9 @@ apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec
     for (size_t i = 0; i < ni; ++i)
       if (!(dt0[i] > 0.0)) dt0[i] = dtinit[i];
   }
-  cudaEvent_t e0, e1;
-  BCK(cudaEventCreate(&e0), "autotune");
-  BCK(cudaEventCreate(&e1), "autotune");
+  BCK(cudaEventCreate(&sc.e0), "autotune");
+  BCK(cudaEventCreate(&sc.e1), "autotune");
+  cudaEvent_t e0 = sc.e0, e1 = sc.e1;
   auto trial = [&](float* ms) -> apollo_status {
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
       apollo_dg* h = b->groups[gi].h;
@@ -478,10 +490,7 @@ apollo_status apollo_dg_batch_autotune(apollo_dg_batch* b, apollo_precision prec
       if (e != cudaSuccess) r = bfail(b, APOLLO_ERR_CUDA, "autotune restore");
       handle_mark_state(h);
     }
-    cudaFree(saved[gi]);
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   for (int i = 0; i < 4; ++i) {
     if (share) share[i] = 0;
     if (shape) shape[i] = -1;
