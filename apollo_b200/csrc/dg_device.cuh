@@ -146,6 +146,8 @@ cudaError_t launch_init_speed(int eq, const DgDev& d, const double* u, cudaStrea
 cudaError_t launch_finalize(const DgDev& d, cudaStream_t s);
 // st[i].lam_bits = 0 for every instance
 cudaError_t launch_reset_lambda(const DgDev& d, cudaStream_t s);
+// *st = v on the stream (no host staging buffer to race with later calls)
+cudaError_t launch_put_state(DevState* st, const DevState& v, cudaStream_t s);
 // Apollo's Euler limiter "eulerLimiterHW" (dg_limiter.cu), orders 2..4: the
 // averaging weights of the nodal basis (half the reference mass matrix's
 // column sums), the face-node mask, and the limiter's own gas_gamma,

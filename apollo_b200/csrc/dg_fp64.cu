@@ -486,6 +486,17 @@ cudaError_t launch_reset_lambda(const DgDev& d, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// the value travels as a kernel argument, captured at launch: the caller's
+// host copy may change before the stream reaches the write
+__global__ void k_put_state(DevState* st, DevState v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *st = v;
+}
+
+cudaError_t launch_put_state(DevState* st, const DevState& v, cudaStream_t s) {
+  k_put_state<<<1, 32, 0, s>>>(st, v);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wmass, cudaStream_t s) {
   const int np = (d.N + 1) * (d.N + 2) / 2;
   int g = (d.K + 255) / 256;

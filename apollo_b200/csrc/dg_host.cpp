@@ -694,28 +694,52 @@ apollo_status apollo_dg_node_coords(apollo_dg* h, double* x, double* y) {
   return APOLLO_OK;
 }
 
+namespace {
+// The resident state in or out, queued on the handle's stream; `wait` returns
+// only once the copy is done.
+apollo_status copy_state(apollo_dg* h, double* dst, const double* src, bool in, int where, bool wait,
+                         const char* what) {
+  const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
+  const cudaMemcpyKind kind = where == APOLLO_DEVICE_PTR ? cudaMemcpyDeviceToDevice
+                              : in                        ? cudaMemcpyHostToDevice
+                                                          : cudaMemcpyDeviceToHost;
+  CK(cudaMemcpyAsync(dst, src, n, kind, h->stream), what);
+  if (wait) CK(cudaStreamSynchronize(h->stream), what);
+  if (in) {
+    h->have_state = true;
+    h->tu_valid = false;
+  }
+  return APOLLO_OK;
+}
+}  // namespace
+
 apollo_status apollo_dg_set_state(apollo_dg* h, const double* U, int where) {
   apollo_status r = check_ready(h);
   if (r) return r;
   if (!U) return APOLLO_ERR_ARG;
-  const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
-  CK(cudaMemcpyAsync(h->U_d, U, n, where == APOLLO_DEVICE_PTR ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                     h->stream), "set state");
-  CK(cudaStreamSynchronize(h->stream), "set state");
-  h->have_state = true;
-  h->tu_valid = false;
-  return APOLLO_OK;
+  return copy_state(h, h->U_d, U, true, where, true, "set state");
 }
 
 apollo_status apollo_dg_get_state(apollo_dg* h, double* U, int where) {
   apollo_status r = check_ready(h);
   if (r) return r;
   if (!U) return APOLLO_ERR_ARG;
-  const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
-  CK(cudaMemcpyAsync(U, h->U_d, n, where == APOLLO_DEVICE_PTR ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                     h->stream), "get state");
-  CK(cudaStreamSynchronize(h->stream), "get state");
-  return APOLLO_OK;
+  return copy_state(h, U, h->U_d, false, where, true, "get state");
+}
+
+apollo_status apollo_dg_set_state_async(apollo_dg* h, const double* U, int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!U) return APOLLO_ERR_ARG;
+  return copy_state(h, h->U_d, U, true, where, false, "set state");
+}
+
+apollo_status apollo_dg_get_state_async(apollo_dg* h, double* U, int where) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!U) return APOLLO_ERR_ARG;
+  if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  return copy_state(h, U, h->U_d, false, where, false, "get state");
 }
 
 apollo_status apollo_dg_init_dt(apollo_dg* h, double* dt) {
@@ -787,8 +811,7 @@ apollo_status apollo_dg_step_async(apollo_dg* h, int nsteps, double t, double dt
   s.dt = dt;
   s.tend = 0.0;
   s.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
-  std::memcpy(h->st_h, &s, sizeof(DevState));
-  CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
+  CK(launch_put_state(h->st_d, s, h->stream), "step state");
   cudaGraphExec_t g = nullptr;
   r = step_graph(h, prec, &g);
   if (r) return r;
@@ -829,8 +852,7 @@ apollo_status apollo_dg_step(apollo_dg* h, int nsteps, double* t, double* dt, do
     s.dt = dd;
     s.tend = tend;
     s.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
-    std::memcpy(h->st_h, &s, sizeof(DevState));
-    CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
+    CK(launch_put_state(h->st_d, s, h->stream), "step state");
     cudaGraphExec_t g = nullptr;
     r = step_graph(h, prec, &g);
     if (r) return r;
@@ -1389,8 +1411,7 @@ apollo_status apollo_dg_dist_start(apollo_dg* h, double t, double dt, apollo_pre
   s.t = t;
   s.dt = dt;
   s.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
-  std::memcpy(h->st_h, &s, sizeof(DevState));
-  CK(cudaMemcpyAsync(h->st_d, h->st_h, sizeof(DevState), cudaMemcpyHostToDevice, h->stream), "step state");
+  CK(launch_put_state(h->st_d, s, h->stream), "step state");
   return handle_prepare_step(h, prec);
 }
 

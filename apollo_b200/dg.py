@@ -79,6 +79,8 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_node_coords": (C.c_int, [H, _dp, _dp]),
         "apollo_dg_set_state": (C.c_int, [H, C.c_void_p, C.c_int]),
         "apollo_dg_get_state": (C.c_int, [H, C.c_void_p, C.c_int]),
+        "apollo_dg_set_state_async": (C.c_int, [H, C.c_void_p, C.c_int]),
+        "apollo_dg_get_state_async": (C.c_int, [H, C.c_void_p, C.c_int]),
         "apollo_dg_init_dt": (C.c_int, [H, _dp]),
         "apollo_dg_rhs": (C.c_int, [H, C.c_double, C.c_double, C.c_void_p, C.c_void_p, _dp, C.c_int, C.c_int]),
         "apollo_dg_step": (C.c_int, [H, C.c_int, _dp, _dp, C.c_double, C.c_int]),
@@ -133,8 +135,9 @@ def load_library(path: str = LIB_PATH):
     return lib
 
 
-def _ptr(a):
-    """(pointer, where) of a numpy array or a torch tensor."""
+def _ptr(a, sync: bool = True):
+    """(pointer, where) of a numpy array or a torch tensor.  With sync, torch's
+    current stream is drained first when the tensor is on the device."""
     if isinstance(a, np.ndarray):
         assert a.dtype == np.float64 and a.flags.c_contiguous
         return C.c_void_p(a.ctypes.data), APOLLO_HOST_PTR
@@ -144,8 +147,9 @@ def _ptr(a):
         # the library works on its own stream: whatever torch queued that
         # produces or still reads this tensor must finish first (the library's
         # calls return with their own stream synchronised)
-        import torch
-        torch.cuda.current_stream(a.device).synchronize()
+        if sync:
+            import torch
+            torch.cuda.current_stream(a.device).synchronize()
         return C.c_void_p(a.data_ptr()), APOLLO_DEVICE_PTR
     return C.c_void_p(a.data_ptr()), APOLLO_HOST_PTR
 
@@ -253,6 +257,20 @@ class NodalDG2d:
             out = np.empty(self.shape)
         p, where = _ptr(out)
         self._check(self.lib.apollo_dg_get_state(self.h, p, where))
+        return out
+
+    def set_state_async(self, U):
+        """Queue the copy of U into the resident state on the handle's stream
+        and return (apollo_dg_set_state_async): the caller orders it against
+        the stream that produces U, and a host U should be page-locked."""
+        p, where = _ptr(U, sync=False)
+        self._check(self.lib.apollo_dg_set_state_async(self.h, p, where))
+
+    def get_state_async(self, out):
+        """Queue the copy of the resident state into ``out`` (a device tensor or
+        page-locked host memory) on the handle's stream and return."""
+        p, where = _ptr(out, sync=False)
+        self._check(self.lib.apollo_dg_get_state_async(self.h, p, where))
         return out
 
     def init_dt(self) -> float:

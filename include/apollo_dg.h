@@ -155,6 +155,16 @@ apollo_status apollo_dg_node_coords(apollo_dg* h, double* x, double* y);
 apollo_status apollo_dg_set_state(apollo_dg* h, const double* U, int where);
 apollo_status apollo_dg_get_state(apollo_dg* h, double* U, int where);
 
+/* The same copies queued on the handle's stream, returning at once (no
+ * counterpart in Apollo, whose state is a host-side PETSc Vec).  The caller
+ * orders them against its own streams (a handle created on the caller's
+ * stream, or apollo_dg_synchronize) and keeps U untouched until the stream
+ * has passed the copy; a host U must be page-locked for the copy to be
+ * asynchronous.  Together with apollo_dg_step_async they let independent
+ * states stream through one handle without a host wait per step. */
+apollo_status apollo_dg_set_state_async(apollo_dg* h, const double* U, int where);
+apollo_status apollo_dg_get_state_async(apollo_dg* h, double* U, int where);
+
 /* Initial dt from the resident state: 2/3 cfl dtscale rmin / max wave speed,
  * wave speeds from the Riemann solver at every node. */
 apollo_status apollo_dg_init_dt(apollo_dg* h, double* dt);
