@@ -1018,36 +1018,60 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   if (warp == 0) umma::tmem_dealloc(tb, C::TCOLS);
 }
 
-// Face traces [K][3][TS] of a state: one thread per (element, field, face).
+// Face traces [K][3][TS] of a state.  A block of 128 threads takes 128 / M
+// elements: their states, one contiguous range of x, are read into shared
+// memory with coalesced loads (at most NP per thread, all in flight at once),
+// then each thread owns one (element, field) row and writes its traces on all
+// three faces, so every state value is read from HBM once.
+constexpr int kTraceThreads = 128;
 template <int N, int M>
-__global__ void __launch_bounds__(256) k_mixed_traces(int K, const double* __restrict__ x,
-                                                      const double* __restrict__ I, float* __restrict__ T) {
+__global__ void __launch_bounds__(kTraceThreads) k_mixed_traces(int K, const double* __restrict__ x,
+                                                                const double* __restrict__ I, float* __restrict__ T) {
   constexpr int NP = Sizes<N>::NP, NG = Sizes<N>::NG, NF = Sizes<N>::NF;
   constexpr int IFS = round_up_c(NP, 4), TS = trace_stride(NG, M);
+  constexpr int EB = kTraceThreads / M;  // elements per block
+  static_assert(EB * NP * M <= NP * kTraceThreads, "NP loads per thread cover the block's states");
   __shared__ __align__(16) float IF[NF * IFS];
-  for (int i = threadIdx.x; i < NF * IFS; i += blockDim.x) IF[i] = (i % IFS) < NP ? (float)I[(i / IFS) * NP + i % IFS] : 0.f;
+  __shared__ double XS[EB * NP * M];
+  const long long k0 = (long long)blockIdx.x * EB;
+  const int ne = (int)min((long long)EB, (long long)K - k0);
+  const int nx = ne * NP * M;
+  const double* xb = x + k0 * NP * M;
+  double ld[NP];
+#pragma unroll
+  for (int u = 0; u < NP; ++u) {
+    const int i = threadIdx.x + u * kTraceThreads;
+    ld[u] = i < nx ? xb[i] : 0.0;
+  }
+  for (int i = threadIdx.x; i < NF * IFS; i += kTraceThreads)
+    IF[i] = (i % IFS) < NP ? (float)I[(i / IFS) * NP + i % IFS] : 0.f;
+#pragma unroll
+  for (int u = 0; u < NP; ++u) {
+    const int i = threadIdx.x + u * kTraceThreads;
+    if (i < nx) XS[i] = ld[u];
+  }
   __syncthreads();
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)K * M * 3) return;
-  const int fc = (int)(t % 3);
-  const long long rest = t / 3;
-  const int f = (int)(rest % M);
-  const int k = (int)(rest / M);
+  const int e = threadIdx.x / M, f = threadIdx.x - e * M;
+  if (e >= ne) return;
   double v[NP];
 #pragma unroll
-  for (int j = 0; j < NP; ++j) v[j] = x[((size_t)k * NP + j) * M + f];
+  for (int j = 0; j < NP; ++j) v[j] = XS[(e * NP + j) * M + f];
   const double m = tree_mean<NP>(v);
   float dv[NP];
 #pragma unroll
   for (int j = 0; j < NP; ++j) dv[j] = (float)(v[j] - m);
-  row_traces<NP, NG, IFS>(IF, dv, m, fc, T + ((size_t)k * 3 + fc) * TS + f, M);
+  float* Tk = T + (size_t)(k0 + e) * 3 * TS + f;
+#pragma unroll 1
+  for (int fc = 0; fc < 3; ++fc) row_traces<NP, NG, IFS>(IF, dv, m, fc, Tk + fc * TS, M);
 }
 
 template <int N, int M>
 cudaError_t launch_traces_t(const DgDev& d, const double* x, float* T, cudaStream_t s) {
-  const long long n = (long long)d.K * M * 3;
-  const int blocks = (int)((n + 255) / 256);
-  k_mixed_traces<N, M><<<blocks, 256, 0, s>>>(d.K, x, d.I, T);
+  constexpr int EB = kTraceThreads / M;
+  const long long blocks = ((long long)d.K + EB - 1) / EB;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+  if (blocks == 0) return cudaSuccess;
+  k_mixed_traces<N, M><<<(unsigned)blocks, kTraceThreads, 0, s>>>(d.K, x, d.I, T);
   return cudaGetLastError();
 }
 
