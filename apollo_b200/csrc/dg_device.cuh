@@ -156,6 +156,7 @@ struct LimArgs {
   double ave[15];
   int fmask[15];
   double gamma, minP, minD;
+  int kind;  // 0: eulerLimiterHW; 1: tuAliabadiLimiter (the equation's primitive floors and parameters)
 };
 size_t limiter_work_doubles(int K);
 // limits x into out (may be x), scratch work[limiter_work_doubles(K)]; xn, yn

@@ -467,14 +467,22 @@ apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double
     h->lim_on = false;
     return APOLLO_OK;
   }
-  if (std::string(kind) != "eulerLimiterHW") return fail(h, APOLLO_ERR_CONFIG, std::string("unknown limiter ") + kind);
-  if (h->eq != EQ_EULER && h->eq != EQ_EULER2D) return fail(h, APOLLO_ERR_CONFIG, "eulerLimiterHW needs an Euler equation");
-  if (h->ops.N > 4) return fail(h, APOLLO_ERR_CONFIG, "eulerLimiterHW supports orders up to 4");
-  if (nparams != 3 || !params) return fail(h, APOLLO_ERR_ARG, "eulerLimiterHW takes gas_gamma, min_pressure, min_density");
+  const std::string k_name(kind);
+  const bool ta = k_name == "tuAliabadiLimiter";
+  if (!ta && k_name != "eulerLimiterHW") return fail(h, APOLLO_ERR_CONFIG, std::string("unknown limiter ") + kind);
+  const bool euler = h->eq == EQ_EULER || h->eq == EQ_EULER2D;
+  const bool maxwell = h->eq == EQ_MAXWELL || h->eq == EQ_MAXWELL_TM;
+  if (!ta && !euler) return fail(h, APOLLO_ERR_CONFIG, "eulerLimiterHW needs an Euler equation");
+  // Apollo's advection equation has no limiterTuAndAliabadi (it throws)
+  if (ta && !euler && !maxwell) return fail(h, APOLLO_ERR_CONFIG, "tuAliabadiLimiter needs an Euler or Maxwell equation");
+  if (h->ops.N > 4) return fail(h, APOLLO_ERR_CONFIG, "the limiters support orders up to 4");
+  if (!ta && (nparams != 3 || !params))
+    return fail(h, APOLLO_ERR_ARG, "eulerLimiterHW takes gas_gamma, min_pressure, min_density");
+  if (ta && nparams != 0) return fail(h, APOLLO_ERR_ARG, "tuAliabadiLimiter takes the equation's parameters, none of its own");
   if (!h->peers.empty()) return fail(h, APOLLO_ERR_CONFIG, "partitioned meshes do not support the limiter");
-  // Apollo's limiter hands its boundary conditions two coordinates where they
-  // read (t, x, y): only conditions that read none are accepted
-  for (int i = 0; i < h->bcs.n; ++i) {
+  // Apollo's limiters hand the boundary conditions two coordinates where
+  // they read (t, x, y): only conditions that read none are accepted
+  for (int i = 0; i < h->bcs.n && euler; ++i) {
     const int k = h->bcs.kind[i];
     if (k != BC_FIXED && k != BC_EULER_WALL && k != BC_EULER_ZEROGRAD && k != BC_EULER_STATE)
       return fail(h, APOLLO_ERR_CONFIG, "the limiter supports wall, zero-gradient, inflow, Dirichlet and fixed boundaries");
@@ -483,9 +491,12 @@ apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double
   LimArgs L{};
   for (int k = 0; k < o.Np; ++k) L.ave[k] = 0.5 * o.mass_colsum[k];
   for (int i = 0; i < 3 * (o.N + 1); ++i) L.fmask[i] = o.fmask[i];
-  L.gamma = params[0];
-  L.minP = params[1];
-  L.minD = params[2];
+  L.kind = ta ? 1 : 0;
+  // eulerLimiterHW reads its own three parameters; tuAliabadiLimiter takes the
+  // Euler equation's gas_gamma, minPressure, minDensity
+  L.gamma = ta ? h->eqp.p[0] : params[0];
+  L.minP = ta ? h->eqp.p[1] : params[1];
+  L.minD = ta ? h->eqp.p[2] : params[2];
   if (!h->lim_work_d) {
     CK(cudaMalloc((void**)&h->lim_work_d, limiter_work_doubles(h->K) * sizeof(double)), "limiter alloc");
     CK(upload(&h->xn_d, h->xn.data(), h->xn.size()), "limiter coordinates");

@@ -1,4 +1,4 @@
-// Apollo's Euler slope limiter "eulerLimiterHW"
+// Apollo's slope limiters "eulerLimiterHW" and "tuAliabadiLimiter"
 // (WxHestavenWarburtonEulerLimiter::applyLimiter,
 // src/hyperapps/euler/wxhesthavenwarburtoneulerlimiter.cc:44-330), float64,
 // one thread per element in two passes:
@@ -14,6 +14,14 @@
 // coordinates with the averaging weights of nodes 0..2, the third edge's
 // gradient uses the second edge's vertex differences, and the face averages
 // are read at positions given by element node ids.
+//
+// tuAliabadiLimiter (WxTuAliabadiLimiter::applyLimiter,
+// src/hyperapps/multifluid/aptualiabadilimiter.cc:75-410) runs the same patch
+// procedure through the equation set: for Euler the primitive variables come
+// from the equation (with its density and pressure floors, which rewrite the
+// averages they are given) and the equation's gas_gamma, minPressure and
+// minDensity drive the reconstruction; for phMaxwellEqn the reconstruction
+// returns the cell averages, so every node takes its element's average.
 #include "dg_device.cuh"
 
 namespace apollo {
@@ -28,6 +36,25 @@ __device__ __forceinline__ void lim_prim(double gamma, const double* c, double* 
   p[2] = c[2] / c[0];
   p[3] = c3 / c[0];
   p[4] = (gamma - 1.) * (c[M - 1] - 0.5 * (c[1] * c[1] + c[2] * c[2] + c3 * c3) / c[0]);
+}
+
+// The equation's primitive variables as Apollo's tuAliabadiLimiter obtains
+// them (WxEulerEqn::primitiveVariables, src/hyperapps/euler/wxeulereqn.cc:1326-1341):
+// density and pressure floors, which also rewrite the conserved values given.
+__device__ __forceinline__ void ta_prim(double gamma, double minP, double minD, double* c, double* p) {
+  p[0] = c[0];
+  if (p[0] <= 0.) {
+    c[0] = minD;
+    p[0] = minD;
+  }
+  p[1] = c[1] / c[0];
+  p[2] = c[2] / c[0];
+  p[3] = c[3] / c[0];
+  p[4] = (gamma - 1.) * (c[4] - 0.5 * (c[1] * c[1] + c[2] * c[2] + c[3] * c[3]) / c[0]);
+  if (p[4] <= 0.) {
+    p[4] = minP;
+    c[4] = minP / (gamma - 1.) + 0.5 * p[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+  }
 }
 
 // per element: E1x E1y E2x E2y E3x E3y C0x C0y (5 each), cons average, prim average
@@ -86,18 +113,25 @@ __global__ void __launch_bounds__(128) k_limiter_grad(DgDev d, LimArgs L, const 
     if (M == 5) a[3] = b[3];
     a[M - 1] = b[4];
   };
+  // eulerLimiterHW: the limiter's own primitive variables; tuAliabadiLimiter:
+  // the equation's, whose floors rewrite the averages they are given
+  const bool ta = L.kind == 1;
+  auto prim_of = [&](double* c, double* p) {
+    if (ta) ta_prim(L.gamma, L.minP, L.minD, c, p);
+    else lim_prim<5>(L.gamma, c, p);
+  };
   average(q, cons[0]);
-  lim_prim<5>(L.gamma, cons[0], prim[0]);
+  prim_of(cons[0], prim[0]);
   for (int f = 0; f < 3; ++f) {
     if (nb[f] < 0) {
       double qa[M], qb[M];
       from5(cons[0], qa);
       apply_bc<EQ, double>(d.bcs, -nb[f], xc[f + 1], yc[f + 1], 0.0, g.nx[f], g.ny[f], qa, qb);
       to5(qb, cons[f + 1]);
-      lim_prim<5>(L.gamma, cons[f + 1], prim[f + 1]);
+      prim_of(cons[f + 1], prim[f + 1]);
     } else {
       average(x + (size_t)nb[f] * NP * M, cons[f + 1]);
-      lim_prim<5>(L.gamma, cons[f + 1], prim[f + 1]);
+      prim_of(cons[f + 1], prim[f + 1]);
     }
   }
   // Step 3: face averages at the six positions Apollo reads (fConsA at index
@@ -120,6 +154,10 @@ __global__ void __launch_bounds__(128) k_limiter_grad(DgDev d, LimArgs L, const 
     double fa[M], c5[5];
     for (int f = 0; f < M; ++f) fa[f] = 0.5 * (qp[f] + qm[f]);
     to5(fa, c5);
+    if (ta) {
+      ta_prim(L.gamma, L.minP, L.minD, c5, fprim[n]);
+      continue;
+    }
     const double rho = c5[0], rhou = c5[1], rhov = c5[2], rhow = c5[3], en = c5[4];
     fprim[n][0] = rho;
     fprim[n][1] = rhou / rho;
@@ -236,6 +274,9 @@ __global__ void __launch_bounds__(128) k_limiter_apply(DgDev d, LimArgs L, const
       }
     }
     if (!isfinite(Lrho) || !isfinite(Lrhou) || !isfinite(Lrhov) || !isfinite(LEner)) err |= ERRB_NAN;
+    // tuAliabadiLimiter's reconstruction (WxEulerEqn::limiterTuAndAliabadi)
+    // also stops on a non-positive density
+    if (L.kind == 1 && Lrho <= 0.) err |= ERRB_NONPHYS;
     o[n * M + 0] = Lrho;
     o[n * M + 1] = Lrhou;
     o[n * M + 2] = Lrhov;
@@ -243,6 +284,36 @@ __global__ void __launch_bounds__(128) k_limiter_apply(DgDev d, LimArgs L, const
     o[n * M + M - 1] = LEner;
   }
   if (err) atomicOr(&d.st->err, err);
+}
+
+// tuAliabadiLimiter for phMaxwellEqn (WxPHMaxwellEqn::limiterTuAndAliabadi,
+// src/hyperapps/maxwell/wxphmaxwelleqn.cc:740-755, returns the cell averages):
+// every node of an element takes the element average, field by field, summed
+// in node order.  One thread per (element, field); it reads its row before it
+// writes it, so out may be x.
+template <int M, int N>
+__global__ void __launch_bounds__(128) k_limiter_average(int K, LimArgs L, const double* x, double* out) {
+  constexpr int NP = Sizes<N>::NP;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)K * M) return;
+  const long long e = t / M;
+  const int f = (int)(t - e * M);
+  double s = 0.0;
+  for (int n = 0; n < NP; ++n) s += L.ave[n] * x[(e * NP + n) * M + f];
+  for (int n = 0; n < NP; ++n) out[(e * NP + n) * M + f] = s;
+}
+
+template <int M>
+cudaError_t average_n(const DgDev& d, const LimArgs& L, const double* x, double* out, cudaStream_t s) {
+  const long long n = (long long)d.K * M;
+  const int blocks = (int)((n + 127) / 128);
+  switch (d.N) {
+    case 2: k_limiter_average<M, 2><<<blocks, 128, 0, s>>>(d.K, L, x, out); break;
+    case 3: k_limiter_average<M, 3><<<blocks, 128, 0, s>>>(d.K, L, x, out); break;
+    case 4: k_limiter_average<M, 4><<<blocks, 128, 0, s>>>(d.K, L, x, out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 template <int EQ, int N>
@@ -273,6 +344,8 @@ cudaError_t launch_limiter(int eq, const DgDev& d, const LimArgs& L, const doubl
                            const double* yn, double* work, cudaStream_t s) {
   if (eq == EQ_EULER) return limiter_n<EQ_EULER>(d, L, x, out, xn, yn, work, s);
   if (eq == EQ_EULER2D) return limiter_n<EQ_EULER2D>(d, L, x, out, xn, yn, work, s);
+  if (L.kind == 1 && eq == EQ_MAXWELL) return average_n<Eq<EQ_MAXWELL>::M>(d, L, x, out, s);
+  if (L.kind == 1 && eq == EQ_MAXWELL_TM) return average_n<Eq<EQ_MAXWELL_TM>::M>(d, L, x, out, s);
   return cudaErrorInvalidValue;
 }
 

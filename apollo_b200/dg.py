@@ -228,8 +228,9 @@ class NodalDG2d:
         write_vtu(path, self.mesh, self.get_state() if U is None else U, averages=self.averaging_weights(), time=time)
 
     def set_limiter(self, kind: str | None, params=()):
-        """Apollo's limiter on every stage input (kind "eulerLimiterHW", params
-        gas_gamma, min_pressure, min_density); None removes it."""
+        """Apollo's limiter on every stage input: kind "eulerLimiterHW" (params
+        gas_gamma, min_pressure, min_density) or "tuAliabadiLimiter" (no
+        params: the equation's own); None removes it."""
         p = np.asarray(list(params), dtype=np.float64)
         self._check(self.lib.apollo_dg_set_limiter(self.h, kind.encode() if kind else None,
                                                    p.ctypes.data_as(_dp) if len(p) else None, len(p)))

@@ -96,11 +96,17 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
  * WxNodalDG2dMethod::step does (src/subsolvers/wxnodaldg2dmethod.cc:243-247,
  * "Limiter = [...]").  kind "eulerLimiterHW" (WxHestavenWarburtonEulerLimiter,
  * src/hyperapps/euler/wxhesthavenwarburtoneulerlimiter.cc) with params
- * gas_gamma, min_pressure, min_density; NULL or "" removes the limiter.  Call
- * after apollo_dg_set_mesh and the boundary conditions.  Euler kinds, orders
- * 2..4 (at order 5 Apollo reads past its face-average array); boundary
- * conditions that read no time or position (wall, zero gradient, inflow,
- * Dirichlet, fixed), since Apollo's limiter hands them none.  apollo_dg_step
+ * gas_gamma, min_pressure, min_density, Euler kinds only; or kind
+ * "tuAliabadiLimiter" (WxTuAliabadiLimiter,
+ * src/hyperapps/multifluid/aptualiabadilimiter.cc) with no params: Euler kinds
+ * with the equation's own gas_gamma, minPressure, minDensity and its
+ * primitive-variable floors, and the Maxwell kinds, whose nodes it sets to the
+ * element averages (advection has no such hook in Apollo).  NULL or "" removes
+ * the limiter.  Call after apollo_dg_set_mesh and the boundary conditions.
+ * Orders 2..4 (at order 5 Apollo reads past its face-average array); for the
+ * Euler kinds, boundary conditions that read no time or position (wall, zero
+ * gradient, inflow, Dirichlet, fixed), since Apollo's limiters hand them
+ * none.  apollo_dg_step
  * limits each stage's work state (the step's solution is combined unlimited,
  * as in PETSc's SSP stepper); apollo_dg_rhs limits a copy of its input.
  * Mixed precision, partitioned meshes and the derivatives refuse it

@@ -238,6 +238,7 @@ struct Oracle {
   std::vector<double> area_total; // per-field area integrals of the last RHS
   // Euler limiter eulerLimiterHW (orc_set_limiter)
   bool lim_on = false;
+  int lim_kind = 0;  // 0: eulerLimiterHW, 1: tuAliabadiLimiter
   double lim_gamma = 1.4, lim_minP = 0.0, lim_minD = 0.0;
   std::vector<double> lim_ave;
 };
@@ -841,9 +842,101 @@ static void lim_prim(const Oracle& o, const double* qc, double* qp) {
   qp[4] = (o.lim_gamma - 1.) * (qc[4] - 0.5 * (qc[1] * qc[1] + qc[2] * qc[2] + qc[3] * qc[3]) / qc[0]);
 }
 
+// "tuAliabadiLimiter" (WxTuAliabadiLimiter::applyLimiter,
+// src/hyperapps/multifluid/aptualiabadilimiter.cc:75-410) is the same patch
+// procedure written against the equation set: the primitive variables come
+// from the equation's primitiveVariables, which for Euler applies the density
+// and pressure floors and rewrites the conserved values it was given
+// (wxeulereqn.cc:1326-1341), and the reconstruction is the equation's
+// limiterTuAndAliabadi: for Euler the formulas above with the equation's own
+// gas_gamma, minPressure and minDensity (wxeulereqn.cc:1345-1450), for
+// phMaxwellEqn every node set to the element average (wxphmaxwelleqn.cc:740-755).
+static void ta_prim(const Oracle& o, double* qc, double* qp) {
+  const double g = o.eqp[0], minP = o.eqp[1], minD = o.eqp[2];
+  qp[0] = qc[0];
+  if (qp[0] <= 0.) {
+    qc[0] = minD;
+    qp[0] = minD;
+  }
+  qp[1] = qc[1] / qc[0];
+  qp[2] = qc[2] / qc[0];
+  qp[3] = qc[3] / qc[0];
+  qp[4] = (g - 1.) * (qc[4] - 0.5 * (qc[1] * qc[1] + qc[2] * qc[2] + qc[3] * qc[3]) / qc[0]);
+  if (qp[4] <= 0.) {
+    qp[4] = minP;
+    qc[4] = minP / (g - 1.) + 0.5 * qp[0] * (qp[1] * qp[1] + qp[2] * qp[2] + qp[3] * qp[3]);
+  }
+}
+
+// One node's limited conserved state from the cell averages (conserved cc,
+// primitive cp) and the node's limited primitive deviations dq: the limiter's
+// density and pressure fixes (wxhesthavenwarburtoneulerlimiter.cc:236-318;
+// the same arithmetic as WxEulerEqn::limiterTuAndAliabadi, wxeulereqn.cc:1345-1450,
+// whose checks ta adds).
+static void lim_reconstruct(double g, double minP, double minD, const double* cc, const double* cp, const double* dq,
+                            double* out, bool ta, int& err) {
+  double averho = cp[0], aveu = cp[1], avev = cp[2], avew = cp[3], avep = cp[4];
+  double drho = dq[0], du = dq[1], dv = dq[2], dw = dq[3], dp = dq[4];
+  double Lrho = averho + drho;
+  if (Lrho < minD) {
+    for (int r = 0; r < 4; ++r) {
+      drho *= 0.5;
+      Lrho = averho + drho;
+      if (Lrho > minD) break;
+      else if (r == 3) Lrho = cc[0];
+    }
+  }
+  double Lrhou = cc[1] + averho * du + drho * aveu;
+  double Lrhov = cc[2] + averho * dv + drho * avev;
+  double Lrhow = cc[3] + averho * dw + drho * avew;
+  double dEner = dp / (g - 1.) + 0.5 * drho * (aveu * aveu + avev * avev + avew * avew) + averho * (aveu * du + avev * dv + avew * dw);
+  double LEner = cc[4] + dEner;
+  double Lp = (g - 1.) * (LEner - 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho);
+  if (Lp < minP) {
+    for (int r = 0; r < 4; ++r) {
+      dp *= 0.5;
+      dEner = dp / (g - 1.) + 0.5 * drho * (aveu * aveu + avev * avev + avew * avew) + averho * (aveu * du + avev * dv + avew * dw);
+      LEner = cc[4] + dEner;
+      Lp = (g - 1.) * (LEner - 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho);
+      if (Lp > minP) break;
+      else if (r == 3) LEner = avep / (g - 1.) + 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho;
+    }
+  }
+  out[0] = Lrho;
+  out[1] = Lrhou;
+  out[2] = Lrhov;
+  out[3] = Lrhow;
+  out[4] = LEner;
+  if (!std::isfinite(Lrho) || !std::isfinite(LEner)) err |= ERR_NAN;
+  if (ta && (!std::isfinite(Lrhou) || !std::isfinite(Lrhov))) err |= ERR_NAN;
+  if (ta && Lrho <= 0.) err |= ERR_NONPHYS;
+}
+
 static void apply_limiter(Oracle& o, double* u) {
   const int K = o.K, Np = o.Np, NpF = o.N + 1, meqn = 5;
   const std::vector<double>& AVE = o.lim_ave;
+  const bool ta = o.lim_kind == 1;
+  if (ta && o.eq != EQ_EULER) {
+    // every node of an element takes the element average, field by field
+    const int m = o.meqn;
+    std::vector<double> c(m);
+    for (int e = 0; e < K; ++e) {
+      double* q = &u[(size_t)e * Np * m];
+      for (int f = 0; f < m; ++f) c[f] = 0.;
+      for (int f = 0; f < m; ++f)
+        for (int n = 0; n < Np; ++n) c[f] += AVE[n] * q[n * m + f];
+      for (int n = 0; n < Np; ++n)
+        for (int f = 0; f < m; ++f) q[n * m + f] = c[f];
+    }
+    return;
+  }
+  auto prim = [&](double* qc, double* qp) {
+    if (ta) ta_prim(o, qc, qp);
+    else lim_prim(o, qc, qp);
+  };
+  const double lim_g = ta ? o.eqp[0] : o.lim_gamma;
+  const double lim_mP = ta ? o.eqp[1] : o.lim_minP;
+  const double lim_mD = ta ? o.eqp[2] : o.lim_minD;
   std::vector<double> dropAVE((size_t)Np * Np);
   {
     int sk = 0;
@@ -874,7 +967,7 @@ static void apply_limiter(Oracle& o, double* u) {
     for (int n = 0; n < Np; ++n)
       for (int f = 0; f < 5; ++f) c[f] += AVE[n] * qIn[n * 5 + f];
     for (int f = 0; f < 5; ++f) qCons[f] = c[f];
-    lim_prim(o, qCons, qPrim);
+    prim(qCons, qPrim);
   };
   // the reference hands the boundary conditions two coordinates where they
   // read (t, x, y); only conditions that read none are accepted with the limiter
@@ -927,7 +1020,7 @@ static void apply_limiter(Oracle& o, double* u) {
         double NX[2] = {normals[3 * el], normals[3 * el + 1]};
         for (int c = 0; c < meqn; ++c) qCons[c] = ConsAve[c][0];
         bc(-connect[2 * el], xc[el + 1], yc[el + 1], NX, qCons, qBC);
-        lim_prim(o, qBC, qPrim);
+        prim(qBC, qPrim);
         for (int c = 0; c < meqn; ++c) {
           ConsAve[c][el + 1] = qBC[c];
           PrimAve[c][el + 1] = qPrim[c];
@@ -953,7 +1046,12 @@ static void apply_limiter(Oracle& o, double* u) {
     for (int i = 0; i < 3 * NpF * meqn; ++i) fConsA[i] = 0.5 * (QP[i] + QM[i]);
     int endIDs[6] = {o.fmask[0], o.fmask[NpF - 1], o.fmask[NpF], o.fmask[2 * NpF - 1], o.fmask[2 * NpF], o.fmask[3 * NpF - 1]};
     double fPrimA[6 * 5];
-    for (int n = 0; n < 6; ++n) {
+    for (int n = 0; n < 6 && ta; ++n) {
+      double Conserved[5];
+      for (int c = 0; c < meqn; ++c) Conserved[c] = fConsA[endIDs[n] * meqn + c];
+      prim(Conserved, &fPrimA[n * meqn]);
+    }
+    for (int n = 0; n < 6 && !ta; ++n) {
       double rho = fConsA[endIDs[n] * meqn + 0], rhou = fConsA[endIDs[n] * meqn + 1],
              rhov = fConsA[endIDs[n] * meqn + 2], rhow = fConsA[endIDs[n] * meqn + 3],
              Ener = fConsA[endIDs[n] * meqn + 4];
@@ -1014,42 +1112,10 @@ static void apply_limiter(Oracle& o, double* u) {
     double* qOut = &u[(size_t)e * Np * meqn];
     const double* cp = &cellAVEprim[(size_t)e * meqn];
     const double* cc = &cellAVEcons[(size_t)e * meqn];
-    const double g = o.lim_gamma;
     for (int n = 0; n < Np; ++n) {
-      double averho = cp[0], aveu = cp[1], avev = cp[2], avew = cp[3], avep = cp[4];
-      double drho = qdv[n * meqn + 0], du = qdv[n * meqn + 1], dv = qdv[n * meqn + 2], dw = qdv[n * meqn + 3],
-             dp = qdv[n * meqn + 4];
-      double Lrho = averho + drho;
-      if (Lrho < o.lim_minD) {
-        for (int r = 0; r < 4; ++r) {
-          drho *= 0.5;
-          Lrho = averho + drho;
-          if (Lrho > o.lim_minD) break;
-          else if (r == 3) Lrho = cc[0];
-        }
-      }
-      double Lrhou = cc[1] + averho * du + drho * aveu;
-      double Lrhov = cc[2] + averho * dv + drho * avev;
-      double Lrhow = cc[3] + averho * dw + drho * avew;
-      double dEner = dp / (g - 1.) + 0.5 * drho * (aveu * aveu + avev * avev + avew * avew) + averho * (aveu * du + avev * dv + avew * dw);
-      double LEner = cc[4] + dEner;
-      double Lp = (g - 1.) * (LEner - 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho);
-      if (Lp < o.lim_minP) {
-        for (int r = 0; r < 4; ++r) {
-          dp *= 0.5;
-          dEner = dp / (g - 1.) + 0.5 * drho * (aveu * aveu + avev * avev + avew * avew) + averho * (aveu * du + avev * dv + avew * dw);
-          LEner = cc[4] + dEner;
-          Lp = (g - 1.) * (LEner - 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho);
-          if (Lp > o.lim_minP) break;
-          else if (r == 3) LEner = avep / (g - 1.) + 0.5 * (Lrhou * Lrhou + Lrhov * Lrhov + Lrhow * Lrhow) / Lrho;
-        }
-      }
-      qOut[n * meqn + 0] = Lrho;
-      qOut[n * meqn + 1] = Lrhou;
-      qOut[n * meqn + 2] = Lrhov;
-      qOut[n * meqn + 3] = Lrhow;
-      qOut[n * meqn + 4] = LEner;
-      if (!std::isfinite(Lrho) || !std::isfinite(LEner)) o.err |= ERR_NAN;
+      double out[5];
+      lim_reconstruct(lim_g, lim_mP, lim_mD, cc, cp, &qdv[n * meqn], out, ta, o.err);
+      for (int c = 0; c < meqn; ++c) qOut[n * meqn + c] = out[c];
     }
   }
 }
@@ -1087,6 +1153,7 @@ int orc_set_limiter(void* h, double gamma, double minP, double minD) {
   Oracle& o = *(Oracle*)h;
   if (o.eq != EQ_EULER || o.N > 4) return -1;
   o.lim_on = true;
+  o.lim_kind = 0;
   o.lim_gamma = gamma;
   o.lim_minP = minP;
   o.lim_minD = minD;
@@ -1098,7 +1165,38 @@ int orc_set_limiter(void* h, double gamma, double minP, double minD) {
   return 0;
 }
 
-// The limiter applied in place to a state u [K][Np][5].
+// Enables "tuAliabadiLimiter" (N <= 4): for eulerEqn with the equation's own
+// gas_gamma, minPressure and minDensity, for phMaxwellEqn as element
+// averaging; returns 0, or -1 if not applicable (advection has no
+// limiterTuAndAliabadi in Apollo).
+int orc_set_limiter_ta(void* h) {
+  Oracle& o = *(Oracle*)h;
+  if ((o.eq != EQ_EULER && o.eq != EQ_MAXWELL) || o.N > 4) return -1;
+  int r = orc_set_limiter(h, o.eqp[0], o.eqp[1], o.eqp[2]);
+  if (o.eq == EQ_MAXWELL) {
+    o.lim_on = true;
+    std::vector<double> Mass = invert(o.VVT, o.Np);
+    o.lim_ave.assign(o.Np, 0.0);
+    for (int k = 0; k < o.Np; ++k)
+      for (int m = 0; m < o.Np; ++m) o.lim_ave[k] += 0.5 * Mass[k + m * o.Np];
+    r = 0;
+  }
+  if (r == 0) o.lim_kind = 1;
+  return r;
+}
+
+// Pinning helpers for the tuAliabadiLimiter pieces taken from the equation:
+// the Euler primitive variables with their floors (qc rewritten in place), and
+// one node's reconstruction with the equation's parameters.
+void orc_ta_prim(void* h, double* qc, double* qp) { ta_prim(*(Oracle*)h, qc, qp); }
+int orc_ta_node(void* h, const double* cc, const double* cp, const double* dq, double* out) {
+  Oracle& o = *(Oracle*)h;
+  int err = 0;
+  lim_reconstruct(o.eqp[0], o.eqp[1], o.eqp[2], cc, cp, dq, out, true, err);
+  return err;
+}
+
+// The limiter applied in place to a state u [K][Np][m].
 void orc_limit(void* h, double* u) { apply_limiter(*(Oracle*)h, u); }
 
 // Run nsteps steps (stopping early at tend) with Apollo's dt policy: the

@@ -71,6 +71,12 @@ def _lib():
     lib.orc_set_limiter.restype = C.c_int
     lib.orc_limit.argtypes = [C.c_void_p, _dp]
     lib.orc_limit.restype = None
+    lib.orc_set_limiter_ta.argtypes = [C.c_void_p]
+    lib.orc_set_limiter_ta.restype = C.c_int
+    lib.orc_ta_prim.argtypes = [C.c_void_p, _dp, _dp]
+    lib.orc_ta_prim.restype = None
+    lib.orc_ta_node.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+    lib.orc_ta_node.restype = C.c_int
     return lib
 
 
@@ -166,6 +172,27 @@ class Oracle:
         if self.lib.orc_set_limiter(self.h, gamma, min_pressure, min_density) != 0:
             raise ValueError("the limiter needs eulerEqn at order <= 4")
 
+    def set_limiter_ta(self) -> None:
+        """Apollo's tuAliabadiLimiter on every stage input (eulerEqn with the
+        equation's own gas_gamma, minPressure, minDensity; phMaxwellEqn as
+        element averaging; N <= 4)."""
+        if self.lib.orc_set_limiter_ta(self.h) != 0:
+            raise ValueError("tuAliabadiLimiter needs eulerEqn or phMaxwellEqn at order <= 4")
+
+    def ta_prim(self, qc):
+        """(floored conserved, primitive) of one Euler state, as the limiter computes them."""
+        c = np.array(qc, dtype=np.float64, copy=True)
+        p = np.zeros(5)
+        self.lib.orc_ta_prim(self.h, _p(c), _p(p))
+        return c, p
+
+    def ta_node(self, cc, cp, dq):
+        """(limited conserved state, error bits) of one node."""
+        out = np.zeros(5)
+        a, b, d = (np.ascontiguousarray(v, dtype=np.float64) for v in (cc, cp, dq))
+        err = self.lib.orc_ta_node(self.h, _p(a), _p(b), _p(d), _p(out))
+        return out, err
+
     def limit(self, u):
         """The limiter applied to a copy of u."""
         v = np.array(u, dtype=np.float64, order="C", copy=True)
@@ -204,6 +231,8 @@ class RefPlugins:
         lib.ref_exprfunc_size.restype = C.c_int
         lib.ref_exprfunc_eval.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _dp]
         lib.ref_exprfunc_destroy.argtypes = [C.c_void_p]
+        lib.ref_primitive.argtypes = [C.c_void_p, _dp, _dp]
+        lib.ref_ta_limit.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         self.lib = lib
 
     @staticmethod
@@ -232,6 +261,20 @@ class RefPlugins:
         lam = C.c_double(0.0)
         self.lib.ref_numflux(h, _p(n), _p(qM), _p(qP), _p(f), C.byref(lam))
         return f, lam.value
+
+    def primitive(self, h, qc):
+        """(conserved as rewritten by the equation, primitive) of one state."""
+        c = np.array(qc, dtype=np.float64, copy=True)
+        p = np.zeros_like(c)
+        self.lib.ref_primitive(h, _p(c), _p(p))
+        return c, p
+
+    def ta_limit(self, h, cc, cp, dq):
+        """One node of the equation's Tu-Aliabadi reconstruction."""
+        a, b, d = (np.array(v, dtype=np.float64, copy=True) for v in (cc, cp, dq))
+        out = np.zeros_like(a)
+        self.lib.ref_ta_limit(h, _p(a), _p(b), _p(d), _p(out))
+        return out
 
     def speed2(self, h, q) -> float:
         q = np.ascontiguousarray(q, dtype=np.float64)

@@ -94,6 +94,19 @@ void ref_numflux(void* h, const double* n, double* qM, double* qP, double* f, do
   r->set.DGnumericalFlux(nn, qM, qP, f, lam);
 }
 
+// The equation set's primitive variables (WxHyperbolicEqnSet::getPrimitiveVariable);
+// qc is mutable because Apollo's Euler floors rewrite it.
+void ref_primitive(void* h, double* qc, double* qp) {
+  RefEqn* r = (RefEqn*)h;
+  r->set.getPrimitiveVariable(qc, qp);
+}
+
+// One node of the Tu-Aliabadi reconstruction (WxHyperbolicEqnSet::tuAndAliabadiLimiter).
+void ref_ta_limit(void* h, double* avg_cons, double* avg_prim, double* dgrads, double* out) {
+  RefEqn* r = (RefEqn*)h;
+  r->set.tuAndAliabadiLimiter(avg_cons, avg_prim, dgrads, out);
+}
+
 // Wave speeds of the Riemann problem with ql = qr = q in x and y, reduced the
 // way WxNodalDG2dMethod::init does (wxnodaldg2dmethod.cc:201-209): returns the
 // max over waves of max(sx^2, sy^2).

@@ -85,10 +85,17 @@ CASES = [
      dict(gas_gamma=1.4, Numerical_Flux="Wave"), CHANNEL_BCS, 1),  # non-physical from the second step
     ("euler_hll_limiter_N3", channel, dict(N=3, n=9, seed=4), orc.EQ_EULER, (1.4, 0.0, 0.0, orc.NF_HLL), "eulerEqn",
      dict(gas_gamma=1.4, Numerical_Flux="HLL"), CHANNEL_BCS, 4),
+    ("euler_hll_talimiter_N3", channel, dict(N=3, n=9, seed=6), orc.EQ_EULER, (1.4, 1e-6, 1e-6, orc.NF_HLL),
+     "eulerEqn", dict(gas_gamma=1.4, Numerical_Flux="HLL", minPressure=1e-6, minDensity=1e-6), CHANNEL_BCS, 4),
+    ("maxwell_talimiter_N3", problems.maxwell_tm, dict(n=6, N=3, fields=8, seed=7), orc.EQ_MAXWELL, (1.0, 0.0, 0.0),
+     "phMaxwellEqn", dict(c0=1.0), ((orc.BC_TM, ()),), 3),
 ]
 
-# the eulerLimiterHW parameters (gas_gamma, min_pressure, min_density) per case
-LIMITERS = {"euler_hll_limiter_N3": (1.4, 1e-6, 1e-6)}
+# the limiter per case: eulerLimiterHW with its own (gas_gamma, min_pressure,
+# min_density), or tuAliabadiLimiter, which takes the equation's parameters
+LIMITERS = {"euler_hll_limiter_N3": ("eulerLimiterHW", (1.4, 1e-6, 1e-6)),
+            "euler_hll_talimiter_N3": ("tuAliabadiLimiter", ()),
+            "maxwell_talimiter_N3": ("tuAliabadiLimiter", ())}
 
 FLUX_NAMES = {orc.NF_LF: "LF", orc.NF_HLL: "HLL", orc.NF_ROE: "Roe", orc.NF_WAVE: "Wave"}
 
@@ -106,8 +113,13 @@ def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref)
     if lim is not None:
         # the limiter (restated in the oracle; Apollo's needs PETSc's DMPlex)
         # acts on every stage input, and on the input of a single right-hand side
-        o.set_limiter(*lim)
-        extra["limiter"] = np.asarray(lim, dtype=np.float64)
+        kind, params = lim
+        if kind == "eulerLimiterHW":
+            o.set_limiter(*params)
+        else:
+            o.set_limiter_ta()
+        extra["limiter"] = np.asarray(params, dtype=np.float64)
+        extra["limiter_kind"] = kind
         rhs, sugg = o.rhs(o.limit(U0), 0.0, 0.0)
     else:
         rhs, sugg = o.rhs(U0, 0.0, 0.0)

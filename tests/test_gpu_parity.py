@@ -19,7 +19,7 @@ def _solver(g):
     s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
                   numerical_flux=g["numflux"])
     if "limiter" in g:
-        s.set_limiter("eulerLimiterHW", g["limiter"])
+        s.set_limiter(str(g.get("limiter_kind", "eulerLimiterHW")), g["limiter"])
     return s
 
 
@@ -251,6 +251,34 @@ def test_limiter_refusals_and_removal():
     sv = NodalDG2d(int(v["N"]), float(v["cfl"]), v["equation"], v["eqp"][:3], v["mesh"], bcs=v["bcs"])
     with pytest.raises(ApolloError):
         sv.set_limiter("eulerLimiterHW", (1.4, 1e-6, 1e-6))
+
+
+def test_tu_aliabadi_limiter_kinds():
+    """tuAliabadiLimiter: Maxwell nodes become the element averages; on an
+    Euler state away from the floors it equals eulerLimiterHW given the
+    equation's parameters; advection and explicit parameters are refused."""
+    from apollo_b200 import ApolloError
+    g = load("maxwell_talimiter_N3")
+    s = _solver(g)
+    w = s.averaging_weights()
+    rng = np.random.default_rng(3)
+    U = rng.normal(size=s.shape)
+    out, _ = s.step(0.0, 0.0, U)
+    s.set_limiter(None)
+    avg = np.einsum("n,knm->km", w, U)
+    ref, _ = s.step(0.0, 0.0, np.ascontiguousarray(np.broadcast_to(avg[:, None, :], U.shape)))
+    np.testing.assert_allclose(out, ref, rtol=0, atol=1e-13 * np.abs(ref).max())
+    e = load("euler_hll_talimiter_N3")
+    a, b = _solver(e), _solver(e)
+    b.set_limiter("eulerLimiterHW", tuple(float(v) for v in e["eqp"][:3]))
+    ra, rb = a.step(0.0, 0.0, e["U0"])[0], b.step(0.0, 0.0, e["U0"])[0]
+    assert rel_l2(ra, rb) <= 1e-14
+    with pytest.raises(ApolloError):
+        a.set_limiter("tuAliabadiLimiter", (1.4, 1e-6, 1e-6))
+    adv = load("adv_N3")
+    sa = _solver(adv)
+    with pytest.raises(ApolloError):
+        sa.set_limiter("tuAliabadiLimiter")
 
 
 def test_averaging_weights_and_vtu(tmp_path):

@@ -23,7 +23,10 @@ def test_oracle_port_reproduces_golden(oracle_lib, name):
     x, y = o.node_coords()
     np.testing.assert_array_equal(x, g["x"])
     if "limiter" in g:
-        o.set_limiter(*g["limiter"])
+        if str(g.get("limiter_kind", "eulerLimiterHW")) == "tuAliabadiLimiter":
+            o.set_limiter_ta()
+        else:
+            o.set_limiter(*g["limiter"])
         rhs, sugg = o.rhs(o.limit(g["U0"]))
     else:
         rhs, sugg = o.rhs(g["U0"])
@@ -212,3 +215,54 @@ def test_conservation_periodic(oracle_lib):
     tot = np.einsum("k,j,kjf->f", J, w, rhs)
     scale = np.einsum("k,j,kjf->f", J, w, np.abs(rhs))
     assert np.all(np.abs(tot) <= 1e-12 * np.maximum(scale, 1.0))
+
+
+def test_tu_aliabadi_pieces_bitexact_vs_reference(oracle_lib):
+    """The Tu-Aliabadi limiter's equation hooks restated in the oracle (Euler
+    primitive variables with their floors, which rewrite the conserved input,
+    and one node's reconstruction) equal Apollo's compiled eulerEqn plugin bit
+    for bit, on states that do and do not reach the floors."""
+    orc = oracle_lib
+    ref = _ref(orc)
+    rng = np.random.default_rng(11)
+    minP, minD = 1e-3, 1e-2
+    h = ref.equation("eulerEqn", gas_gamma=1.4, minPressure=minP, minDensity=minD)
+    mesh = jittered_square(4, (0.0, 0.0), (1.0, 1.0), jitter=0.1, seed=1, periodic=True)
+    o = orc.Oracle(mesh, 2, orc.EQ_EULER, (1.4, minP, minD))
+    o.set_limiter_ta()
+    for trial in range(400):
+        q = rng.uniform(-1, 1, 5)
+        q[0] = rng.uniform(-0.2, 2.0)           # some at or below zero density
+        q[4] = rng.uniform(-0.5, 3.0)           # some with negative pressure
+        if abs(q[0]) < 1e-9:
+            q[0] = 0.5
+        ca, pa = o.ta_prim(q)
+        cb, pb = ref.primitive(h, q)
+        np.testing.assert_array_equal(ca, cb)
+        np.testing.assert_array_equal(pa, pb)
+    for trial in range(400):
+        rho = rng.uniform(0.05, 2.0)
+        u = rng.uniform(-1, 1, 3)
+        p = rng.uniform(0.01, 2.0)
+        cp = np.array([rho, u[0], u[1], u[2], p])
+        cc = np.array([rho, rho * u[0], rho * u[1], rho * u[2], p / 0.4 + 0.5 * rho * (u @ u)])
+        # deviations large enough to reach the density and pressure fixes now and then
+        dq = rng.normal(0, 1, 5) * np.array([rho, 0.5, 0.5, 0.5, p]) * rng.choice([0.1, 1.0, 3.0])
+        out, err = o.ta_node(cc, cp, dq)
+        if err or out[0] <= 0 or not np.all(np.isfinite(out)):
+            continue  # Apollo's plugin exits the process on these
+        np.testing.assert_array_equal(out, ref.ta_limit(h, cc, cp, dq))
+
+
+def test_tu_aliabadi_equals_hw_without_floors(oracle_lib):
+    """Away from the floors the two Euler limiters compute the same state."""
+    orc = oracle_lib
+    g = load("euler_hll_talimiter_N3")
+    bcs = tuple((int(k), tuple(g["bc_params"][i])) for i, k in enumerate(g["bc_kinds"]))
+    a = orc.Oracle(g["mesh"], int(g["N"]), int(g["eq"]), g["eqp"], bcs=bcs)
+    b = orc.Oracle(g["mesh"], int(g["N"]), int(g["eq"]), g["eqp"], bcs=bcs)
+    a.set_limiter_ta()
+    b.set_limiter(float(g["eqp"][0]), float(g["eqp"][1]), float(g["eqp"][2]))
+    la, lb = a.limit(g["U0"]), b.limit(g["U0"])
+    assert not np.array_equal(la, g["U0"])
+    np.testing.assert_array_equal(la, lb)
