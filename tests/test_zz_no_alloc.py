@@ -35,7 +35,7 @@ def test_noalloc_matches_rhs_twice(name):
     u = torch.from_numpy(g["U0"]).cuda()
     if "limiter" in g:
         # the limiter needs scratch of its own: such handles are refused
-        s.set_limiter("eulerLimiterHW", g["limiter"])
+        s.set_limiter(str(g.get("limiter_kind", "eulerLimiterHW")), g["limiter"])
         rc, _ = _noalloc(s, 0.25, 1e-3, u, torch.empty_like(u), torch.cuda.current_stream().cuda_stream)
         assert rc == 7
         return
