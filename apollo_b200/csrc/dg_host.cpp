@@ -193,11 +193,8 @@ apollo_status check_ready(apollo_dg* h) {
   return APOLLO_OK;
 }
 
-// the mixed stage's fp32 face flux is the Lax-Friedrichs flux, and its
-// stage inputs are never limited
+// the mixed stage's stage inputs are never limited
 apollo_status check_mixed_flux(apollo_dg* h) {
-  if ((h->eq == EQ_EULER || h->eq == EQ_EULER2D) && (int)h->eqp.p[3] != NF_LF)
-    return fail(h, APOLLO_ERR_CONFIG, "mixed precision supports the Lax-Friedrichs flux only");
   if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "mixed precision does not support the limiter");
   return APOLLO_OK;
 }

@@ -322,7 +322,12 @@ __device__ __forceinline__ void cp_async_arrive(uint32_t mbar) {
 // ring (full/empty mbarriers), and finish with the float64 epilogue and the
 // result's face traces.  The next tile's operand build and GEMM-A overlap
 // this tile's epilogue; per-tile data live in two slots by tile parity.
-template <int EQ, int N, int SH>
+//
+// GF (Euler kinds): the face flux is the equation's Numerical_Flux (HLL, Roe,
+// Wave) in fp32 instead of the Lax-Friedrichs form, and the float64 face
+// constants are that flux's value at the mean (a separate instantiation, so
+// the Lax-Friedrichs kernels keep their registers).
+template <int EQ, int N, int SH, bool GF = false>
 __global__ void __launch_bounds__(kMixThreads, 1)
     k_mixed_stage(DgDev d, StageArgs a, const double* __restrict__ rowsum, int flags) {
   using P = Eq<EQ>;
@@ -630,8 +635,20 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       }
     };
     // reference fluxes at the fp32 mean of tile i (tasks: volume + 3 faces per element)
+    // the fp32 numerical flux of a face point (qa, qb are not modified)
+    auto face_nf = [&](float nx, float ny, const float* qa, const float* qb, float* nf) -> float {
+      if constexpr (GF) {
+        float x[M], y[M];
+#pragma unroll
+        for (int f = 0; f < M; ++f) { x[f] = qa[f]; y[f] = qb[f]; }
+        return P::numflux(d.eqp, nx, ny, x, y, nf, &err);
+      } else {
+        return Q::lf(d.eqp, nx, ny, qa, qb, nf, &err);
+      }
+    };
     auto refs = [&](int i, int t0, int nt) {
       const int tile = tile_of(i), k0 = tile * E, ne = min(E, d.K - k0);
+      constexpr bool lf_flux = !GF;
       unsigned char* td = slot(i);
       const float* GEO = (const float*)(td + C::TD_GEO);
       const float* QF = (const float*)(td + C::TD_QF);
@@ -667,12 +684,27 @@ __global__ void __launch_bounds__(kMixThreads, 1)
           // term vanishes for equal states) with float64 normals
           const int fc = kind - 1;
           float nf[M];
-          Q::lf(d.eqp, GEO[(4 + fc) * E + e], GEO[(7 + fc) * E + e], qc, qc, nf, &err);
+          face_nf(GEO[(4 + fc) * E + e], GEO[(7 + fc) * E + e], qc, qc, nf);
           const double w = G64[(10 + fc) * E + e], nx = G64[(4 + fc) * E + e], ny = G64[(7 + fc) * E + e];
+          if constexpr (lf_flux) {
 #pragma unroll
-          for (int f = 0; f < M; ++f) {
-            P0[((2 + fc) * M + f) * E + e] = nf[f];
-            Fb[(fc * M + f) * E + e] = w * (nx * (double)F[f] + ny * (double)G[f]);
+            for (int f = 0; f < M; ++f) {
+              P0[((2 + fc) * M + f) * E + e] = nf[f];
+              Fb[(fc * M + f) * E + e] = w * (nx * (double)F[f] + ny * (double)G[f]);
+            }
+          } else {
+            // the other Euler fluxes need not reduce to n.F at equal states
+            // (Apollo's Roe flux does not): the float64 constant is the
+            // float64 numerical flux of the same fp32 mean on both sides
+            double qa[M], qb[M], nd[M];
+#pragma unroll
+            for (int f = 0; f < M; ++f) { qa[f] = (double)qc[f]; qb[f] = (double)qc[f]; }
+            Eq<EQ>::numflux(d.eqp, nx, ny, qa, qb, nd, &err);
+#pragma unroll
+            for (int f = 0; f < M; ++f) {
+              P0[((2 + fc) * M + f) * E + e] = nf[f];
+              Fb[(fc * M + f) * E + e] = w * nd[f];
+            }
           }
         }
       }
@@ -851,7 +883,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
                 bc_coords(k, fc, g, x, y);
                 apply_bc<EQ, float>(d.bcs, -nb, stage_t(k), x, y, nx, ny, qM, qP);
               }
-              const float lam = Q::lf(d.eqp, nx, ny, qM, qP, nf, &err);
+              const float lam = face_nf(nx, ny, qM, qP, nf);
               if (want_lambda) lam_acc.add(d.st, inst_of(d, k), fabs((double)lam));
               const float w = GEO[(10 + fc) * E + e];
 #pragma unroll
@@ -1075,7 +1107,7 @@ cudaError_t launch_traces_t(const DgDev& d, const double* x, float* T, cudaStrea
   return cudaGetLastError();
 }
 
-template <int EQ, int N, int SH>
+template <int EQ, int N, int SH, bool GF = false>
 cudaError_t launch_mixed_sh(MixedPlan* p, const DgDev& d, const StageArgs& a0, cudaStream_t s, cudaEvent_t* ev) {
   using C = MixCfg<N, Eq<EQ>::M, SH>;
   if constexpr (!C::FITS) {
@@ -1085,7 +1117,7 @@ cudaError_t launch_mixed_sh(MixedPlan* p, const DgDev& d, const StageArgs& a0, c
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(configured & (1u << (dev & 31)))) {
-      cudaError_t e = cudaFuncSetAttribute(k_mixed_stage<EQ, N, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
+      cudaError_t e = cudaFuncSetAttribute(k_mixed_stage<EQ, N, SH, GF>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
       if (e != cudaSuccess) return e;
       configured |= 1u << (dev & 31);
     }
@@ -1114,7 +1146,7 @@ cudaError_t launch_mixed_sh(MixedPlan* p, const DgDev& d, const StageArgs& a0, c
     // bit 0: the state is bulk-copied (16-byte aligned); bit 1: warm L2 with u0
     const int flags = (((uintptr_t)a.x & 15) == 0 ? 1 : 0) |
                       (a.mode == MODE_FINAL && ((uintptr_t)a.u0 & 15) == 0 ? 2 : 0);
-    k_mixed_stage<EQ, N, SH><<<grid, kMixThreads, C::BYTES, s>>>(d, a, p->rowsum, flags);
+    k_mixed_stage<EQ, N, SH, GF><<<grid, kMixThreads, C::BYTES, s>>>(d, a, p->rowsum, flags);
     if (ev) {
       cudaEventRecord(ev[2], s);
       cudaEventRecord(ev[3], s);
@@ -1126,6 +1158,10 @@ cudaError_t launch_mixed_sh(MixedPlan* p, const DgDev& d, const StageArgs& a0, c
 // the second chunk shape for the Euler kinds (the batched ensembles' equations)
 template <int EQ, int N>
 cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+  if constexpr (EQ == EQ_EULER || EQ == EQ_EULER2D) {
+    // Apollo's other Euler numerical fluxes: their own instantiation
+    if ((int)d.eqp.p[3] != NF_LF) return launch_mixed_sh<EQ, N, 0, true>(p, d, a, s, ev);
+  }
   if constexpr ((EQ == EQ_EULER || EQ == EQ_EULER2D) && MixCfg<N, Eq<EQ>::M, 1>::FITS) {
     if (d.tile_shape == 1) return launch_mixed_sh<EQ, N, 1>(p, d, a, s, ev);
   }

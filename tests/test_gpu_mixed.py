@@ -49,6 +49,32 @@ def test_mixed_steps_close_to_fp64(name):
     assert tmx == pytest.approx(t64, rel=1e-7)
 
 
+@pytest.mark.parametrize("name", ["euler_hll_N3", "euler_roe_N4", "euler_wave_N2"])
+def test_mixed_other_euler_fluxes_close_to_fp64(name):
+    """HLL, Roe and Wave (Apollo's arithmetic, quirks included) in the mixed
+    stage: its fp32 face flux is the equation's own, and the float64 face
+    constants are that flux at the element mean, so the mixed right-hand side
+    and steps track the float64 ones as closely as with Lax-Friedrichs."""
+    g = load(name)
+    s = _solver(g)
+    r64, s64 = s.step(0.0, 0.0, g["U0"])
+    rmx, smx = s.step(0.0, 0.0, g["U0"], precision="mixed")
+    dt0 = float(g["dt0"])
+    e_stage = rel_l2(g["U0"] + dt0 * rmx, g["U0"] + dt0 * r64)
+    print(name, "stage", e_stage, "rhs", rel_l2(rmx, r64))
+    assert e_stage <= 1e-6
+    assert smx == pytest.approx(s64, rel=1e-5)
+    if int(g["steps"]) > 0:
+        s.set_state(g["U0"])
+        s.advance(int(g["steps"]), 0.0, dt0)
+        U64 = s.get_state()
+        s.set_state(g["U0"])
+        s.advance(int(g["steps"]), 0.0, dt0, precision="mixed")
+        e = rel_l2(s.get_state(), U64)
+        print(name, "steps", e)
+        assert e <= 1e-6
+
+
 def test_mixed_vortex_l2_after_steps():
     """Euler vortex (N = 4) on a 64 x 64 grid: mixed stays within 1e-6 relative L2 of float64."""
     p = problems.euler_vortex(n=64, N=4, fields=4)

@@ -202,13 +202,10 @@ def test_unknown_flux_name_is_lax_friedrichs():
     assert rel_l2(hll, lf) > 1e-3
 
 
-def test_non_lf_fluxes_refused_by_mixed_and_adjoint():
+def test_non_lf_fluxes_refused_by_adjoint():
     from apollo_b200 import ApolloError
     g = load("euler_hll_N3")
     s = _channel_solver(g)
-    with pytest.raises(ApolloError) as e:
-        s.step(0.0, 0.0, g["U0"], precision="mixed")
-    assert e.value.code == 1
     with pytest.raises(ApolloError) as e:
         s.rhs_vjp(0.0, g["U0"], np.ones_like(g["U0"]))
     assert e.value.code == 1
