@@ -193,9 +193,10 @@ apollo_status check_ready(apollo_dg* h) {
   return APOLLO_OK;
 }
 
-// the mixed stage's stage inputs are never limited
+// mixed precision takes every flux and the limiters (the stepper rebuilds
+// the face traces of each limited stage input)
 apollo_status check_mixed_flux(apollo_dg* h) {
-  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "mixed precision does not support the limiter");
+  (void)h;
   return APOLLO_OK;
 }
 
@@ -285,6 +286,12 @@ apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
       apollo_status rl = enqueue_limiter(h, a.x, h->W_d);
       if (rl) return rl;
       a.x = h->W_d;
+      if (prec == APOLLO_PREC_MIXED && h->mixed) {
+        // the mixed stage reads the face traces of its input, which the
+        // previous stage wrote for the unlimited state: those of W instead
+        DgDev d = make_dev(h);
+        CK(mixed_launch_traces(h->mixed, d, h->W_d, (float*)a.tr_in, h->stream), "trace launch");
+      }
     }
     apollo_status r = enqueue_stage(h, a, prec);
     if (r != APOLLO_OK) return r;

@@ -110,7 +110,8 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
  * none.  apollo_dg_step
  * limits each stage's work state (the step's solution is combined unlimited,
  * as in PETSc's SSP stepper); apollo_dg_rhs limits a copy of its input.
- * Mixed precision, partitioned meshes and the derivatives refuse it
+ * In mixed precision the stepper also rebuilds the fp32 face traces of each
+ * limited stage input.  Partitioned meshes and the derivatives refuse it
  * (APOLLO_ERR_CONFIG). */
 apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double* params, int nparams);
 

@@ -75,6 +75,28 @@ def test_mixed_other_euler_fluxes_close_to_fp64(name):
         assert e <= 1e-6
 
 
+@pytest.mark.parametrize("name", ["euler_hll_limiter_N3", "euler_hll_talimiter_N3", "maxwell_talimiter_N3"])
+def test_mixed_with_limiter_close_to_fp64(name):
+    """With a limiter the mixed stepper limits each stage input in float64 and
+    rebuilds that state's face traces before the stage; a right-hand side
+    limits a copy of its input.  Both track the float64 path."""
+    g = load(name)
+    s = _solver(g)
+    r64, _ = s.step(0.0, 0.0, g["U0"])
+    rmx, _ = s.step(0.0, 0.0, g["U0"], precision="mixed")
+    dt0 = float(g["dt0"])
+    e_stage = rel_l2(g["U0"] + dt0 * rmx, g["U0"] + dt0 * r64)
+    s.set_state(g["U0"])
+    s.advance(int(g["steps"]), 0.0, dt0)
+    U64 = s.get_state()
+    s.set_state(g["U0"])
+    s.advance(int(g["steps"]), 0.0, dt0, precision="mixed")
+    e = rel_l2(s.get_state(), U64)
+    print(name, "stage", e_stage, "steps", e)
+    assert e_stage <= 1e-6
+    assert e <= 1e-6
+
+
 def test_mixed_vortex_l2_after_steps():
     """Euler vortex (N = 4) on a 64 x 64 grid: mixed stays within 1e-6 relative L2 of float64."""
     p = problems.euler_vortex(n=64, N=4, fields=4)
