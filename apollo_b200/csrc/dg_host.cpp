@@ -193,12 +193,6 @@ apollo_status check_ready(apollo_dg* h) {
   return APOLLO_OK;
 }
 
-// mixed precision takes every flux and the limiters (the stepper rebuilds
-// the face traces of each limited stage input)
-apollo_status check_mixed_flux(apollo_dg* h) {
-  (void)h;
-  return APOLLO_OK;
-}
 
 // the adjoint's face terms are written for the Lax-Friedrichs flux, and the
 // derivatives do not differentiate the limiter
@@ -238,8 +232,6 @@ apollo_status enqueue_stage(apollo_dg* h, const StageArgs& a, apollo_precision p
   cudaError_t e;
   if (prec == APOLLO_PREC_MIXED) {
     if (!h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision is not available for this equation/order");
-    apollo_status rf = check_mixed_flux(h);
-    if (rf) return rf;
     StageArgs am = a;
     if (am.mode == MODE_RHS) am.tr_scratch = h->T0_d;
     e = mixed_launch_rhs(h->mixed, h->eq, d, am, h->stream, ev);
@@ -1136,10 +1128,6 @@ apollo_status handle_enqueue_step(apollo_dg* h, apollo_precision prec) {
 }
 apollo_status handle_enqueue_step_raw(apollo_dg* h, apollo_precision prec) { return enqueue_step(h, prec); }
 apollo_status handle_prepare_step(apollo_dg* h, apollo_precision prec) {
-  if (prec == APOLLO_PREC_MIXED) {
-    apollo_status rf = check_mixed_flux(h);
-    if (rf) return rf;
-  }
   if (prec == APOLLO_PREC_MIXED && h->mixed && !h->tu_valid) {
     DgDev d = make_dev(h);
     CK(mixed_launch_traces(h->mixed, d, h->U_d, h->TU_d, h->stream), "trace launch");
@@ -1434,7 +1422,6 @@ apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision pr
   apollo_status r = check_ready(h);
   if (r) return r;
   if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "partitioned meshes do not support the limiter");
-  if (prec == APOLLO_PREC_MIXED && (r = check_mixed_flux(h))) return r;
   if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
   if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");
   StageArgs a = stage_args(h, stage);
@@ -1457,7 +1444,6 @@ apollo_status apollo_dg_stage_end(apollo_dg* h, int stage, apollo_precision prec
   apollo_status r = check_ready(h);
   if (r) return r;
   if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "partitioned meshes do not support the limiter");
-  if (prec == APOLLO_PREC_MIXED && (r = check_mixed_flux(h))) return r;
   if (stage < 0 || stage > 4) return APOLLO_ERR_ARG;
   if (prec == APOLLO_PREC_MIXED && !h->mixed) return fail(h, APOLLO_ERR_CONFIG, "mixed precision not available");
   StageArgs a = stage_args(h, stage);
