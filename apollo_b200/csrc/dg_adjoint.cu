@@ -239,6 +239,63 @@ template <int M> struct DVec {
   double v[M];
 };
 
+// (d f*(n, a, b) / d a)^T dv and, with want_b, (d f* / d b)^T dv, by forward
+// differentiation of the equation's own numerical flux (any Numerical_Flux)
+template <int EQ, int M>
+__device__ __forceinline__ void dual_face(const EqParams& P, double nx, double ny, const DVec<M>& a,
+                                          const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
+                                          bool want_b, int* err) {
+  for (int side = 0; side < (want_b ? 2 : 1); ++side) {
+    Dual<M> A[M], B[M], nf[M];
+#pragma unroll
+    for (int f = 0; f < M; ++f) {
+      A[f] = Dual<M>(a.v[f]);
+      B[f] = Dual<M>(b.v[f]);
+      if (side == 0) A[f].d[f] = 1.0;
+      else B[f].d[f] = 1.0;
+    }
+    Eq<EQ>::numflux(P, Dual<M>(nx), Dual<M>(ny), A, B, nf, err);
+    DVec<M>& out = side == 0 ? abar : bbar;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      double sum = 0.0;
+#pragma unroll
+      for (int f = 0; f < M; ++f) sum += dv.v[f] * nf[f].d[j];
+      out.v[j] = sum;
+    }
+  }
+}
+
+// The same by one-component forward passes (2 M evaluations of the flux in
+// Dual<1>, the instantiation the tangent kernels already use): for the Euler
+// fluxes other than Lax-Friedrichs, whose Dual<M> code would be several times
+// larger.
+template <int EQ, int M>
+__device__ __forceinline__ void dual1_face(const EqParams& P, double nx, double ny, const DVec<M>& a,
+                                           const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
+                                           bool want_b, int* err) {
+#pragma unroll 1
+  for (int side = 0; side < (want_b ? 2 : 1); ++side) {
+    DVec<M>& out = side == 0 ? abar : bbar;
+#pragma unroll 1
+    for (int j = 0; j < M; ++j) {
+      Dual<1> A[M], B[M], nf[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) {
+        A[f] = Dual<1>(a.v[f]);
+        B[f] = Dual<1>(b.v[f]);
+      }
+      if (side == 0) A[j].d[0] = 1.0;
+      else B[j].d[0] = 1.0;
+      Eq<EQ>::numflux(P, Dual<1>(nx), Dual<1>(ny), A, B, nf, err);
+      double sum = 0.0;
+#pragma unroll
+      for (int f = 0; f < M; ++f) sum += dv.v[f] * nf[f].d[0];
+      out.v[j] = sum;
+    }
+  }
+}
+
 template <int EQ> struct AdjPhys {
   static constexpr int M = Eq<EQ>::M;
   // (dR/dq)^T aR + (dS/dq)^T aS,  R = rx F + ry G,  S = sx F + sy G
@@ -267,25 +324,7 @@ template <int EQ> struct AdjPhys {
   __device__ __forceinline__ static void face(const EqParams& P, double nx, double ny, const DVec<M>& a,
                                               const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
                                               bool want_b, int* err) {
-    for (int side = 0; side < (want_b ? 2 : 1); ++side) {
-      Dual<M> A[M], B[M], nf[M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) {
-        A[f] = Dual<M>(a.v[f]);
-        B[f] = Dual<M>(b.v[f]);
-        if (side == 0) A[f].d[f] = 1.0;
-        else B[f].d[f] = 1.0;
-      }
-      Eq<EQ>::numflux(P, Dual<M>(nx), Dual<M>(ny), A, B, nf, err);
-      DVec<M>& out = side == 0 ? abar : bbar;
-#pragma unroll
-      for (int j = 0; j < M; ++j) {
-        double sum = 0.0;
-#pragma unroll
-        for (int f = 0; f < M; ++f) sum += dv.v[f] * nf[f].d[j];
-        out.v[j] = sum;
-      }
-    }
+    dual_face<EQ, M>(P, nx, ny, a, b, dv, abar, bbar, want_b, err);
   }
 };
 
@@ -379,6 +418,11 @@ template <int MF> struct EulerAdjPhys {
   __device__ __forceinline__ static void face(const EqParams& P, double nx, double ny, const DVec<M>& a,
                                               const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
                                               bool want_b, int* err) {
+    if ((int)P.p[3] != NF_LF) {
+      // HLL, Roe, Wave: the derivative of Apollo's own flux, quirks included
+      dual1_face<MF == 5 ? EQ_EULER : EQ_EULER2D, M>(P, nx, ny, a, b, dv, abar, bbar, want_b, err);
+      return;
+    }
     double ga[M], gb[M];
     const double ca = EulerAdj<MF>::speed(P, a.v, ga, err), cb = EulerAdj<MF>::speed(P, b.v, gb, err);
     const bool a_wins = ca > cb;  // the branch the forward flux takes
@@ -551,6 +595,7 @@ __global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
       for (int j = 0; j < M; ++j) sQC[c * LDB + e * M + j] = gbar.v[j];
     }
     // faces: w_g (s_own - s_partner) d f*(n_own, a, b) / d a at every Gauss point
+    const bool two_sided = flux_two_sided<EQ>(d.eqp);
     for (int idx = tid; idx < ne * NF; idx += kDThreads) {
       const int e = idx / NF, fg = idx - e * NF, fc = fg / NG, gq = fg - fc * NG;
       const int k = k0 + e;
@@ -564,6 +609,26 @@ __global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
         // the flux's Gauss weight is its first side's (face list: 3 nb + f2 > 3 k + fc)
         const double w = d.gw[(3 * nb + f2 > 3 * k + fc) ? gq : NG - 1 - gq] * g.sJ[fc];
         DVec<M> qa, qb, dvec;
+        if (two_sided) {
+          // each side holds its own evaluation f*(n_side, own, partner) times
+          // its own weight (the forward face kernel's two-sided form): the
+          // own slot differentiated in its first argument, the partner's in
+          // its second
+          const ElemGeo& h2 = d.geo[nb];
+          const double w1 = d.gw[gq] * g.sJ[fc], w2 = d.gw[NG - 1 - gq] * h2.sJ[f2];
+          DVec<M> dv2, unused, bbar;
+#pragma unroll
+          for (int f = 0; f < M; ++f) {
+            qa.v[f] = d.trace[own + f];
+            qb.v[f] = d.trace[par + f];
+            dvec.v[f] = w1 * a.sbar[own + f];
+            dv2.v[f] = w2 * a.sbar[par + f];
+          }
+          AdjPhys<EQ>::face(d.eqp, g.nx[fc], g.ny[fc], qa, qb, dvec, abar, unused, false, &err);
+          AdjPhys<EQ>::face(d.eqp, h2.nx[f2], h2.ny[f2], qb, qa, dv2, unused, bbar, true, &err);
+#pragma unroll
+          for (int j = 0; j < M; ++j) abar.v[j] += bbar.v[j];
+        } else {
 #pragma unroll
         for (int f = 0; f < M; ++f) {
           qa.v[f] = d.trace[own + f];
@@ -572,6 +637,7 @@ __global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
         }
         DVec<M> unused;
         AdjPhys<EQ>::face(d.eqp, g.nx[fc], g.ny[fc], qa, qb, dvec, abar, unused, false, &err);
+        }
       } else {
         // boundary: ghost state b = A a + c (every supported boundary hook is
         // affine in the trace); abar = (df*/da)^T dv + A^T (df*/db)^T dv

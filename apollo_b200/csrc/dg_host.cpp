@@ -194,11 +194,8 @@ apollo_status check_ready(apollo_dg* h) {
 }
 
 
-// the adjoint's face terms are written for the Lax-Friedrichs flux, and the
-// derivatives do not differentiate the limiter
+// the derivatives do not differentiate the limiter
 apollo_status check_adjoint_flux(apollo_dg* h) {
-  if ((h->eq == EQ_EULER || h->eq == EQ_EULER2D) && (int)h->eqp.p[3] != NF_LF)
-    return fail(h, APOLLO_ERR_CONFIG, "the adjoint supports the Lax-Friedrichs flux only");
   if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "the derivatives do not support the limiter");
   return APOLLO_OK;
 }

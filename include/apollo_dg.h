@@ -88,9 +88,8 @@ apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const doubl
  * including its HLL bound |S_R| truncated to an integer, its Roe flux's
  * y-momentum component of 0 and x-momentum component set from the rotated
  * y-momentum flux, and Wave's fall-through to LF on rotated traces.  Other
- * equations have only LF (the name is ignored).  Mixed precision evaluates
- * every one of them (its fp32 face flux is the named flux); the adjoint
- * supports LF only (APOLLO_ERR_CONFIG otherwise). */
+ * equations have only LF (the name is ignored).  Mixed precision and the
+ * derivatives (tangent and adjoint) take every one of them. */
 apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
 
 /* Limiter applied to every stage input before its right-hand side, as

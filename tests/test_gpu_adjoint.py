@@ -152,3 +152,34 @@ def test_torch_autograd_wrapper():
     eps = 1e-6
     fd = (_J(s, u0n + eps * d, targetn, nsteps, dt, 5)[0] - _J(s, u0n - eps * d, targetn, nsteps, dt, 5)[0]) / (2 * eps)
     assert abs(float(np.vdot(g, d)) - fd) <= 1e-6 * abs(fd)
+
+
+def test_trajectory_adjoint_with_hll_flux():
+    """The trajectory gradient with Apollo's HLL flux (two-sided faces, wall,
+    zero-gradient, inflow and Dirichlet boundaries) agrees with the tangent and
+    with central finite differences."""
+    from golden_cases import load
+    g = load("euler_hll_N3")
+    s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
+                  numerical_flux="HLL")
+    u0 = g["U0"].copy()
+    dt = 0.5 * float(g["dt0"])
+    nsteps = 4
+    s.set_state(u0)
+    s.forward_fixed(nsteps, 0.0, dt, 2)
+    target = s.get_state() + 1e-3
+    J0, uT = _J(s, u0, target, nsteps, dt, 2)
+    grad = s.backward(uT - target)
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        d = rng.standard_normal(u0.shape)
+        d[..., 3] = 0.0
+        g_adj = float(np.vdot(grad, d))
+        s.set_state(u0)
+        duT = s.tangent(nsteps, 0.0, dt, d)
+        g_tan = float(np.vdot(uT - target, duT))
+        eps = 1e-6
+        fd = (_J(s, u0 + eps * d, target, nsteps, dt, 2)[0] - _J(s, u0 - eps * d, target, nsteps, dt, 2)[0]) / (2 * eps)
+        print(g_adj, g_tan, fd)
+        assert abs(g_adj - g_tan) <= 1e-10 * abs(g_tan)
+        assert abs(g_adj - fd) <= 1e-5 * abs(fd)
