@@ -44,6 +44,7 @@ struct apollo_dg_batch {
   apollo_dg_config cfg{};
   std::string eq_kind;
   std::vector<double> eqp;
+  std::string numflux;  // Numerical_Flux name, empty: the default
   std::vector<std::pair<std::string, std::vector<double>>> bcs;
   struct MeshIn {
     int N = 0, nverts = 0, K = 0;
@@ -165,6 +166,13 @@ apollo_status apollo_dg_batch_create(const apollo_dg_config* cfg, const char* eq
   return APOLLO_OK;
 }
 
+apollo_status apollo_dg_batch_set_numerical_flux(apollo_dg_batch* b, const char* name) {
+  if (!b || !name) return APOLLO_ERR_ARG;
+  if (b->finalized) return bfail(b, APOLLO_ERR_STATE, "batch already finalized");
+  b->numflux = name;
+  return APOLLO_OK;
+}
+
 apollo_status apollo_dg_batch_add_bc(apollo_dg_batch* b, const char* kind, const double* params, int n_params) {
   if (!b || !kind || n_params < 0 || (n_params > 0 && !params)) return APOLLO_ERR_ARG;
   if (b->finalized) return bfail(b, APOLLO_ERR_STATE, "batch already finalized");
@@ -238,6 +246,7 @@ apollo_status apollo_dg_batch_finalize(apollo_dg_batch* b) {
     G.h = h;
     G.insts = ids;
     r = from_handle(b, h, apollo_dg_set_equation(h, b->eq_kind.c_str(), b->eqp.data(), (int)b->eqp.size()));
+    if (!r && !b->numflux.empty()) r = from_handle(b, h, apollo_dg_set_numerical_flux(h, b->numflux.c_str()));
     for (size_t j = 0; j < b->bcs.size() && !r; ++j)
       r = from_handle(b, h, apollo_dg_add_bc(h, b->bcs[j].first.c_str(), b->bcs[j].second.data(),
                                              (int)b->bcs[j].second.size()));

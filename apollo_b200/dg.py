@@ -98,6 +98,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_adjoint_memory": (C.c_int, [H, C.POINTER(C.c_size_t)]),
         "apollo_dg_batch_create": (C.c_int, [C.POINTER(_Config), C.c_char_p, _dp, C.c_int, C.POINTER(H)]),
         "apollo_dg_batch_add_bc": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
+        "apollo_dg_batch_set_numerical_flux": (C.c_int, [H, C.c_char_p]),
         "apollo_dg_batch_add_mesh": (C.c_int, [H, C.c_int, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip]),
         "apollo_dg_batch_finalize": (C.c_int, [H]),
         "apollo_dg_batch_size": (C.c_int, [H]),
@@ -375,7 +376,7 @@ class NodalDG2dBatch:
     together: each order's instances share one discretisation and every stage
     is one persistent launch; one CUDA graph per step (apollo_dg_batch_*)."""
 
-    def __init__(self, cfl: float, equation: str, eq_params, bcs=(), device: int = 0):
+    def __init__(self, cfl: float, equation: str, eq_params, bcs=(), device: int = 0, numerical_flux: str = "LF"):
         self.lib = load_library()
         cfg = _Config(0, cfl, device, None)
         h = C.c_void_p()
@@ -383,6 +384,8 @@ class NodalDG2dBatch:
         self._check(self.lib.apollo_dg_batch_create(C.byref(cfg), equation.encode(), p.ctypes.data_as(_dp), len(p),
                                                     C.byref(h)), h=None)
         self.h = h
+        if numerical_flux != "LF":
+            self._check(self.lib.apollo_dg_batch_set_numerical_flux(h, numerical_flux.encode()))
         for kind, params in bcs:
             bp = np.asarray(list(params), dtype=np.float64)
             self._check(self.lib.apollo_dg_batch_add_bc(h, kind.encode(), bp.ctypes.data_as(_dp), len(bp)))

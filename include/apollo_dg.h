@@ -273,6 +273,9 @@ typedef struct apollo_dg_batch apollo_dg_batch;
 apollo_status apollo_dg_batch_create(const apollo_dg_config* cfg, const char* eq_kind, const double* eq_params,
                                      int n_params, apollo_dg_batch** out);
 apollo_status apollo_dg_batch_add_bc(apollo_dg_batch* b, const char* kind, const double* params, int n_params);
+/* Every instance's Euler numerical flux (apollo_dg_set_numerical_flux's
+ * names); before apollo_dg_batch_finalize. */
+apollo_status apollo_dg_batch_set_numerical_flux(apollo_dg_batch* b, const char* name);
 /* Adds one mesh (the arguments of apollo_dg_set_mesh) of order N; *instance
  * receives its index. */
 apollo_status apollo_dg_batch_add_mesh(apollo_dg_batch* b, int N, int nverts, const double* vx, const double* vy,

@@ -155,3 +155,29 @@ def test_batch_errors():
         b.add_mesh(ps[1].N, ps[1].mesh)   # after finalize
     with pytest.raises(ApolloError):
         b.set_state(5, np.zeros(b.shape(0)))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_with_hll_flux_and_boundaries(precision):
+    """A batch with Apollo's HLL flux and the channel's four boundary kinds
+    steps every instance exactly as a handle of its own does."""
+    from golden_cases import load
+    g = load("euler_hll_N3")
+    bcs = g["bcs"]
+    b = NodalDG2dBatch(float(g["cfl"]), g["equation"], g["eqp"][:3], bcs=bcs, numerical_flux="HLL")
+    for _ in range(2):
+        b.add_mesh(int(g["N"]), g["mesh"])
+    b.finalize()
+    U = [g["U0"], g["U0"] * np.array([1.0, 1.02, 0.98, 0.0, 1.01])]
+    for i, u in enumerate(U):
+        b.set_state(i, np.ascontiguousarray(u))
+    dt = b.init_dt()
+    t, d = b.step(3, np.zeros(2), dt, precision=precision)
+    for i, u in enumerate(U):
+        s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=bcs,
+                      numerical_flux="HLL")
+        s.set_state(np.ascontiguousarray(u))
+        ts, ds = s.advance(3, 0.0, dt[i], precision=precision)
+        np.testing.assert_array_equal(b.get_state(i), s.get_state())
+        assert t[i] == ts and d[i] == ds
+        s.close()
