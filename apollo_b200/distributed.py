@@ -120,12 +120,13 @@ class DistNodalDG2d:
     SSPRK(5,2) stepper (Apollo's dt policy, dt reduced over the ranks)."""
 
     def __init__(self, N: int, cfl: float, equation: str, eq_params, mesh: Mesh, part, comm, bcs=(),
-                 device: int = 0):
+                 device: int = 0, numerical_flux: str = "LF"):
         import torch
         self.comm = comm
         self.torch_stream = torch.cuda.Stream(device=device)
         self.solver = NodalDG2d(N, cfl, equation, eq_params, mesh, bcs=bcs, device=device,
-                                stream=self.torch_stream.cuda_stream, part=part, rank=comm.rank)
+                                stream=self.torch_stream.cuda_stream, part=part, rank=comm.rank,
+                                numerical_flux=numerical_flux)
         s = self.solver
         self.lib, self.h = s.lib, s.h
         n = C.c_int()

@@ -96,3 +96,32 @@ def test_partitioned_handle_refuses_whole_mesh_calls():
     with pytest.raises(ApolloError):
         s.step(0.0, 0.0, np.ascontiguousarray(p.ic(x, y)))
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_partitioned_hll_channel_equals_whole(precision):
+    """Apollo's HLL flux (evaluated from both sides of a face, ghost slots
+    included) and the channel's four boundary kinds on 2 ranks: bit for bit
+    what one handle on the whole mesh computes."""
+    from golden_cases import load
+    g = load("euler_hll_N3")
+    N, cfl, eq, eqp, bcs = int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["bcs"]
+    s = NodalDG2d(N, cfl, eq, eqp, g["mesh"], bcs=bcs, numerical_flux="HLL")
+    s.set_state(g["U0"])
+    dt0 = s.init_dt()
+    tw, dtw = s.advance(3, 0.0, dt0, precision=precision)
+    Uw = s.get_state()
+    s.close()
+    part = partition(g["mesh"], 2)
+
+    def fn(rank, comm):
+        d = DistNodalDG2d(N, cfl, eq, eqp, g["mesh"], part, comm, bcs=bcs, numerical_flux="HLL")
+        d.set_state(np.ascontiguousarray(g["U0"][part == rank]))
+        t, dt = d.advance(3, 0.0, dt0, precision=precision)
+        U = d.get_state()
+        d.close()
+        return U, t, dt
+
+    for r, (U, t, dt) in enumerate(run_ranks(2, fn)):
+        np.testing.assert_array_equal(U, Uw[part == r])
+        assert t == tw and dt == dtw
