@@ -56,6 +56,11 @@ struct DgDev {
   int ninst;
   int grid_div;    // launch shape: persistent grids use SMs / grid_div (>= 1; 0 means 1)
   int tile_shape;  // mixed stage operand chunking (0 or 1), picked by the batch autotuner
+  // bounded device waits of the mixed stage kernel: polls before a wait gives
+  // up (0: the default, about 2 s), and a test switch that points the kernel's
+  // first wait at a barrier nothing completes (apollo_dg_debug_set_waits)
+  unsigned wait_limit;
+  int debug_stall;
   const double *V, *Dr, *Ds, *I, *L, *gz, *gw;
   double *vol, *trace, *flux;  // scratch: [K][NP][M], [K][NF][M], [K][NF][M]
   DevState* st;
@@ -168,6 +173,7 @@ cudaError_t launch_limiter(int eq, const DgDev& d, const LimArgs& L, const doubl
 cudaError_t launch_halo_blocks(const void* src, void* dst, const int* idx, int n, int block_bytes, bool scatter,
                                cudaStream_t s);
 cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wJ, cudaStream_t s);
+cudaError_t launch_energy(int eq, const DgDev& d, const double* u, const double* mass, cudaStream_t s);
 int fp64_supported(int eq, int N);
 
 }  // namespace apollo

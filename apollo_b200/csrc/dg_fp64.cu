@@ -325,6 +325,40 @@ __global__ void k_integrals(DgDev d, const double* u, const double* wmass, int N
   }
 }
 
+// Per-field integrals of u^2 over the mesh: sum_k J_k u_k^T Mref u_k with the
+// reference-element mass matrix Mref = (V V^T)^-1 (the inverse of Apollo's
+// VVT, wxnodaldggeometry2d.cc:71-75), one thread per element.
+template <int EQ>
+__global__ void k_energy(DgDev d, const double* __restrict__ u, const double* __restrict__ mass, int NP) {
+  constexpr int M = Eq<EQ>::M;
+  double acc[M];
+#pragma unroll
+  for (int f = 0; f < M; ++f) acc[f] = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < d.K; k += gridDim.x * blockDim.x) {
+    const double J = d.geo[k].J;
+    const double* uk = u + (size_t)k * NP * M;
+    for (int i = 0; i < NP; ++i) {
+      double mu[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) mu[f] = 0.0;
+      for (int j = 0; j < NP; ++j) {
+        const double w = mass[i * NP + j];
+#pragma unroll
+        for (int f = 0; f < M; ++f) mu[f] += w * uk[j * M + f];
+      }
+#pragma unroll
+      for (int f = 0; f < M; ++f) acc[f] += J * uk[i * M + f] * mu[f];
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < M; ++f) {
+    double v = acc[f];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&d.st->sums[f], v);
+  }
+}
+
 int g_num_sms = 0;
 int num_sms() {
   if (g_num_sms == 0) {
@@ -508,6 +542,22 @@ cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const doub
     case EQ_MAXWELL: k_integrals<EQ_MAXWELL><<<g, 256, 0, s>>>(d, u, wmass, np); break;
     case EQ_EULER2D: k_integrals<EQ_EULER2D><<<g, 256, 0, s>>>(d, u, wmass, np); break;
     case EQ_MAXWELL_TM: k_integrals<EQ_MAXWELL_TM><<<g, 256, 0, s>>>(d, u, wmass, np); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energy(int eq, const DgDev& d, const double* u, const double* mass, cudaStream_t s) {
+  const int np = (d.N + 1) * (d.N + 2) / 2;
+  int g = (d.K + 127) / 128;
+  if (g > num_sms() * 8) g = num_sms() * 8;
+  if (g < 1) g = 1;
+  switch (eq) {
+    case EQ_ADVECTION: k_energy<EQ_ADVECTION><<<g, 128, 0, s>>>(d, u, mass, np); break;
+    case EQ_EULER: k_energy<EQ_EULER><<<g, 128, 0, s>>>(d, u, mass, np); break;
+    case EQ_MAXWELL: k_energy<EQ_MAXWELL><<<g, 128, 0, s>>>(d, u, mass, np); break;
+    case EQ_EULER2D: k_energy<EQ_EULER2D><<<g, 128, 0, s>>>(d, u, mass, np); break;
+    case EQ_MAXWELL_TM: k_energy<EQ_MAXWELL_TM><<<g, 128, 0, s>>>(d, u, mass, np); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

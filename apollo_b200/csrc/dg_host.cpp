@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -45,8 +46,10 @@ struct apollo_dg {
   int ninst = 1;
   int grid_div = 1;    // launch shape picked by the batch autotuner
   int tile_shape = 0;  // mixed stage operand chunking picked by the batch autotuner
+  unsigned wait_limit = 0;  // apollo_dg_debug_set_waits
+  int debug_stall = 0;
   double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
-         *gw_d = nullptr, *wmass_d = nullptr;
+         *gw_d = nullptr, *wmass_d = nullptr, *mass_d = nullptr;
   double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
   // mixed precision: fp32 face traces of U (TU) and of the stage states (T0, T1)
   float *TU_d = nullptr, *T0_d = nullptr, *T1_d = nullptr;
@@ -99,7 +102,19 @@ apollo_status fail(apollo_dg* h, apollo_status code, const std::string& msg) {
 }
 
 apollo_status cuda_fail(apollo_dg* h, cudaError_t e, const char* where) {
-  return fail(h, APOLLO_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+  return fail(h, e == cudaErrorMemoryAllocation ? APOLLO_ERR_ALLOC : APOLLO_ERR_CUDA,
+              std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Device allocations of the handles go through here, so that a test can make
+// the n-th next one fail (apollo_dg_debug_fail_alloc; -1: never).
+std::atomic<int> g_alloc_fail_in{-1};
+cudaError_t dev_malloc(void** p, size_t bytes) {
+  if (g_alloc_fail_in.load() >= 0 && g_alloc_fail_in.fetch_sub(1) == 0) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
 }
 
 #define CK(call, where)                          \
@@ -130,7 +145,7 @@ void free_mesh(apollo_dg* h) {
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   dfree(h->geo_d); dfree(h->faces_d); dfree(h->conn_d); dfree(h->einst_d);
   dfree(h->V_d); dfree(h->Dr_d); dfree(h->Ds_d); dfree(h->I_d); dfree(h->L_d); dfree(h->gz_d); dfree(h->gw_d);
-  dfree(h->wmass_d);
+  dfree(h->wmass_d); dfree(h->mass_d);
   dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
   dfree(h->TU_d); dfree(h->T0_d); dfree(h->T1_d);
   h->tu_valid = false;
@@ -159,7 +174,7 @@ void free_mesh(apollo_dg* h) {
 
 template <class T>
 cudaError_t upload(T** dst, const T* src, size_t n) {
-  cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T) + 16);
+  cudaError_t e = dev_malloc((void**)dst, n * sizeof(T) + 16);
   if (e != cudaSuccess) return e;
   return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
 }
@@ -179,6 +194,8 @@ DgDev make_dev(const apollo_dg* h) {
   d.ninst = h->ninst;
   d.grid_div = h->grid_div;
   d.tile_shape = h->tile_shape;
+  d.wait_limit = h->wait_limit;
+  d.debug_stall = h->debug_stall;
   d.eqp = h->eqp;
   d.bcs = h->bcs;
   d.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
@@ -334,7 +351,7 @@ apollo_status apollo_dg_create(const apollo_dg_config* cfg, apollo_dg** out) {
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return APOLLO_ERR_CUDA; }
     h->own_stream = true;
   }
-  if (cudaMalloc((void**)&h->st_d, sizeof(DevState)) != cudaSuccess ||
+  if (dev_malloc((void**)&h->st_d, sizeof(DevState)) != cudaSuccess ||
       cudaMallocHost((void**)&h->st_h, sizeof(DevState)) != cudaSuccess) {
     apollo_dg_destroy(h);
     return APOLLO_ERR_ALLOC;
@@ -491,7 +508,7 @@ apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double
   L.minP = ta ? h->eqp.p[1] : params[1];
   L.minD = ta ? h->eqp.p[2] : params[2];
   if (!h->lim_work_d) {
-    CK(cudaMalloc((void**)&h->lim_work_d, limiter_work_doubles(h->K) * sizeof(double)), "limiter alloc");
+    CK(dev_malloc((void**)&h->lim_work_d, limiter_work_doubles(h->K) * sizeof(double)), "limiter alloc");
     CK(upload(&h->xn_d, h->xn.data(), h->xn.size()), "limiter coordinates");
     CK(upload(&h->yn_d, h->yn.data(), h->yn.size()), "limiter coordinates");
   }
@@ -506,7 +523,7 @@ namespace {
 
 // The handle's mesh: the whole mesh (part == nullptr) or the elements of one
 // rank plus ghost slots for their remote neighbours' traces.
-apollo_status set_mesh_impl(apollo_dg* h, int nverts, const double* vx, const double* vy, int Kg, const int* etov,
+apollo_status set_mesh_body(apollo_dg* h, int nverts, const double* vx, const double* vy, int Kg, const int* etov,
                             const int* face_tag, const int* vert_canon, const int* part, int rank) {
   if (!h || !vx || !vy || !etov || nverts < 3 || Kg < 1) return APOLLO_ERR_ARG;
   if (h->eq < 0) return fail(h, APOLLO_ERR_STATE, "set the equation before the mesh");
@@ -629,22 +646,24 @@ apollo_status set_mesh_impl(apollo_dg* h, int nverts, const double* vx, const do
   CK(upload(&h->gz_d, o.gz.data(), o.gz.size()), "op upload");
   CK(upload(&h->gw_d, o.gw.data(), o.gw.size()), "op upload");
   CK(upload(&h->wmass_d, o.mass_colsum.data(), o.mass_colsum.size()), "op upload");
-  CK(cudaMalloc((void**)&h->U_d, nU * sizeof(double)), "state alloc");
-  CK(cudaMalloc((void**)&h->W_d, nU * sizeof(double)), "state alloc");
-  CK(cudaMalloc((void**)&h->in_d, nU * sizeof(double)), "state alloc");
-  CK(cudaMalloc((void**)&h->out_d, nU * sizeof(double)), "state alloc");
-  CK(cudaMalloc((void**)&h->vol_d, nU * sizeof(double)), "scratch alloc");
-  CK(cudaMalloc((void**)&h->trace_d, nT * sizeof(double)), "scratch alloc");
-  CK(cudaMalloc((void**)&h->flux_d, nT * sizeof(double)), "scratch alloc");
+  const Mat mass = inverse(o.VVT);
+  CK(upload(&h->mass_d, mass.a.data(), mass.a.size()), "op upload");
+  CK(dev_malloc((void**)&h->U_d, nU * sizeof(double)), "state alloc");
+  CK(dev_malloc((void**)&h->W_d, nU * sizeof(double)), "state alloc");
+  CK(dev_malloc((void**)&h->in_d, nU * sizeof(double)), "state alloc");
+  CK(dev_malloc((void**)&h->out_d, nU * sizeof(double)), "state alloc");
+  CK(dev_malloc((void**)&h->vol_d, nU * sizeof(double)), "scratch alloc");
+  CK(dev_malloc((void**)&h->trace_d, nT * sizeof(double)), "scratch alloc");
+  CK(dev_malloc((void**)&h->flux_d, nT * sizeof(double)), "scratch alloc");
   CK(cudaMemset(h->U_d, 0, nU * sizeof(double)), "state clear");
   CK(cudaMemset(h->trace_d, 0, nT * sizeof(double)), "scratch clear");
   h->K = K;
   h->mixed = mixed_create(h->eq, o, K, h->M);
   if (h->mixed) {
     const size_t nTr = mixed_trace_floats(h->mixed, K + G);
-    CK(cudaMalloc((void**)&h->TU_d, nTr * sizeof(float)), "trace alloc");
-    CK(cudaMalloc((void**)&h->T0_d, nTr * sizeof(float)), "trace alloc");
-    CK(cudaMalloc((void**)&h->T1_d, nTr * sizeof(float)), "trace alloc");
+    CK(dev_malloc((void**)&h->TU_d, nTr * sizeof(float)), "trace alloc");
+    CK(dev_malloc((void**)&h->T0_d, nTr * sizeof(float)), "trace alloc");
+    CK(dev_malloc((void**)&h->T1_d, nTr * sizeof(float)), "trace alloc");
     CK(cudaMemset(h->TU_d, 0, nTr * sizeof(float)), "trace clear");
     CK(cudaMemset(h->T0_d, 0, nTr * sizeof(float)), "trace clear");
     CK(cudaMemset(h->T1_d, 0, nTr * sizeof(float)), "trace clear");
@@ -665,6 +684,19 @@ apollo_status set_mesh_impl(apollo_dg* h, int nverts, const double* vx, const do
     CK(upload(&h->halo_dst_d, dst.data(), dst.size()), "halo upload");
   }
   return APOLLO_OK;
+}
+
+// A mesh that fails part way (a bad element, a failed allocation) leaves the
+// handle with no mesh rather than a partial one.
+apollo_status set_mesh_impl(apollo_dg* h, int nverts, const double* vx, const double* vy, int Kg, const int* etov,
+                            const int* face_tag, const int* vert_canon, const int* part, int rank) {
+  const apollo_status r = set_mesh_body(h, nverts, vx, vy, Kg, etov, face_tag, vert_canon, part, rank);
+  if (r != APOLLO_OK && h) {
+    free_mesh(h);
+    h->K = 0;
+    h->have_state = false;
+  }
+  return r;
 }
 
 }  // namespace
@@ -892,6 +924,29 @@ apollo_status apollo_dg_integrals(apollo_dg* h, const double* U, int where, doub
   return APOLLO_OK;
 }
 
+apollo_status apollo_dg_energy(apollo_dg* h, const double* U, int where, double* sums) {
+  apollo_status r = check_ready(h);
+  if (r) return r;
+  if (!sums) return APOLLO_ERR_ARG;
+  const double* x = h->U_d;
+  if (U) {
+    if (where == APOLLO_DEVICE_PTR) {
+      x = U;
+    } else {
+      const size_t n = (size_t)h->K * h->ops.Np * h->M * sizeof(double);
+      CK(cudaMemcpyAsync(h->in_d, U, n, cudaMemcpyHostToDevice, h->stream), "energy input");
+      x = h->in_d;
+    }
+  }
+  CK(cudaMemsetAsync(h->st_d->sums, 0, sizeof(h->st_d->sums), h->stream), "energy");
+  DgDev d = make_dev(h);
+  CK(launch_energy(h->eq, d, x, h->mass_d, h->stream), "energy");
+  CK(cudaMemcpyAsync(h->st_h, h->st_d, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream), "energy");
+  CK(cudaStreamSynchronize(h->stream), "energy");
+  for (int f = 0; f < h->M; ++f) sums[f] = h->st_h->sums[f];
+  return APOLLO_OK;
+}
+
 apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int iters, double* ms, int* nk) {
   apollo_status r = check_whole(h);
   if (r) return r;
@@ -929,13 +984,13 @@ namespace {
 apollo_status ensure_deriv_buffers(apollo_dg* h) {
   if (h->dvol_d) return APOLLO_OK;
   const size_t nU = (size_t)h->K * h->ops.Np * h->M, nT = (size_t)h->K * h->ops.Nf * h->M;
-  CK(cudaMalloc((void**)&h->dvol_d, nU * sizeof(double)), "derivative scratch");
-  CK(cudaMalloc((void**)&h->dtrace_d, nT * sizeof(double)), "derivative scratch");
-  CK(cudaMalloc((void**)&h->dflux_d, nT * sizeof(double)), "derivative scratch");
-  CK(cudaMalloc((void**)&h->sbar_d, nT * sizeof(double)), "derivative scratch");
-  CK(cudaMalloc((void**)&h->tU_d, nU * sizeof(double)), "derivative state");
-  CK(cudaMalloc((void**)&h->tW_d, nU * sizeof(double)), "derivative state");
-  for (auto& p : h->A_d) CK(cudaMalloc((void**)&p, nU * sizeof(double)), "adjoint state");
+  CK(dev_malloc((void**)&h->dvol_d, nU * sizeof(double)), "derivative scratch");
+  CK(dev_malloc((void**)&h->dtrace_d, nT * sizeof(double)), "derivative scratch");
+  CK(dev_malloc((void**)&h->dflux_d, nT * sizeof(double)), "derivative scratch");
+  CK(dev_malloc((void**)&h->sbar_d, nT * sizeof(double)), "derivative scratch");
+  CK(dev_malloc((void**)&h->tU_d, nU * sizeof(double)), "derivative state");
+  CK(dev_malloc((void**)&h->tW_d, nU * sizeof(double)), "derivative state");
+  for (auto& p : h->A_d) CK(dev_malloc((void**)&p, nU * sizeof(double)), "adjoint state");
   return APOLLO_OK;
 }
 
@@ -1041,14 +1096,17 @@ namespace apollo {
 
 // Read-only view of a handle's discretisation for the no-allocation entry
 // point (dg_noalloc.cu); the scratch pointers are left for the caller to set.
-bool handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size_t* nU, size_t* nT) {
-  if (!h || h->eq < 0 || h->K == 0 || !h->peers.empty()) return false;
+const char* handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size_t* nU, size_t* nT) {
+  if (!h) return "null handle";
+  if (h->eq < 0) return "no equation set";
+  if (h->K == 0) return "no mesh set";
+  if (!h->peers.empty()) return "partitioned mesh with peers: use the staged calls (apollo_dg_stage_begin/end)";
   *d = make_dev(h);
   *eq = h->eq;
   *device = h->cfg.device;
   *nU = (size_t)h->K * h->ops.Np * h->M;
   *nT = (size_t)h->K * h->ops.Nf * h->M;
-  return true;
+  return nullptr;
 }
 
 void handle_set_error(apollo_dg* h, const char* msg) {
@@ -1063,7 +1121,7 @@ apollo_status handle_set_instances(apollo_dg* h, int ninst, const int* einst) {
   if (!h || h->K == 0 || ninst < 1) return APOLLO_ERR_ARG;
   DevState* st_d = nullptr;
   DevState* st_h = nullptr;
-  CK(cudaMalloc((void**)&st_d, (size_t)ninst * sizeof(DevState)), "instance states");
+  CK(dev_malloc((void**)&st_d, (size_t)ninst * sizeof(DevState)), "instance states");
   if (cudaMallocHost((void**)&st_h, (size_t)ninst * sizeof(DevState)) != cudaSuccess) {
     cudaFree(st_d);
     return fail(h, APOLLO_ERR_ALLOC, "instance states");
@@ -1157,6 +1215,18 @@ void handle_set_grid_div(apollo_dg* h, int div) {
 
 extern "C" {
 
+void apollo_dg_debug_fail_alloc(int n) { g_alloc_fail_in.store(n < 0 ? -1 : n); }
+
+apollo_status apollo_dg_debug_set_waits(apollo_dg* h, unsigned polls, int stall_first_wait) {
+  if (!h) return APOLLO_ERR_ARG;
+  h->wait_limit = polls;
+  h->debug_stall = stall_first_wait ? 1 : 0;
+  // the step graphs captured the old values
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return APOLLO_OK;
+}
+
 const char* apollo_dg_last_error(const apollo_dg* h) { return h ? h->err.c_str() : "null handle"; }
 
 apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, double dt, int checkpoint_every) {
@@ -1171,7 +1241,7 @@ apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, doubl
   const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
   while ((int)h->ckpt.size() < nck) {
     double* p = nullptr;
-    CK(cudaMalloc((void**)&p, nU * sizeof(double)), "checkpoint alloc");
+    CK(dev_malloc((void**)&p, nU * sizeof(double)), "checkpoint alloc");
     h->ckpt.push_back(p);
   }
   h->tr_valid = false;
@@ -1207,7 +1277,7 @@ apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* uba
   if (h->seg_steps < C) {
     dfree(h->seg_d);
     h->seg_steps = 0;
-    CK(cudaMalloc((void**)&h->seg_d, (size_t)5 * C * nU * sizeof(double)), "segment alloc");
+    CK(dev_malloc((void**)&h->seg_d, (size_t)5 * C * nU * sizeof(double)), "segment alloc");
     h->seg_steps = C;
   }
   auto S = [&](int j, int s) { return h->seg_d + ((size_t)j * 5 + s) * nU; };

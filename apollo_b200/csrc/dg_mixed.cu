@@ -357,6 +357,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   volatile int* abort_flag = (volatile int*)(sm + C::O_TSL + 4);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool x_bulk = flags & 1, u0_prefetch = flags & 2;
+  const uint32_t wlim = d.wait_limit ? d.wait_limit : (1u << 22);
   auto xs_buf = [&](int i) { return (double*)(sm + C::O_XS + (C::XS2 ? (i & 1) * C::SZ_XS : 0)); };
 
   // ---- once per CTA: operators split into tf32 halves (K-major)
@@ -473,7 +474,10 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     for (int i = 0; i < my_tiles && ok; ++i) {
       const int tile = tile_of(i);
       // GEMM-A once the workers have written the A operand
-      ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mbA, i & 1));  // warp-uniform
+      // (debug_stall: the first wait is on the drain barrier, which nothing
+      // completes before the abort path, so it runs out)
+      const uint32_t mb_a = (d.debug_stall && i == 0) ? mbDrain : mbA;
+      ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mb_a, i & 1, wlim));  // warp-uniform
       if (!ok) break;
       umma::fence_after_sync();
       if (lane == 0) {
@@ -492,7 +496,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       // the next state tile: its buffer is free once the operand build (single
       // buffer) or the epilogue two tiles back (two buffers) is done with it
       if (x_bulk && i + 1 < my_tiles) {
-        if (C::XS2 && i >= 1) ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mbE, (i - 1) & 1));
+        if (C::XS2 && i >= 1) ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mbE, (i - 1) & 1, wlim));
         if (!ok) break;
         if (lane == 0) issue_x(i + 1);
         x_issued++;
@@ -504,7 +508,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       // GEMM-B, chunk by chunk as the workers fill the ring
       for (int ch = 0; ch < C::NCH && ok; ++ch, ++cc) {
         const int b = cc % NBUF;
-        ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mb_full(b), (cc / NBUF) & 1));
+        ok = __all_sync(0xffffffffu, umma::mbar_wait_bounded(mb_full(b), (cc / NBUF) & 1, wlim));
         if (!ok) break;
         umma::fence_after_sync();
         if (lane == 0) {
@@ -565,7 +569,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       const double* XSb = xs_buf(i);
       int nx = 0;
       if (x_bulk) {
-        if (!umma::mbar_wait_bounded(mbX, i & 1)) {
+        if (!umma::mbar_wait_bounded(mbX, i & 1, wlim)) {
           *abort_flag = 1;  // no arrival: the control warp's wait times out as well
           return;
         }
@@ -711,7 +715,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     };
     // cubature deviations of tile i from TMEM to ST (warps by lane quadrant)
     auto stage = [&](int i) {
-      if (!umma::mbar_wait_bounded(mbD1, i & 1)) *abort_flag = 1;
+      if (!umma::mbar_wait_bounded(mbD1, i & 1, wlim)) *abort_flag = 1;
       umma::fence_after_sync();
       const int q = warp & 3, nwq = q < 3 ? 3 : 2;  // workers 0..10: three warps per quadrant, two for the last
 #pragma unroll 1
@@ -760,7 +764,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         const int b = cc % NBUF;
         const int rot = (int)((cc * 32u) % NW);
         const int wid = wtid >= rot ? wtid - rot : wtid + NW - rot;
-        if (cc >= NBUF && !umma::mbar_wait_bounded(mb_empty(b), ((cc / NBUF) - 1) & 1)) *abort_flag = 1;
+        if (cc >= NBUF && !umma::mbar_wait_bounded(mb_empty(b), ((cc / NBUF) - 1) & 1, wlim)) *abort_flag = 1;
         unsigned char* bh = RING + b * 2 * C::SZ_CH;
         unsigned char* bl = bh + C::SZ_CH;
         if (ch < NV && FIXED_E) {
@@ -851,7 +855,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
           // faces: Lax-Friedrichs flux of the stored traces, deviation from the
           // reference flux, times -sJ/J; column fc NG + g
           if constexpr (C::TRS) {
-            if (ch == NV && !(umma::mbar_wait_bounded(mbT, i & 1) && umma::mbar_wait_bounded(mbTP, i & 1)))
+            if (ch == NV && !(umma::mbar_wait_bounded(mbT, i & 1, wlim) && umma::mbar_wait_bounded(mbTP, i & 1, wlim)))
               *abort_flag = 1;
           }
           const int col0 = (ch - NV) * KV;
@@ -915,7 +919,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       const unsigned char* td = slot(i);
       const double* Rb = (const double*)(td + C::TD_RB);
       const double* Fb = (const double*)(td + C::TD_FB);
-      if (!umma::mbar_wait_bounded(mbD2, i & 1)) *abort_flag = 1;
+      if (!umma::mbar_wait_bounded(mbD2, i & 1, wlim)) *abort_flag = 1;
       umma::fence_after_sync();
       float dv[C::NPN];
 #pragma unroll
@@ -1039,6 +1043,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     if (warp == kMixThreads / 32 - 1) {
       if (lane == 0) umma::commit(mbDrain);
       __syncwarp();
+      // (the default limit: the drain must not give up while work is in flight)
       umma::mbar_wait_bounded(mbDrain, 0);
       if (x_issued > 0) umma::mbar_wait_bounded(mbX, (x_issued - 1) & 1);
     }

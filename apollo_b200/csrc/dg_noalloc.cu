@@ -11,14 +11,15 @@
 #include <atomic>
 #include <cstring>
 #include <mutex>
+#include <string>
 
 #include "apollo_dg.h"
 #include "dg_device.cuh"
 
 namespace apollo {
 
-// Reads the discretisation of a handle (dg_host.cpp).
-bool handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size_t* nU, size_t* nT);
+// Reads the discretisation of a handle (dg_host.cpp); returns why it cannot, or nullptr.
+const char* handle_device_view(const apollo_dg* h, DgDev* d, int* eq, int* device, size_t* nU, size_t* nT);
 void handle_set_error(apollo_dg* h, const char* msg);
 bool handle_has_limiter(const apollo_dg* h);
 
@@ -70,7 +71,10 @@ extern "C" apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt
     handle_set_error(h, "apollo_dg_rhs_noalloc: the handle has a limiter; use apollo_dg_rhs");
     return APOLLO_ERR_STATE;
   }
-  if (!handle_device_view(h, &d, &eq, &device, &nU, &nT)) return APOLLO_ERR_STATE;
+  if (const char* why = handle_device_view(h, &d, &eq, &device, &nU, &nT)) {
+    handle_set_error(h, (std::string("apollo_dg_rhs_noalloc: ") + why).c_str());
+    return APOLLO_ERR_STATE;
+  }
   const size_t need = kHeader + align256(nU * sizeof(double)) + 2 * align256(nT * sizeof(double));
   if (need > kScratchBytes) {
     handle_set_error(h, "apollo_dg_rhs_noalloc: this mesh needs more scratch than the 64 MiB static array; "
@@ -84,6 +88,15 @@ extern "C" apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt
     return APOLLO_ERR_CUDA;
   }
   cudaStream_t s = (cudaStream_t)stream;
+  if (suggested_dt) {
+    // the suggestion is read back after a wait on the stream, which a stream
+    // being captured does not allow
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      handle_set_error(h, "apollo_dg_rhs_noalloc: suggested_dt needs a stream the call can wait on; pass NULL");
+      return APOLLO_ERR_STATE;
+    }
+  }
   unsigned char* p = (unsigned char*)base;
   // per-call state starts at zero (wave-speed maximum, error word); the three
   // arrays are written in full by the kernels before they are read

@@ -10,7 +10,7 @@ this library's own layout.  It reads the Apollo source tree given on the
 command line and is run by hand when the tables change; the build uses the
 committed dg_tables.inc.
 
-    python apollo_b200/csrc/gen_tables.py /root/reference/src/lib > apollo_b200/csrc/dg_tables.inc
+    python apollo_b200/csrc/gen_tables.py $APOLLO_SRC/lib > apollo_b200/csrc/dg_tables.inc
 """
 import re
 import sys
@@ -78,5 +78,7 @@ def emit(rules, sets):
 
 
 if __name__ == "__main__":
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_tables.py <Apollo src/lib directory>   (e.g. $APOLLO_SRC/lib)")
     lib = sys.argv[1]
     sys.stdout.write(emit(cubature_rules(lib), node_sets(lib)))

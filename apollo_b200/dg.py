@@ -88,6 +88,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_get_time": (C.c_int, [H, _dp, _dp]),
         "apollo_dg_synchronize": (C.c_int, [H]),
         "apollo_dg_integrals": (C.c_int, [H, C.c_void_p, C.c_int, _dp]),
+        "apollo_dg_energy": (C.c_int, [H, C.c_void_p, C.c_int, _dp]),
         "apollo_dg_kernel_times": (C.c_int, [H, C.c_int, C.c_int, _dp, _ip]),
         "apollo_dg_rhs_noalloc": (C.c_int, [H, C.c_double, C.c_double, C.c_void_p, C.c_void_p, _dp, C.c_void_p]),
         "apollo_dg_forward_fixed": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_int]),
@@ -125,6 +126,8 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_stage_begin": (C.c_int, [H, C.c_int, C.c_int]),
         "apollo_dg_stage_end": (C.c_int, [H, C.c_int, C.c_int]),
         "apollo_dg_step_end": (C.c_int, [H]),
+        "apollo_dg_debug_set_waits": (C.c_int, [H, C.c_uint, C.c_int]),
+        "apollo_dg_debug_fail_alloc": (None, [C.c_int]),
         "apollo_dg_last_error": (C.c_char_p, [H]),
         "apollo_dg_destroy": (C.c_int, [H]),
     }
@@ -323,6 +326,16 @@ class NodalDG2d:
         else:
             p, where = _ptr(U)
             self._check(self.lib.apollo_dg_integrals(self.h, p, where, sums.ctypes.data_as(_dp)))
+        return sums
+
+    def square_integrals(self, U=None):
+        """Per-field integrals of U^2 over the mesh (apollo_dg_energy)."""
+        sums = np.zeros(self.m)
+        if U is None:
+            self._check(self.lib.apollo_dg_energy(self.h, None, 0, sums.ctypes.data_as(_dp)))
+        else:
+            p, where = _ptr(U)
+            self._check(self.lib.apollo_dg_energy(self.h, p, where, sums.ctypes.data_as(_dp)))
         return sums
 
     # ---- derivatives (float64; fixed step size dt) ------------------------------

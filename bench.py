@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-l2-500", action="store_true", help="skip the 500-step mixed vs float64 comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the advection (K = 1,922) and Maxwell TM (N = 5) configurations")
+    ap.add_argument("--maxwell-n", type=int, default=512, help="vertex grid of the Maxwell TM configuration")
+    ap.add_argument("--maxwell-steps", type=int, default=1000)
     ap.add_argument("--replicas", action="store_true",
                     help="N>1: independent replicas instead of one partitioned mesh")
     ap.add_argument("--partitioned", action="store_true",
@@ -62,6 +66,8 @@ def parse():
                     help="random directions of the adjoint's finite-difference check")
     ap.add_argument("--rhs-only", type=int, default=0,
                     help="profiling driver: set up the workload, run this many RHS evaluations, exit")
+    ap.add_argument("--steps-only", type=int, default=0,
+                    help="profiling driver: set up the workload, advance this many SSPRK steps, exit")
     return ap.parse_args()
 
 
@@ -80,6 +86,24 @@ def rhs_only(args):
     torch.cuda.synchronize()
     print(json.dumps({"rhs_only": args.rhs_only, "K": s.K, "precision": prec,
                       "checksum": float(out.abs().sum().item())}))
+    s.close()
+    return 0
+
+
+def steps_only(args):
+    """Set up the benchmark workload and advance it a few steps (for ncu: the
+    stepper's stage-mode launches)."""
+    import torch
+    from apollo_b200 import NodalDG2d, problems
+    p = problems.euler_vortex(n=args.n, N=args.order, fields=4)
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=0)
+    x, y = s.node_coords()
+    s.set_state(np.ascontiguousarray(p.ic(x, y)))
+    prec = "fp64" if args.precision == "auto" else args.precision
+    t, dt = s.advance(args.steps_only, 0.0, s.init_dt(), precision=prec)
+    torch.cuda.synchronize()
+    print(json.dumps({"steps_only": args.steps_only, "K": s.K, "precision": prec, "t": t,
+                      "checksum": float(np.abs(s.get_state()).sum())}))
     s.close()
     return 0
 
@@ -160,6 +184,154 @@ def adjoint_measure(args, device: int):
     }
     s.close()
     return out
+
+
+def _device_run(s, stream, U0, dt0, prec: str, steps: int, warmup: int = 3):
+    """ms for `steps` steps of the resident state from U0 at t = 0 (CUDA events on
+    the handle's stream, after `warmup` untimed steps from U0), and (t, dt)."""
+    import torch
+    s.set_state(U0)
+    s.advance(warmup, 0.0, dt0, precision=prec)
+    s.set_state(U0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        s.advance_async(steps, 0.0, dt0, precision=prec)
+        e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), s.time()
+
+
+def _cpu_rate(o, U, steps: int, threads: int):
+    """DOF-updates/s of the oracle on `threads` threads over `steps` steps of U
+    (advanced in place), and the seconds taken."""
+    o.set_threads(threads)
+    dt = o.init_dt(U)
+    t0 = time.perf_counter()
+    n, _, _ = o.run(U, steps, 0.0, dt)
+    return n, time.perf_counter() - t0
+
+
+def advection_measure(args, device: int, cpu: bool):
+    """Scalar advection by (1, 0.5) of the Gaussian exp(-r^2/0.01) on the periodic
+    unit square, jittered 32 x 32 vertex grid (K = 1,922), N = 3, CFL 0.5, 200
+    steps of the adaptive SSPRK(5,2) stepper: both GPU forms, the mixed form's
+    error against float64, and the CPU oracle on the same run (all host threads,
+    200 steps: its rate and the float64 GPU state's relative L2 against it) and
+    on one thread (a 10-step sample)."""
+    import torch
+    from apollo_b200 import NodalDG2d, problems
+    p = problems.advection(n=32, N=3)
+    stream = torch.cuda.Stream()
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=device, stream=stream.cuda_stream)
+    x, y = s.node_coords()
+    U0 = np.ascontiguousarray(p.ic(x, y))
+    s.set_state(U0)
+    dt0 = s.init_dt()
+    steps = 200
+    dofs = s.K * s.Np * s.m
+    out = {"config": {"workload": "advection_N3_K1922_200steps", "K": s.K, "N": p.N, "fields": 1,
+                      "velocity": [1.0, 0.5], "flux": "LF", "cfl": p.cfl, "steps": steps}}
+    ends = {}
+    for prec in ("fp64", "mixed"):
+        ms, (t, dt) = _device_run(s, stream, U0, dt0, prec, steps)
+        ends[prec] = s.get_state()
+        out[prec] = {"value": dofs * steps / (ms / 1000.0), "ms_per_step": ms / steps, "t_end": t}
+    out["l2_mixed_vs_fp64"] = float(np.linalg.norm(ends["mixed"] - ends["fp64"]) / np.linalg.norm(ends["fp64"]))
+    if cpu:
+        from oracle import oracle as orc
+        threads = os.cpu_count() or 1
+        o = orc.Oracle(p.mesh, p.N, orc.EQ_ADVECTION, p.eq_params, cfl=p.cfl)
+        Uc = U0.copy()
+        n, el = _cpu_rate(o, Uc, steps, threads)
+        out["cpu_all_cores"] = {"value": dofs * n / el, "cores": threads, "steps": n, "seconds": el}
+        out["l2_fp64_gpu_vs_cpu_oracle"] = float(np.linalg.norm(ends["fp64"] - Uc) / np.linalg.norm(Uc))
+        n1, el1 = _cpu_rate(o, U0.copy(), 10, 1)
+        out["cpu_1_thread"] = {"value": dofs * n1 / el1, "cores": 1, "steps": n1, "seconds": el1}
+    s.close()
+    return out
+
+
+def maxwell_measure(args, device: int, cpu: bool):
+    """Maxwell TM cavity (Ez, Bx, By; c = 1) on the unit square with Apollo's
+    mirror wall condition (maxwellTransverseMagneticBC), jittered 512 x 512
+    vertex grid (K = 522,242), N = 5, CFL 0.5, 1000 steps from the mode
+    Ez = sin(pi x) sin(pi y): both GPU forms (their device time over the 1000
+    steps), the drift of the energy 1/2 int (Ez^2 + Bx^2 + By^2) dA, the
+    relative L2 error against the exact mode at the time reached, the mixed form
+    against float64; the CPU oracle's rate on bounded samples (one step of the
+    same physics on a 128 x 128 grid on all host threads, one step on a 48 x 48
+    grid on one thread)."""
+    import torch
+    from apollo_b200 import NodalDG2d, problems
+    n = args.maxwell_n
+    p = problems.maxwell_tm(n=n, N=5)
+    stream = torch.cuda.Stream()
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, bcs=p.bcs, device=device,
+                  stream=stream.cuda_stream)
+    x, y = s.node_coords()
+    U0 = np.ascontiguousarray(p.ic(x, y))
+    s.set_state(U0)
+    dt0 = s.init_dt()
+    steps = args.maxwell_steps
+    dofs = s.K * s.Np * s.m
+    e0 = 0.5 * float(np.sum(s.square_integrals(U0)))
+    out = {"config": {"workload": f"maxwell_tm_N5_K{s.K}_{steps}steps", "K": s.K, "N": p.N, "fields": 3,
+                      "bc": "maxwellTransverseMagneticBC (PEC)", "flux": "LF", "cfl": p.cfl, "steps": steps},
+           "energy_0": e0}
+    ends = {}
+    for prec in ("fp64", "mixed"):
+        ms, (t, dt) = _device_run(s, stream, U0, dt0, prec, steps, warmup=2)
+        U = s.get_state()
+        ends[prec] = U
+        ex = p.exact(x, y, t)
+        e1 = 0.5 * float(np.sum(s.square_integrals(U)))
+        out[prec] = {"value": dofs * steps / (ms / 1000.0), "ms_per_step": ms / steps, "t_end": t,
+                     "energy_drift_rel": (e1 - e0) / e0,
+                     "l2_vs_exact_mode": float(np.linalg.norm(U - ex) / np.linalg.norm(ex))}
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["l2_mixed_vs_fp64"] = float(np.linalg.norm(ends["mixed"] - ends["fp64"]) / np.linalg.norm(ends["fp64"]))
+    if cpu:
+        from oracle import oracle as orc
+        threads = os.cpu_count() or 1
+        for key, ng, th in (("cpu_all_cores", 128, threads), ("cpu_1_thread", 48, 1)):
+            q = problems.maxwell_tm(n=ng, N=5)
+            o = orc.Oracle(q.mesh, q.N, orc.EQ_MAXWELL, (1.0, 0.0, 0.0), bcs=((orc.BC_TM, ()),), cfl=q.cfl)
+            xo, yo = o.node_coords()
+            U8 = np.zeros((q.mesh.K, o.Np, 8))
+            U8[..., 2:5] = q.ic(xo, yo)
+            nst, el = _cpu_rate(o, U8, 1, th)
+            out[key] = {"value": q.mesh.K * o.Np * 3 * nst / el, "cores": th, "steps": nst, "seconds": el,
+                        "sample": f"{nst} step on a {ng}x{ng} vertex grid (K={q.mesh.K}), N = 5, 8 Apollo fields"}
+    s.close()
+    return out
+
+
+def cpu_extra(threads: int):
+    """CPU oracle rates the single-GPU line reports beside its own numbers: the
+    Euler vortex at N = 4 on one thread (one step of a 64 x 64 grid), and the
+    float64 forward of the adjoint configuration (Euler vortex, N = 3, 128 x 128
+    grid, K = 32,258) on all host threads (two steps), with the 400-step forward
+    time that rate implies."""
+    from apollo_b200 import problems
+    from oracle import oracle as orc
+    res = {}
+    p = problems.euler_vortex(n=64, N=4, fields=5)
+    o = orc.Oracle(p.mesh, p.N, orc.EQ_EULER, p.eq_params, cfl=p.cfl)
+    x, y = o.node_coords()
+    n, el = _cpu_rate(o, np.ascontiguousarray(p.ic(x, y)), 1, 1)
+    res["euler_vortex_N4_cpu_1_thread"] = {"value": p.mesh.K * o.Np * 4 * n / el, "cores": 1, "steps": n,
+                                           "seconds": el, "sample": f"{n} step, 64x64 vertex grid (K={p.mesh.K})"}
+    p = problems.euler_vortex(n=128, N=3, fields=5)
+    o = orc.Oracle(p.mesh, p.N, orc.EQ_EULER, p.eq_params, cfl=p.cfl)
+    x, y = o.node_coords()
+    n, el = _cpu_rate(o, np.ascontiguousarray(p.ic(x, y)), 2, threads)
+    res["adjoint_config_cpu_forward"] = {"ms_per_step": 1000 * el / n, "forward_400_steps_s": 400 * el / n,
+                                         "cores": threads, "steps": n,
+                                         "sample": f"{n} steps, 128x128 vertex grid (K={p.mesh.K}), N = 3"}
+    return res
 
 
 def dist_env():
@@ -745,6 +917,17 @@ def ours_arm(args):
             extra["ensemble"] = ensemble_measure(args, local)
         except Exception as exc:  # reported, never hides the headline
             extra["ensemble"] = {"error": str(exc)}
+    if rank == 0 and world == 1 and not args.no_configs:
+        for key, fn in (("advection", advection_measure), ("maxwell_tm", maxwell_measure)):
+            try:
+                extra[key] = fn(args, local, cpu=not args.no_cpu_baseline)
+            except Exception as exc:  # reported, never hides the headline
+                extra[key] = {"error": str(exc)}
+        if not args.no_cpu_baseline:
+            try:
+                extra["cpu_extra"] = cpu_extra(os.cpu_count() or 1)
+            except Exception as exc:
+                extra["cpu_extra"] = {"error": str(exc)}
 
     if rank == 0:
         # our kernels per step: float64 5 x (volume, face, lift) + finalize;
@@ -775,6 +958,8 @@ def main():
     args = parse()
     if args.rhs_only:
         return rhs_only(args)
+    if args.steps_only:
+        return steps_only(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

@@ -202,6 +202,14 @@ apollo_status apollo_dg_synchronize(apollo_dg* h);
 /* Per-field sums of the element integrals of U (M J U summed), float64. */
 apollo_status apollo_dg_integrals(apollo_dg* h, const double* U, int where, double* sums);
 
+/* Per-field sums of the element integrals of U^2 (J u^T Mref u summed, with
+ * Mref = (V V^T)^-1 the reference mass matrix whose inverse Apollo keeps as VVT,
+ * src/lib/wxnodaldggeometry2d.cc:71-75), float64: the electromagnetic energy
+ * of the Maxwell TM fields is half the sum over Ez, Bx, By.  U as in
+ * apollo_dg_integrals (NULL: the resident state).  Apollo has no such sum; it
+ * serves the energy-drift check of the cavity mode. */
+apollo_status apollo_dg_energy(apollo_dg* h, const double* U, int where, double* sums);
+
 /* Diagnostics: average device time in milliseconds of each kernel of one
  * right-hand side, over `iters` evaluations of the resident state (CUDA events
  * on the handle's stream).  ms[0..2] = volume, face, LIFT + update.  *nk
@@ -210,7 +218,7 @@ apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int it
 
 /* The float64 right-hand side for callers that cannot allocate device memory
  * when they evaluate it (a host framework that owns all device memory through
- * its own allocator, code inside another library's stream capture, a loop that
+ * its own allocator and forbids allocations behind its back, or a loop that
  * must not take the device-wide synchronisation of cudaMalloc).  No counterpart
  * in Apollo.  Same result as apollo_dg_rhs with APOLLO_PREC_FP64 on device
  * pointers; the kernels' scratch (volume term, face traces, face fluxes) lives
@@ -219,7 +227,10 @@ apollo_status apollo_dg_kernel_times(apollo_dg* h, apollo_precision prec, int it
  * was built (and allocated) by apollo_dg_create / apollo_dg_set_mesh.
  *   in, out       device pointers [K][Np][m], distinct
  *   suggested_dt  may be NULL; when given, the call waits for the stream and
- *                 reports non-physical states and NaN like apollo_dg_rhs
+ *                 reports non-physical states and NaN like apollo_dg_rhs.
+ *                 With NULL the call does not wait and reports no such
+ *                 status: a NaN or non-physical state goes unreported, and
+ *                 the next call clears the evidence
  *   stream        cudaStream_t to run on (NULL: the legacy default stream)
  * Meshes whose scratch exceeds 64 MiB ((Np + 6 (N + 1) * 2) * m * 8 bytes per
  * element, about 28,000 elements at N = 4 with 4 fields) are rejected with
@@ -393,6 +404,22 @@ apollo_status apollo_dg_dist_start(apollo_dg* h, double t, double dt, apollo_pre
 apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision prec);
 apollo_status apollo_dg_stage_end(apollo_dg* h, int stage, apollo_precision prec);
 apollo_status apollo_dg_step_end(apollo_dg* h);
+
+/* Test hook for the failure path of the mixed-precision stage kernel (no
+ * counterpart in Apollo).  polls: how many polls a bounded device wait makes
+ * before it gives up (0 restores the default, about 2 s); stall_first_wait != 0
+ * points the kernel's first wait at a barrier that nothing completes, so the
+ * wait runs out, the kernel drains its tensor-core work and copies, frees its
+ * tensor memory and returns, and the call reports APOLLO_ERR_TIMEOUT.  No GPU
+ * fault is involved; the handle stays usable once the switch is cleared. */
+apollo_status apollo_dg_debug_set_waits(apollo_dg* h, unsigned polls, int stall_first_wait);
+
+/* Test hook for allocation failures (no counterpart in Apollo): the n-th
+ * device allocation the library makes from now on, counting from 0 and over
+ * all handles of the process, fails as if the device were out of memory (the
+ * call reports APOLLO_ERR_ALLOC; a mesh that fails leaves its handle with no
+ * mesh).  n < 0 switches the hook off. */
+void apollo_dg_debug_fail_alloc(int n);
 
 /* Error text of the last failing call on this handle. */
 const char* apollo_dg_last_error(const apollo_dg* h);

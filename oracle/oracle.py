@@ -31,10 +31,26 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
+def reference_src() -> str:
+    """Apollo's source tree (its ``src`` directory): ``$APOLLO_SRC`` where set,
+    else the default of the build recipe (oracle/Makefile, ``make print-src``).
+    The tree is only read to build the reference plugins and by the tests that
+    parse Apollo's example inputs; nothing needs it at run time."""
+    src = os.environ.get("APOLLO_SRC")
+    if src:
+        return src
+    out = subprocess.run(["make", "-s", "-C", HERE, "print-src"], capture_output=True, text=True)
+    return out.stdout.strip()
+
+
+def have_reference() -> bool:
+    return os.path.isdir(reference_src())
+
+
 def build(with_ref: bool = True) -> None:
     """Compile the oracle (and the reference plugins where the source exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    src = os.environ.get("APOLLO_SRC", "/root/reference/src")
+    src = reference_src()
     if with_ref and os.path.isdir(src):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"APOLLO_SRC={src}"], check=True)
 

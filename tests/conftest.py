@@ -23,5 +23,5 @@ def gpu_available() -> bool:
 @pytest.fixture(scope="session")
 def oracle_lib():
     from oracle import oracle as orc
-    orc.build(with_ref=os.path.isdir(os.environ.get("APOLLO_SRC", "/root/reference/src")))
+    orc.build(with_ref=orc.have_reference())
     return orc

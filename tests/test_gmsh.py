@@ -12,7 +12,9 @@ from apollo_b200.mesh import jittered_square
 from golden_cases import load
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_EXAMPLES = os.path.join(os.environ.get("APOLLO_SRC", "/root/reference/src"), "..", "examples", "unstructuredDG")
+from oracle.oracle import reference_src
+
+REF_EXAMPLES = os.path.join(reference_src(), "..", "examples", "unstructuredDG")
 
 
 def test_round_trip_keeps_mesh_and_side_tags(tmp_path):

@@ -26,7 +26,7 @@ def _noalloc(s, t, dt, u, out, stream):
     return rc, sugg.value
 
 
-@pytest.mark.parametrize("name", [n for n in NAMES if n.startswith(("euler", "maxwell"))])
+@pytest.mark.parametrize("name", NAMES)
 def test_noalloc_matches_rhs_twice(name):
     torch = pytest.importorskip("torch")
     g = load(name)
@@ -82,3 +82,21 @@ def test_noalloc_rejects_oversized_mesh():
     rc, _ = _noalloc(s, 0.0, 0.0, u, out, torch.cuda.current_stream().cuda_stream)
     assert rc == 8  # APOLLO_ERR_ARG
     assert b"64 MiB" in s.lib.apollo_dg_last_error(s.h)
+
+
+def test_noalloc_refusals_say_why():
+    """A handle without a mesh is refused with its reason in the error text."""
+    torch = pytest.importorskip("torch")
+    from apollo_b200.dg import _Config, load_library
+    lib = load_library()
+    cfg = _Config(3, 0.5, 0, None)
+    h = C.c_void_p()
+    assert lib.apollo_dg_create(C.byref(cfg), C.byref(h)) == 0
+    try:
+        u = torch.zeros(16, dtype=torch.float64, device="cuda")
+        rc = lib.apollo_dg_rhs_noalloc(h, 0.0, 0.0, C.c_void_p(u.data_ptr()), C.c_void_p(u.data_ptr()), None,
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 7  # APOLLO_ERR_STATE
+        assert b"no equation set" in lib.apollo_dg_last_error(h)
+    finally:
+        lib.apollo_dg_destroy(h)
