@@ -234,9 +234,11 @@ apollo_status check_whole(apollo_dg* h) {
 }
 
 apollo_status read_errors(apollo_dg* h) {
+  // a stage that gave up wrote no result, so whatever the later stages of the
+  // step flagged on that input says nothing: the timeout is reported first
+  if (h->st_h->err & ERRB_TIMEOUT) return fail(h, APOLLO_ERR_TIMEOUT, "device wait timed out");
   if (h->st_h->err & ERRB_NONPHYS) return fail(h, APOLLO_ERR_NONPHYSICAL, "negative density or pressure in the Euler flux");
   if (h->st_h->err & ERRB_NAN) return fail(h, APOLLO_ERR_NAN, "NaN in the right-hand side");
-  if (h->st_h->err & ERRB_TIMEOUT) return fail(h, APOLLO_ERR_TIMEOUT, "device wait timed out");
   return APOLLO_OK;
 }
 
