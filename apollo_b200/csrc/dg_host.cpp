@@ -458,7 +458,7 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name) {
 }
 
 apollo_status apollo_dg_set_launch_shape(apollo_dg* h, int grid_share, int tile_shape) {
-  if (!h || grid_share < 1 || tile_shape < 0 || tile_shape > 1) return APOLLO_ERR_ARG;
+  if (!h || grid_share < 1 || tile_shape < 0 || tile_shape > 2) return APOLLO_ERR_ARG;
   handle_set_grid_div(h, grid_share);
   handle_set_tile_shape(h, tile_shape);
   return APOLLO_OK;
@@ -1197,7 +1197,7 @@ apollo_status handle_prepare_step(apollo_dg* h, apollo_precision prec) {
 }
 apollo_status handle_read_errors(apollo_dg* h) { return read_errors(h); }
 void handle_set_tile_shape(apollo_dg* h, int shape) {
-  shape = shape == 1 ? 1 : 0;
+  shape = (shape >= 0 && shape <= 2) ? shape : 0;
   if (shape != h->tile_shape) {
     h->tile_shape = shape;
     for (auto& g : h->graph)

@@ -1055,6 +1055,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   if (warp == 0) umma::tmem_dealloc(tb, C::TCOLS);
 }
 
+#include "dg_mixed_fused.cuh"
+
 // Face traces [K][3][TS] of a state.  A block of 128 threads takes 128 / M
 // elements: their states, one contiguous range of x, are read into shared
 // memory with coalesced loads (at most NP per thread, all in flight at once),
@@ -1160,6 +1162,55 @@ cudaError_t launch_mixed_sh(MixedPlan* p, const DgDev& d, const StageArgs& a0, c
   }
 }
 
+// the fused form (dg_mixed_fused.cuh): four-field Euler, Lax-Friedrichs, orders 2..4
+template <int EQ, int N>
+cudaError_t launch_fused(MixedPlan* p, const DgDev& d, const StageArgs& a0, cudaStream_t s, cudaEvent_t* ev) {
+  using C = FusedCfg<N>;
+  if constexpr (!C::FITS) {
+    return cudaErrorNotSupported;
+  } else {
+    static unsigned configured = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured & (1u << (dev & 31)))) {
+      cudaError_t e = cudaFuncSetAttribute(k_mixed_fused<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::BYTES);
+      if (e != cudaSuccess) return e;
+      configured |= 1u << (dev & 31);
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (d.grid_div > 1) sms = (sms + d.grid_div - 1) / d.grid_div;
+    const int ntiles = (d.K + C::E - 1) / C::E;
+    int grid = sms;
+    if (grid > ntiles) grid = ntiles;
+    StageArgs a = a0;
+    if (a.reset_lambda && a.mode != MODE_STAGE) {
+      cudaError_t e = launch_reset_lambda(d, s);
+      if (e != cudaSuccess) return e;
+    }
+    if (ev) cudaEventRecord(ev[0], s);
+    if (a.mode == MODE_RHS) {
+      if (!a.tr_scratch) return cudaErrorInvalidValue;
+      cudaError_t e = launch_traces_t<N, 4>(d, a.x, a.tr_scratch, s);
+      if (e != cudaSuccess) return e;
+      a.tr_in = a.tr_scratch;
+      a.tr_out = nullptr;
+    }
+    if (!a.tr_in) return cudaErrorInvalidValue;
+    // the trace bulk stores need a 16-byte aligned destination
+    if (a.tr_out && ((uintptr_t)a.tr_out & 15)) return cudaErrorInvalidValue;
+    if (ev) cudaEventRecord(ev[1], s);
+    const int flags = (((uintptr_t)a.x & 15) == 0 ? 1 : 0) |
+                      (a.mode == MODE_FINAL && ((uintptr_t)a.u0 & 15) == 0 ? 2 : 0);
+    k_mixed_fused<EQ, N><<<grid, kFusedThreads, C::BYTES, s>>>(d, a, p->rowsum, flags);
+    if (ev) {
+      cudaEventRecord(ev[2], s);
+      cudaEventRecord(ev[3], s);
+    }
+    return cudaGetLastError();
+  }
+}
+
 // the second chunk shape for the Euler kinds (the batched ensembles' equations)
 template <int EQ, int N>
 cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a, cudaStream_t s, cudaEvent_t* ev) {
@@ -1167,9 +1218,14 @@ cudaError_t launch_mixed_t(MixedPlan* p, const DgDev& d, const StageArgs& a, cud
     // Apollo's other Euler numerical fluxes: their own instantiation
     if ((int)d.eqp.p[3] != NF_LF) return launch_mixed_sh<EQ, N, 0, true>(p, d, a, s, ev);
   }
+  if constexpr (EQ == EQ_EULER2D && N <= 4 && FusedCfg<N>::FITS) {
+    if (d.tile_shape == 0) return launch_fused<EQ, N>(p, d, a, s, ev);
+  }
   if constexpr ((EQ == EQ_EULER || EQ == EQ_EULER2D) && MixCfg<N, Eq<EQ>::M, 1>::FITS) {
     if (d.tile_shape == 1) return launch_mixed_sh<EQ, N, 1>(p, d, a, s, ev);
   }
+  // tile_shape 2 (and 0 where the fused form does not apply): the chunked
+  // kernel with 24-column chunks
   return launch_mixed_sh<EQ, N, 0>(p, d, a, s, ev);
 }
 

@@ -71,10 +71,11 @@ template <int N> struct FusedCfg {
   static constexpr int TD_P0 = TD_QF + M * E * 4;         // [5M][E] float references
   static constexpr int TD_RB = round_up_c(TD_P0 + 5 * M * E * 4, 8);  // [2M][E] double
   static constexpr int TD_FB = TD_RB + 2 * M * E * 8;     // [3M][E] double
-  static constexpr int TD_G64 = TD_FB + 3 * M * E * 8;    // [13][E] double
-  static constexpr int TD_XB = TD_G64 + 13 * E * 8;       // [128] double result means
+  static constexpr int TD_XB = TD_FB + 3 * M * E * 8;     // [128] double means (state, then result)
   static constexpr int TD_PS = TD_XB + 128 * 8;           // [4][128] double partial sums
-  static constexpr int SZ_TD = TD_PS + 4 * 128 * 8;
+  static constexpr int TD_GT = round_up_c(TD_PS + 4 * 128 * 8, 16);  // [E] ElemGeo of the tile (bulk copy)
+  static constexpr int TD_CT = TD_GT + E * (int)sizeof(ElemGeo);     // [E][6] int connectivity (bulk copy)
+  static constexpr int SZ_TD = TD_CT + E * 6 * 4 + 16;
   // layout
   static constexpr int O_A2 = 0;                                   // hi, lo
   static constexpr int O_B2 = O_A2 + 2 * SZ_A2;
@@ -82,19 +83,23 @@ template <int N> struct FusedCfg {
   static constexpr int O_B1 = O_A1 + 2 * SZ_A1;                    // hi, lo
   static constexpr int O_B3 = O_B1 + 2 * SZ_B1;                    // hi, lo
   static constexpr int O_XS = round_up_c(O_B3 + 2 * SZ_B3, 16);
-  static constexpr int O_SCR = O_XS + SZ_XS;
+  // the state tile is staged in shared memory (one bulk copy, prefetched a
+  // tile ahead) where it fits; otherwise the operand build reads it directly
+  static constexpr int FIXED = O_XS + SZ_SCR + NP * 5 * 8 + SZ_TD + 128;
+  static constexpr int LIMIT = 227 * 1024;
+  static constexpr bool XSM = FIXED + SZ_XS <= LIMIT;
+  static constexpr int O_SCR = O_XS + (XSM ? SZ_XS : 0);
   static constexpr int O_RS = O_SCR + SZ_SCR;                      // [NP][5] double row sums
   static constexpr int O_TD = round_up_c(O_RS + NP * 5 * 8, 16);
-  static constexpr int O_MB = round_up_c(O_TD + SZ_TD, 8);         // mbarriers: x, D1, D2, D3, drain
+  static constexpr int O_MB = round_up_c(O_TD + SZ_TD, 8);         // mbarriers: x, D1, D2, D3, drain, geometry
   static constexpr int O_TSL = O_MB + 8 * 8;                       // TMEM base, abort flag
   static constexpr int BYTES = O_TSL + 16;
-  static constexpr int LIMIT = 227 * 1024;
-  static constexpr bool FITS = BYTES <= LIMIT;
   static constexpr int T_D1 = 0, T_D2 = NC16, T_D3 = 0;
   static constexpr int TCOLS = tmem_cols(NC16 + 2 * NPN);
-  static_assert(NFN <= NC16 || N == 2, "the trace accumulator reuses the cubature columns");
-  static_assert(SZ_TR <= SZ_A2, "the trace staging reuses the A2 hi half");
-  static_assert(NC16 / 16 <= 4, "four warps of a quarter cover the cubature columns");
+  // the form applies where shared memory holds it, the four warps of a quarter
+  // cover the cubature columns, the trace accumulator fits in the cubature
+  // columns and the trace staging in the A2 hi half
+  static constexpr bool FITS = BYTES <= LIMIT && NC16 / 16 <= 4 && NFN <= NC16 && SZ_TR <= SZ_A2;
 };
 
 template <int EQ, int N>
@@ -124,17 +129,18 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   float* P0 = (float*)(td + C::TD_P0);
   double* RB = (double*)(td + C::TD_RB);
   double* FB = (double*)(td + C::TD_FB);
-  double* G64 = (double*)(td + C::TD_G64);
+  const ElemGeo* GT = (const ElemGeo*)(td + C::TD_GT);
+  const int* CT = (const int*)(td + C::TD_CT);
   double* XB = (double*)(td + C::TD_XB);
   double* PS = (double*)(td + C::TD_PS);
   uint64_t* mbar = (uint64_t*)(sm + C::O_MB);
   uint32_t* tslot = (uint32_t*)(sm + C::O_TSL);
   volatile int* abort_flag = (volatile int*)(sm + C::O_TSL + 4);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const bool x_bulk = flags & 1, u0_prefetch = flags & 2;
+  const bool x_bulk = C::XSM && (flags & 1), u0_prefetch = flags & 2;
   const uint32_t wlim = d.wait_limit ? d.wait_limit : (1u << 22);
   const uint32_t mbX = umma::smem_u32(mbar + 0), mbD1 = umma::smem_u32(mbar + 1), mbD2 = umma::smem_u32(mbar + 2),
-                 mbD3 = umma::smem_u32(mbar + 3), mbDrain = umma::smem_u32(mbar + 4);
+                 mbD3 = umma::smem_u32(mbar + 3), mbDrain = umma::smem_u32(mbar + 4), mbG = umma::smem_u32(mbar + 5);
 
   // ---- once per CTA: operators split into tf32 halves (K-major), zeroed operands
   for (int i = tid; i < C::NC16 * K1; i += kFusedThreads) {
@@ -178,7 +184,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   for (int i = tid; i < 2 * C::SZ_A1 / 16; i += kFusedThreads) ((float4*)A1h)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int i = tid; i < NP * 5; i += kFusedThreads) RSUM[i] = rowsum[i];
   if (tid == 0) {
-    for (int b = 0; b < 5; ++b) umma::mbar_init(umma::smem_u32(mbar + b), 1);
+    for (int b = 0; b < 6; ++b) umma::mbar_init(umma::smem_u32(mbar + b), 1);
     *abort_flag = 0;
   }
   if (warp == 0) umma::tmem_alloc(umma::smem_u32(tslot), C::TCOLS);
@@ -196,11 +202,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     const int ne = min(E, d.K - tile * E);
     return ((ne * NP * M * 8) & ~15) / 8;
   };
-  auto issue_x = [&](int i) {  // thread 0
+  auto issue_x = [&](int i) {  // thread 0: the state tile into XS
     const int tile = tile_of(i);
     const uint32_t bytes = (uint32_t)x_doubles(tile) * 8u;
     umma::mbar_expect_tx(mbX, bytes);
     umma::bulk_g2s(umma::smem_u32(XS), a.x + (size_t)tile * E * NP * M, bytes, mbX);
+  };
+  auto issue_geo = [&](int i) {  // thread 0: geometry and connectivity of tile i into GT, CT
+    const int k0 = tile_of(i) * E, ne = min(E, d.K - k0);
+    const uint32_t gb = (uint32_t)(ne * (int)sizeof(ElemGeo));  // a multiple of 16
+    // (rounded up to 16 bytes: the connectivity array has 16 bytes of slack)
+    const uint32_t cb = (uint32_t)((ne * 24 + 15) & ~15);
+    umma::mbar_expect_tx(mbG, gb + cb);
+    umma::bulk_g2s(umma::smem_u32(GT), d.geo + k0, gb, mbG);
+    umma::bulk_g2s(umma::smem_u32(CT), d.conn + (size_t)k0 * 6, cb, mbG);
   };
   auto wait = [&](uint32_t mb, uint32_t parity) {
     if (!umma::mbar_wait_bounded(mb, parity, wlim)) *abort_flag = 1;
@@ -225,85 +240,102 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   // this thread's row in the TMEM quarter of its warp: element e_q (0..7 in the
   // quarter), field f; the warp's sub-index g = warp / 4 splits the columns
   const int q = warp & 3, g4 = warp >> 2, f_me = lane & 3, e_me = 8 * q + (lane >> 2);
-  const int r_me = 32 * q + lane;  // = 4 e_me + f_me
   const uint32_t tlane = tb + ((uint32_t)(32 * q) << 16);
   float* scr = (float*)(sm + C::O_SCR) + warp * (8 * 20);  // this warp's exchange block
   const int eq_w = lane >> 2;                               // element within the warp's block
+  // the operand build and the epilogue: thread (row, node group); it keeps its
+  // four state values in registers from the one to the other
+  const int r_ep = tid & 127, ng_ep = tid >> 7, e_ep = r_ep >> 2, f_ep = r_ep & 3;
+  const bool node_thread = ng_ep < C::NGRP;
   const bool want_lambda = a.mode != MODE_STAGE;
   const bool write_traces = a.tr_out != nullptr && a.mode != MODE_RHS;
   LamAcc lam_acc;
   int err = 0;
   bool ok = true;
-  int x_issued = 0;
+  int x_issued = 0, g_issued = 0;
   auto stage_t = [&](int k) {
     const DevState& S = d.st[inst_of(d, k)];
     return a.time_from_state ? S.t + S.dt * a.frac : a.t_arg;
   };
   auto stage_dt = [&](int k) { return a.time_from_state ? d.st[inst_of(d, k)].dt : a.dt_arg; };
+  // this thread's state values of tile i straight from global memory (no
+  // shared-memory state tile)
+  double xv[4] = {0.0, 0.0, 0.0, 0.0};
+  auto load_x = [&](int i) {
+    const int k0 = tile_of(i) * E, ne = min(E, d.K - k0);
+    const double* xg = a.x + (size_t)k0 * NP * M;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int j = 4 * ng_ep + u;
+      xv[u] = (node_thread && e_ep < ne && j < NP) ? xg[(e_ep * NP + j) * M + f_ep] : 0.0;
+    }
+  };
 
-  if (tid == 0 && x_bulk && my_tiles > 0) {
-    issue_x(0);
-    x_issued = 1;
+  if (tid == 0 && my_tiles > 0) {
+    issue_geo(0);
+    g_issued = 1;
+    if (x_bulk) {
+      issue_x(0);
+      x_issued = 1;
+    }
   }
+  if (!x_bulk && my_tiles > 0) load_x(0);
   for (int i = 0; i < my_tiles && ok; ++i) {
     const int tile = tile_of(i), k0 = tile * E, ne = min(E, d.K - k0);
     const uint32_t par = i & 1;
-    // ---------------- S0: operand build
+    // ---------------- S0: operand build (one warp waits for the copies)
+    if (warp == 0) {
+      wait(mbG, par);
+      if (x_bulk) wait(mbX, par);
+    }
+    all_sync();
     {
-      int nx = 0;
-      if (x_bulk) {
-        // (the stall switch of the failure tests points this first wait at a
-        // barrier that nothing completes before the abort path)
-        wait((d.debug_stall && i == 0) ? mbDrain : mbX, par);
-        nx = x_doubles(tile);
-      }
-      const double* xg = a.x + (size_t)k0 * NP * M;
-      if (tid < 128 * C::NGRP) {
-        const int r = tid / C::NGRP, grp = tid % C::NGRP, e = r >> 2, f = r & 3;
-        const bool valid = e < ne;
-        double v[4];
+      double v[4];
+      if (node_thread) {
+        const bool valid = e_ep < ne;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const int j = 4 * grp + u, idx = (e * NP + j) * M + f;
-          v[u] = (valid && j < NP) ? (idx < nx ? XS[idx] : xg[idx]) : 0.0;
+          const int j = 4 * ng_ep + u;
+          v[u] = (valid && j < NP) ? (x_bulk ? XS[(e_ep * NP + j) * M + f_ep] : xv[u]) : 0.0;
+          xv[u] = v[u];  // kept for the epilogue
         }
-        double sum = (v[0] + v[1]) + (v[2] + v[3]);
+        PS[ng_ep * 128 + r_ep] = (v[0] + v[1]) + (v[2] + v[3]);
+      }
+      if (tid >= kFusedThreads - E) {
+        // fp32 geometry and connectivity of the tile
+        const int e = tid - (kFusedThreads - E);
+        const bool valid = e < ne;
+        const ElemGeo& gg = GT[e];
+        GEO[0 * E + e] = valid ? (float)gg.rx : 0.f;
+        GEO[1 * E + e] = valid ? (float)gg.ry : 0.f;
+        GEO[2 * E + e] = valid ? (float)gg.sx : 0.f;
+        GEO[3 * E + e] = valid ? (float)gg.sy : 0.f;
 #pragma unroll
-        for (int w = 1; w < C::NGRP; w *= 2) sum = sum + __shfl_xor_sync(0xffffffffu, sum, w);
-        const double qbar = sum * (1.0 / NP);
+        for (int fc = 0; fc < 3; ++fc) {
+          GEO[(4 + fc) * E + e] = valid ? (float)gg.nx[fc] : 0.f;
+          GEO[(7 + fc) * E + e] = valid ? (float)gg.ny[fc] : 0.f;
+          GEO[(10 + fc) * E + e] = valid ? (float)(-gg.sJ[fc] * gg.invJ) : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < 6; ++j) CN[e * 6 + j] = valid ? CT[e * 6 + j] : 0;
+      }
+      all_sync();
+      if (node_thread) {
+        // the nodal mean in the fixed order of the mean tree
+        double s01 = PS[0 * 128 + r_ep] + PS[1 * 128 + r_ep];
+        if (C::NGRP > 2) s01 = s01 + (PS[2 * 128 + r_ep] + PS[3 * 128 + r_ep]);
+        const double qbar = s01 * (1.0 / NP);
+        const bool valid = e_ep < ne;
         float hv[4], lv[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const float xv = (valid && 4 * grp + u < NP) ? (float)(v[u] - qbar) : 0.f;
-          split_tf32(xv, hv[u], lv[u]);
+          const float xd = (valid && 4 * ng_ep + u < NP) ? (float)(v[u] - qbar) : 0.f;
+          split_tf32(xd, hv[u], lv[u]);
         }
-        const uint32_t off = umma::kmajor_offset_sbo(r, grp * 4, C::SBO1);
+        const uint32_t off = umma::kmajor_offset_sbo(r_ep, ng_ep * 4, C::SBO1);
         *(float4*)(A1h + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
         *(float4*)(A1l + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
-        if (grp == 0) QF[f * E + e] = valid ? (float)qbar : 0.f;
-      }
-      if (tid >= kFusedThreads - E) {
-        const int e = tid - (kFusedThreads - E);
-        if (e < ne) {
-          const int k = k0 + e;
-#pragma unroll
-          for (int j = 0; j < 6; ++j) CN[e * 6 + j] = d.conn[(size_t)k * 6 + j];
-          const ElemGeo& gg = d.geo[k];
-          G64[0 * E + e] = gg.rx; G64[1 * E + e] = gg.ry; G64[2 * E + e] = gg.sx; G64[3 * E + e] = gg.sy;
-#pragma unroll
-          for (int fc = 0; fc < 3; ++fc) {
-            G64[(4 + fc) * E + e] = gg.nx[fc];
-            G64[(7 + fc) * E + e] = gg.ny[fc];
-            G64[(10 + fc) * E + e] = -gg.sJ[fc] * gg.invJ;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 13; ++j) G64[j * E + e] = 0.0;
-#pragma unroll
-          for (int j = 0; j < 6; ++j) CN[e * 6 + j] = 0;
-        }
-#pragma unroll
-        for (int j = 0; j < 13; ++j) GEO[j * E + e] = (float)G64[j * E + e];
+        if (ng_ep == 0) QF[f_ep * E + e_ep] = valid ? (float)qbar : 0.f;
       }
       umma::fence_proxy_async();
       all_sync();
@@ -329,6 +361,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       // reference fluxes at the fp32 mean (volume + three faces per element)
       const int kind = tid / E, e = tid % E;
       if (e < ne) {
+        const ElemGeo& gg = GT[e];
         float qc[M];
 #pragma unroll
         for (int f = 0; f < M; ++f) qc[f] = QF[f * E + e];
@@ -341,14 +374,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           for (int f = 0; f < M; ++f) {
             P0[f * E + e] = R0[f];
             P0[(M + f) * E + e] = S0[f];
-            RB[f * E + e] = G64[0 * E + e] * (double)F[f] + G64[1 * E + e] * (double)G[f];
-            RB[(M + f) * E + e] = G64[2 * E + e] * (double)F[f] + G64[3 * E + e] * (double)G[f];
+            RB[f * E + e] = gg.rx * (double)F[f] + gg.ry * (double)G[f];
+            RB[(M + f) * E + e] = gg.sx * (double)F[f] + gg.sy * (double)G[f];
           }
         } else {
           const int fc = kind - 1;
           float nf[M];
           Q::lf(d.eqp, GEO[(4 + fc) * E + e], GEO[(7 + fc) * E + e], qc, qc, nf, &err);
-          const double w = G64[(10 + fc) * E + e], nx = G64[(4 + fc) * E + e], ny = G64[(7 + fc) * E + e];
+          const double w = -gg.sJ[fc] * gg.invJ, nx = gg.nx[fc], ny = gg.ny[fc];
 #pragma unroll
           for (int f = 0; f < M; ++f) {
             P0[((2 + fc) * M + f) * E + e] = nf[f];
@@ -357,8 +390,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         }
       }
     }
-    all_sync();  // references visible
-    wait(mbD1, par);
+    // (the stall switch of the failure tests points the first tile's wait at a
+    // barrier that nothing completes before the abort path)
+    if (warp == kFusedThreads / 32 - 1) wait((d.debug_stall && i == 0) ? mbDrain : mbD1, par);
+    all_sync();  // references visible, cubature values in TMEM
     umma::fence_after_sync();
     // ---------------- S2: volume items.  Warp (q, g4) takes the cubature
     // columns [16 g4, 16 g4 + 16) of its quarter; per group of 4 points a
@@ -433,6 +468,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         umma::mma_tf32(tb + C::T_D2, dA2h + s * KSTEP, dB2 + s * KSTEP, idB, s > 0);
         umma::mma_tf32(tb + C::T_D2, dA2l + s * KSTEP, dB2 + s * KSTEP, idB, 1);
       }
+      // the next tile's geometry and connectivity: this tile's copies were
+      // read into GEO, CN and the reference fluxes before the last barrier
+      if (i + 1 < my_tiles) {
+        issue_geo(i + 1);
+        g_issued++;
+      }
     }
     {
       // warp (q, g4) takes face column groups g4 and g4 + 4; the thread the
@@ -495,13 +536,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         umma::mma_tf32(tb + C::T_D2, dA2l + s * KSTEP, dB2 + s * KSTEP, idB, 1);
       }
       umma::commit(mbD2);
+      wait(mbD2, par);
     }
-    wait(mbD2, par);
+    all_sync();
     umma::fence_after_sync();
     // ---------------- S5: float64 epilogue; thread (row, node group)
     {
-      const int r = tid & 127, ng = tid >> 7, e = r >> 2, f = r & 3;
-      const bool active = ng < C::NGRP;
+      const int r = r_ep, ng = ng_ep, e = e_ep, f = f_ep;
+      const bool active = node_thread;
       const bool rvalid = active && e < ne && !*abort_flag;
       float vh[4], vl[4];
       if (active) {
@@ -517,16 +559,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         const double F0 = FB[(0 * M + f) * E + e], F1 = FB[(1 * M + f) * E + e], F2 = FB[(2 * M + f) * E + e];
         const double dt = stage_dt(k);
         const double c_stage = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
-        const double* xrow = a.x + (size_t)k * NP * M + f;
         const double* urow = a.u0 + (size_t)k * NP * M + f;
         double* orow = a.out + (size_t)k * NP * M + f;
-        double xr[4], ur[4];
+        double ur[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int n = 4 * ng + u;
-          if (n < NP && a.mode != MODE_RHS) xr[u] = xrow[n * M];
           if (n < NP && a.mode == MODE_FINAL) ur[u] = urow[n * M];
         }
+        const double* xr = xv;  // this thread's state values, read in the operand build
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int n = 4 * ng + u;
@@ -545,6 +586,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           if (n < NP) orow[n * M] = o[u];
         }
       }
+      // the next tile's state values: their loads overlap the rest of this tile
+      if (!x_bulk && i + 1 < my_tiles) load_x(i + 1);
       if (write_traces) {
         // the result's mean (the nodal-mean tree: groups of 4 nodes, then pairs)
         if (active) PS[ng * 128 + r] = (o[0] + o[1]) + (o[2] + o[3]);
@@ -575,9 +618,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       // ---------------- S6: the trace GEMM (D3 over the cubature columns)
       if (tid == 0) {
         umma::fence_after_sync();
-        // the previous tile's bulk store has read its staging (A2 hi) long ago;
-        // make sure before the traces are staged there again
-        umma::bulk_wait_read();
 #pragma unroll
         for (int s = 0; s < K1 / 8; ++s) {
           umma::mma_tf32(tb + C::T_D3, dA1h + s * KSTEP, dB3h + s * KSTEP, idC, s > 0);
@@ -586,7 +626,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         }
         umma::commit(mbD3);
       }
-      wait(mbD3, par);
+      if (warp == 0) wait(mbD3, par);
+      all_sync();
       umma::fence_after_sync();
       // ---------------- S7: traces = float(mean) + interpolated deviations
       {
@@ -631,8 +672,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     // let every issued MMA complete (a fresh barrier) and the state copy land
     if (tid == 0) {
       umma::commit(mbDrain);
-      umma::mbar_wait_bounded(mbDrain, (d.debug_stall ? 0u : 0u));
+      umma::mbar_wait_bounded(mbDrain, 0);
       if (x_issued > 0) umma::mbar_wait_bounded(mbX, (uint32_t)((x_issued - 1) & 1));
+      if (g_issued > 0) umma::mbar_wait_bounded(mbG, (uint32_t)((g_issued - 1) & 1));
       atomicOr(&d.st->err, ERRB_TIMEOUT);
     }
     umma::fence_before_sync();

@@ -128,6 +128,16 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_step_end": (C.c_int, [H]),
         "apollo_dg_debug_set_waits": (C.c_int, [H, C.c_uint, C.c_int]),
         "apollo_dg_debug_fail_alloc": (None, [C.c_int]),
+        "apollo_dg_deck_config": (C.c_int, [C.c_char_p, C.POINTER(_Config), C.c_char_p, C.c_int]),
+        "apollo_dg_deck_equation": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, _dp, _ip, C.c_char_p,
+                                              C.c_int, C.c_char_p, C.c_int]),
+        "apollo_dg_deck_bc": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, _ip, C.c_char_p, C.c_int, _dp, _ip,
+                                        C.c_char_p, C.c_int]),
+        "apollo_dg_deck_limiter": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, _dp, _ip, C.c_char_p,
+                                             C.c_int]),
+        "apollo_dg_set_equation_text": (C.c_int, [H, C.c_char_p, C.c_char_p]),
+        "apollo_dg_add_bc_text": (C.c_int, [H, C.c_char_p, C.c_char_p]),
+        "apollo_dg_set_limiter_text": (C.c_int, [H, C.c_char_p, C.c_char_p]),
         "apollo_dg_last_error": (C.c_char_p, [H]),
         "apollo_dg_destroy": (C.c_int, [H]),
     }
@@ -161,19 +171,27 @@ def _ptr(a, sync: bool = True):
 class NodalDG2d:
     """One nodal-DG discretisation on the GPU (Apollo ``Kind = nodalDG2d``)."""
 
-    def __init__(self, N: int, cfl: float, equation: str, eq_params, mesh: Mesh, bcs=(), device: int = 0,
-                 stream: int | None = None, part=None, rank: int = 0, numerical_flux: str = "LF"):
+    def __init__(self, N: int, cfl: float, equation: str | None, eq_params, mesh: Mesh, bcs=(), device: int = 0,
+                 stream: int | None = None, part=None, rank: int = 0, numerical_flux: str = "LF",
+                 deck: str | None = None):
         """``part`` (int32 [K], optional): a partition of ``mesh``; the handle then
         holds the elements with ``part == rank`` (apollo_dg_set_mesh_partition)
-        and steps through ``apollo_b200.distributed.DistNodalDG2d``."""
+        and steps through ``apollo_b200.distributed.DistNodalDG2d``.
+        ``deck`` (with ``equation`` None): Apollo input-deck text whose
+        equation block and boundary-condition list configure the handle
+        (apollo_dg_set_equation_text, apollo_dg_add_bc_text)."""
         self.lib = load_library()
         cfg = _Config(N, cfl, device, C.c_void_p(stream) if stream else None)
         h = C.c_void_p()
         self._check(self.lib.apollo_dg_create(C.byref(cfg), C.byref(h)), h=None)
         self.h = h
-        p = np.asarray(list(eq_params), dtype=np.float64)
-        self._check(self.lib.apollo_dg_set_equation(h, equation.encode(), p.ctypes.data_as(_dp), len(p)))
-        self._check(self.lib.apollo_dg_set_numerical_flux(h, numerical_flux.encode()))
+        if equation is None:
+            self._check(self.lib.apollo_dg_set_equation_text(h, None, deck.encode()))
+            self._check(self.lib.apollo_dg_add_bc_text(h, None, deck.encode()))
+        else:
+            p = np.asarray(list(eq_params), dtype=np.float64)
+            self._check(self.lib.apollo_dg_set_equation(h, equation.encode(), p.ctypes.data_as(_dp), len(p)))
+            self._check(self.lib.apollo_dg_set_numerical_flux(h, numerical_flux.encode()))
         for kind, params in bcs:
             bp = np.asarray(list(params), dtype=np.float64)
             self._check(self.lib.apollo_dg_add_bc(h, kind.encode(), bp.ctypes.data_as(_dp), len(bp)))

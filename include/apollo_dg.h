@@ -81,6 +81,43 @@ apollo_status apollo_dg_create(const apollo_dg_config* cfg, apollo_dg** out);
  * Numerical flux: Lax-Friedrichs unless apollo_dg_set_numerical_flux says otherwise. */
 apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const double* params, int nparams);
 
+/* ---- Apollo input-deck text.  Apollo configures this sub-solver from the
+ * cryptset blocks of its .pin input deck (WxNodalDG2dMethod::setup,
+ * src/subsolvers/wxnodaldg2dmethod.cc:50-152, and WxHyperbolicEqnSet::setup,
+ * src/hyper/wxhyperboliceqnset.cc:43-89): the nodalDG2d block's
+ * polynomialOrder and cfl, and the lists Equations, boundaryConditions and
+ * Limiter naming blocks whose Kind and keys configure each plugin.  These
+ * calls take that text (a whole deck, or one block) with Apollo's key names
+ * and defaults; the deck's Python preamble of "NAME = expression" lines may be
+ * included, and values may be arithmetic over those names.  With kind NULL
+ * the block is found through the list (or is the text's only block); with a
+ * kind, the text's keys are that plugin's.  Errors: APOLLO_ERR_CONFIG with the
+ * reason in err (host-only calls) or apollo_dg_last_error. */
+/* Host only: polynomial_order and cfl of the nodalDG2d block into *cfg (the
+ * device and stream fields are left as they are). */
+apollo_status apollo_dg_deck_config(const char* text, apollo_dg_config* cfg, char* err, int err_len);
+/* Host only: the equation block as apollo_dg_set_equation's kind and
+ * params[nparams] (at most 8), and its Numerical_Flux ("LF" if absent). */
+apollo_status apollo_dg_deck_equation(const char* kind, const char* text, char* kind_out, int kind_len,
+                                      double* params, int* nparams, char* flux_out, int flux_len, char* err,
+                                      int err_len);
+/* Host only: *count receives the number of boundary conditions the deck
+ * lists (the boundaryConditions of the block holding Equations; a text
+ * without Equations is one condition's block); entry `index` (if below
+ * *count) as apollo_dg_add_bc's kind and params. */
+apollo_status apollo_dg_deck_bc(const char* kind, const char* text, int index, int* count, char* kind_out,
+                                int kind_len, double* params, int* nparams, char* err, int err_len);
+/* Host only: the first block of the deck's Limiter list as
+ * apollo_dg_set_limiter's kind and params (kind_out "" when there is none). */
+apollo_status apollo_dg_deck_limiter(const char* kind, const char* text, char* kind_out, int kind_len,
+                                     double* params, int* nparams, char* err, int err_len);
+/* The same, applied to a handle: apollo_dg_set_equation (+ the numerical
+ * flux), apollo_dg_add_bc for every listed condition in order, and
+ * apollo_dg_set_limiter (removed when the deck lists none). */
+apollo_status apollo_dg_set_equation_text(apollo_dg* h, const char* kind, const char* text);
+apollo_status apollo_dg_add_bc_text(apollo_dg* h, const char* kind, const char* text);
+apollo_status apollo_dg_set_limiter_text(apollo_dg* h, const char* kind, const char* text);
+
 /* Euler numerical flux by Apollo's "Numerical_Flux" name (WxEulerEqn::setup,
  * src/hyperapps/euler/wxeulereqn.cc:45-87): "LF" (default), "HLL", "Roe",
  * "Wave"; any other name selects LF, as Apollo does (the call succeeds and
@@ -116,9 +153,15 @@ apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double
 
 /* Launch and tile shape of this handle's kernels, as the batch autotuner
  * picks them (apollo_dg_batch_autotune): the persistent grids use
- * SMs / grid_share CTAs; tile_shape 0 or 1 selects the mixed stage kernel's
- * operand chunking for the Euler kinds (the same arithmetic either way).
- * No counterpart in Apollo. */
+ * SMs / grid_share CTAs; tile_shape selects the mixed stage kernel:
+ *   0  the fused kernel (whole flux-deviation operand of a tile in shared
+ *      memory, tensor-core face traces) where it applies: "eulerEqn2d" with
+ *      the Lax-Friedrichs flux at orders 2..4; elsewhere as 2
+ *   1  the chunked kernel with 16-column operand chunks in three buffers
+ *   2  the chunked kernel with 24-column chunks (16 at order 5) in two buffers
+ * 1 and 2 compute the same result bit for bit (the same MMAs in the same K
+ * order); 0 agrees with them within the mixed form's error.  No counterpart
+ * in Apollo. */
 apollo_status apollo_dg_set_launch_shape(apollo_dg* h, int grid_share, int tile_shape);
 
 /* The element average of a nodal field is sum_n w[n] u[n]: w[Np] receives the

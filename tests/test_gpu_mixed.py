@@ -136,20 +136,38 @@ def test_mixed_nan_reports_error():
 
 @pytest.mark.parametrize("N", [2, 3, 4, 5])
 def test_tile_shapes_compute_the_same_steps(N):
-    """Both operand chunkings of the mixed stage (and a reduced grid) give the
-    same steps bit for bit: the same MMAs in the same K order."""
+    """Both operand chunkings of the chunked mixed stage kernel (shapes 1 and
+    2, and shape 0 where the fused kernel does not apply) give the same steps
+    bit for bit at any grid share: the same MMAs in the same K order.  The
+    fused kernel (shape 0 for four-field Euler at N <= 4) is the same at any
+    grid share, and within the mixed form's error of the chunked one."""
     p = problems.euler_vortex(n=17, N=N)
     s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh)
     x, y = s.node_coords()
     U0 = np.ascontiguousarray(p.ic(x, y))
     s.set_state(U0)
     dt0 = s.init_dt()
-    ends = []
-    for share, shape in ((1, 0), (1, 1), (2, 1), (4, 0)):
+
+    def run(share, shape):
         s.set_launch_shape(share, shape)
         s.set_state(U0)
         t, dt = s.advance(6, 0.0, dt0, precision="mixed")
-        ends.append((s.get_state(), t, dt))
-    for U, t, dt in ends[1:]:
-        np.testing.assert_array_equal(U, ends[0][0])
-        assert t == ends[0][1] and dt == ends[0][2]
+        return s.get_state(), t, dt
+
+    chunked = [run(1, 2), run(1, 1), run(2, 1), run(4, 2)]
+    fused = [run(1, 0), run(4, 0)]
+    if N == 5:
+        chunked += fused
+        fused = []
+    for U, t, dt in chunked[1:]:
+        np.testing.assert_array_equal(U, chunked[0][0])
+        assert t == chunked[0][1] and dt == chunked[0][2]
+    for U, t, dt in fused[1:]:
+        np.testing.assert_array_equal(U, fused[0][0])
+        assert t == fused[0][1] and dt == fused[0][2]
+    if fused:
+        assert rel_l2(fused[0][0], chunked[0][0]) <= 2e-7
+        assert fused[0][1] == pytest.approx(chunked[0][1], rel=1e-7)
+    s.set_state(U0)
+    s.advance(6, 0.0, dt0)
+    assert rel_l2(chunked[0][0], s.get_state()) <= 1e-6
