@@ -26,8 +26,8 @@
 //
 // Phases of a tile (bar = all 512 threads):
 //   S0 operand build: state deviations (A1), means, geometry, connectivity  bar
-//   S1 [t0] GEMM-A  D1 = A1 V^T;  reference fluxes at the means;  wait D1
-//   S2 volume items -> A2 volume columns                                  bar
+//   S1 [t0] GEMM-A  D1 = A1 V^T;  volume references per thread;  wait D1 bar
+//   S2 volume items -> A2 volume columns; face and float64 references     bar
 //   S3 [t0] GEMM-B volume part;  face items -> A2 face columns            bar
 //   S4 [t0] GEMM-B face part;  wait D2
 //   S5 epilogue (float64 result, RK update), result deviations (A3), means bar
@@ -37,6 +37,8 @@
 // Apollo: wxnodaldg2dmethod.cc:235-542 with the TSSSP RK_2 stage update.
 
 constexpr int kFusedThreads = 512;
+
+
 
 template <int N> struct FusedCfg {
   static constexpr int M = 4;
@@ -220,6 +222,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   auto wait = [&](uint32_t mb, uint32_t parity) {
     if (!umma::mbar_wait_bounded(mb, parity, wlim)) *abort_flag = 1;
   };
+
   auto all_sync = [&]() { asm volatile("bar.sync 1, %0;" ::"n"(kFusedThreads) : "memory"); };
 
   // descriptors (the start address field advances by 16 per K step of 256 bytes)
@@ -261,6 +264,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   // this thread's state values of tile i straight from global memory (no
   // shared-memory state tile)
   double xv[4] = {0.0, 0.0, 0.0, 0.0};
+  double dt_ep = 0.0;  // this thread's element's dt, read in the operand build
   auto load_x = [&](int i) {
     const int k0 = tile_of(i) * E, ne = min(E, d.K - k0);
     const double* xg = a.x + (size_t)k0 * NP * M;
@@ -300,6 +304,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           xv[u] = v[u];  // kept for the epilogue
         }
         PS[ng_ep * 128 + r_ep] = (v[0] + v[1]) + (v[2] + v[3]);
+        if (valid) dt_ep = stage_dt(k0 + e_ep);
       }
       if (tid >= kFusedThreads - E) {
         // fp32 geometry and connectivity of the tile
@@ -341,7 +346,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       all_sync();
       if (*abort_flag) { ok = false; break; }
     }
-    // ---------------- S1: GEMM-A, the next state tile, reference fluxes
+    // ---------------- S1: GEMM-A, the next state tile, the volume references
     if (tid == 0) {
       umma::fence_after_sync();
 #pragma unroll
@@ -356,39 +361,24 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         x_issued++;
       }
       if (u0_prefetch) bulk_prefetch_l2(a.u0 + (size_t)k0 * NP * M, (uint32_t)((ne * NP * M * 8) & ~15));
+      // the previous tile's trace store has read its staging (the A2 hi half),
+      // which this tile's volume items overwrite after the next barrier
+      if (write_traces) umma::bulk_wait_read();
     }
-    if (tid < 4 * E) {
-      // reference fluxes at the fp32 mean (volume + three faces per element)
-      const int kind = tid / E, e = tid % E;
-      if (e < ne) {
-        const ElemGeo& gg = GT[e];
-        float qc[M];
+    // this thread's element's volume references (fp32 directional fluxes of
+    // the mean), computed while GEMM-A runs; the face and float64 references
+    // are left to the lightest warps of the volume phase
+    const bool evalid_me = e_me < ne;
+    float kQF[M], kG[4], kP[2 * M];
+    {
 #pragma unroll
-        for (int f = 0; f < M; ++f) qc[f] = QF[f * E + e];
-        float F[M], G[M];
-        Eq<EQ>::flux2(d.eqp, qc, F, G, &err);
-        if (kind == 0) {
-          float R0[M], S0[M];
-          Q::dirflux(d.eqp, qc, GEO[0 * E + e], GEO[1 * E + e], GEO[2 * E + e], GEO[3 * E + e], R0, S0, &err);
+      for (int f = 0; f < M; ++f) kQF[f] = QF[f * E + e_me];
 #pragma unroll
-          for (int f = 0; f < M; ++f) {
-            P0[f * E + e] = R0[f];
-            P0[(M + f) * E + e] = S0[f];
-            RB[f * E + e] = gg.rx * (double)F[f] + gg.ry * (double)G[f];
-            RB[(M + f) * E + e] = gg.sx * (double)F[f] + gg.sy * (double)G[f];
-          }
-        } else {
-          const int fc = kind - 1;
-          float nf[M];
-          Q::lf(d.eqp, GEO[(4 + fc) * E + e], GEO[(7 + fc) * E + e], qc, qc, nf, &err);
-          const double w = -gg.sJ[fc] * gg.invJ, nx = gg.nx[fc], ny = gg.ny[fc];
-#pragma unroll
-          for (int f = 0; f < M; ++f) {
-            P0[((2 + fc) * M + f) * E + e] = nf[f];
-            FB[(fc * M + f) * E + e] = w * (nx * (double)F[f] + ny * (double)G[f]);
-          }
-        }
-      }
+      for (int j = 0; j < 4; ++j) kG[j] = GEO[j * E + e_me];
+      int e_dummy = 0;
+      const typename Q::Side sd = Q::side(d.eqp, kQF, evalid_me ? &err : &e_dummy);
+      Q::along(sd, kQF, kG[0], kG[1], kP);
+      Q::along(sd, kQF, kG[2], kG[3], kP + M);
     }
     // (the stall switch of the failure tests points the first tile's wait at a
     // barrier that nothing completes before the abort path)
@@ -399,16 +389,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     // columns [16 g4, 16 g4 + 16) of its quarter; per group of 4 points a
     // thread computes the fluxes of point 4 j + f_me of its element.
     {
-      const bool evalid = e_me < ne;
-      float kQF[M], kG[4], kP[2 * M];
-#pragma unroll
-      for (int f = 0; f < M; ++f) {
-        kQF[f] = QF[f * E + e_me];
-        kP[f] = P0[f * E + e_me];
-        kP[M + f] = P0[(M + f) * E + e_me];
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) kG[j] = GEO[j * E + e_me];
+      const bool evalid = evalid_me;
       const int c0 = 16 * g4;
       if (c0 < C::NC16) {
         float v[16];
@@ -456,6 +437,49 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           }
         }
       }
+      // reference fluxes for the faces and the float64 epilogue, by the
+      // warps with the fewest volume items (the last four)
+      if (tid >= kFusedThreads - 4 * E) {
+        // reference fluxes at the fp32 mean (volume + three faces per element).
+        // With both traces at the mean the Lax-Friedrichs flux is the normal
+        // flux of the mean exactly (0.5 (F + F + lam 0) = F in fp32), so a face
+        // takes the directional flux unless a clamp sends the flux down its
+        // general path.
+        const int kind = (tid - (kFusedThreads - 4 * E)) / E, e = (tid - (kFusedThreads - 4 * E)) % E;
+        if (e < ne) {
+          const ElemGeo& gg = GT[e];
+          float qc[M];
+#pragma unroll
+          for (int f = 0; f < M; ++f) qc[f] = QF[f * E + e];
+          float F[M], G[M];
+          Eq<EQ>::flux2(d.eqp, qc, F, G, &err);
+          const typename Q::Side sd = Q::side(d.eqp, qc, &err);
+          if (kind == 0) {
+            float R0[M], S0[M];
+            Q::along(sd, qc, GEO[0 * E + e], GEO[1 * E + e], R0);
+            Q::along(sd, qc, GEO[2 * E + e], GEO[3 * E + e], S0);
+#pragma unroll
+            for (int f = 0; f < M; ++f) {
+              P0[f * E + e] = R0[f];
+              P0[(M + f) * E + e] = S0[f];
+              RB[f * E + e] = gg.rx * (double)F[f] + gg.ry * (double)G[f];
+              RB[(M + f) * E + e] = gg.sx * (double)F[f] + gg.sy * (double)G[f];
+            }
+          } else {
+            const int fc = kind - 1;
+            float nf[M];
+            const float nx = GEO[(4 + fc) * E + e], ny = GEO[(7 + fc) * E + e];
+            if (sd.clean) Q::along(sd, qc, nx, ny, nf);
+            else Q::lf(d.eqp, nx, ny, qc, qc, nf, &err);
+            const double w = -gg.sJ[fc] * gg.invJ, nxd = gg.nx[fc], nyd = gg.ny[fc];
+#pragma unroll
+            for (int f = 0; f < M; ++f) {
+              P0[((2 + fc) * M + f) * E + e] = nf[f];
+              FB[(fc * M + f) * E + e] = w * (nxd * (double)F[f] + nyd * (double)G[f]);
+            }
+          }
+        }
+      }
       umma::fence_before_sync();
       umma::fence_proxy_async();
       all_sync();
@@ -482,18 +506,29 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       const int k = k0 + e_me;
       const int rowb = 4 * e_me;
       const uint32_t obase = (uint32_t)((rowb >> 3) * C::SBO2 + (rowb & 7) * 16);
-      for (int j = g4; j < C::NFG; j += 4) {
+      // the traces of this thread's face columns (j = g4 and g4 + 4), both
+      // fetched before either is used
+      static_assert(C::NFG <= 8, "two face column groups per warp");
+      float tM0[M], tP0[M], tM1[M], tP1[M];
+      auto fetch = [&](int j, float* tm, float* tp) {
+        const int col = 4 * j + f_me;
+        if (j < C::NFG && col < NF && evalid) {
+          const int fc = col / NG, g = col - fc * NG;
+          load_fields<M>(a.tr_in + ((size_t)k * 3 + fc) * TS + g * M, tm);
+          const int nb = CN[e_me * 6 + 2 * fc];
+          if (nb >= 0)
+            load_fields<M>(a.tr_in + ((size_t)nb * 3 + CN[e_me * 6 + 2 * fc + 1]) * TS + (NG - 1 - g) * M, tp);
+        }
+      };
+      fetch(g4, tM0, tP0);
+      fetch(g4 + 4, tM1, tP1);
+      auto item = [&](int j, float* qM, float* qP) {
         const int col = 4 * j + f_me;
         float dev[M];
         if (col < NF && evalid) {
           const int fc = col / NG, g = col - fc * NG;
           const int nb = CN[e_me * 6 + 2 * fc];
-          float qM[M], qP[M], nf[M];
-          load_fields<M>(a.tr_in + ((size_t)k * 3 + fc) * TS + g * M, qM);
-          if (nb >= 0) {
-            const int f2 = CN[e_me * 6 + 2 * fc + 1];
-            load_fields<M>(a.tr_in + ((size_t)nb * 3 + f2) * TS + (NG - 1 - g) * M, qP);
-          }
+          float nf[M];
           const float nx = GEO[(4 + fc) * E + e_me], ny = GEO[(7 + fc) * E + e_me];
           if (nb < 0) {
             const ElemGeo& geo = d.geo[k];
@@ -524,7 +559,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           *(float*)(A2h + oc + 16 * f) = h;
           *(float*)(A2l + oc + 16 * f) = l;
         }
-      }
+      };
+      if (g4 < C::NFG) item(g4, tM0, tP0);
+      if (g4 + 4 < C::NFG) item(g4 + 4, tM1, tP1);
       umma::fence_proxy_async();
       all_sync();
     }
@@ -557,7 +594,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         const int k = k0 + e;
         const double Rbar = RB[f * E + e], Sbar = RB[(M + f) * E + e];
         const double F0 = FB[(0 * M + f) * E + e], F1 = FB[(1 * M + f) * E + e], F2 = FB[(2 * M + f) * E + e];
-        const double dt = stage_dt(k);
+        const double dt = dt_ep;
         const double c_stage = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
         const double* urow = a.u0 + (size_t)k * NP * M + f;
         double* orow = a.out + (size_t)k * NP * M + f;
@@ -658,9 +695,6 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         umma::bulk_commit();
       }
     }
-    // the next tile's volume items overwrite the staging (A2 hi): thread 0
-    // waits for the store's reads before the first barrier of that tile
-    if (tid == 0 && write_traces) umma::bulk_wait_read();
   }
   if (want_lambda) lam_acc.flush_warp(d.st);
   if (err) atomicOr(&d.st->err, err);
