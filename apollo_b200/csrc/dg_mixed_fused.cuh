@@ -219,8 +219,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     umma::bulk_g2s(umma::smem_u32(GT), d.geo + k0, gb, mbG);
     umma::bulk_g2s(umma::smem_u32(CT), d.conn + (size_t)k0 * 6, cb, mbG);
   };
+  // (a single warp waits; it spins, so it passes the phase the moment the
+  // tensor core or the copy completes it)
   auto wait = [&](uint32_t mb, uint32_t parity) {
-    if (!umma::mbar_wait_bounded(mb, parity, wlim)) *abort_flag = 1;
+    if (!umma::mbar_spin_bounded(mb, parity, wlim)) *abort_flag = 1;
   };
 
   auto all_sync = [&]() { asm volatile("bar.sync 1, %0;" ::"n"(kFusedThreads) : "memory"); };
@@ -506,46 +508,89 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       const int k = k0 + e_me;
       const int rowb = 4 * e_me;
       const uint32_t obase = (uint32_t)((rowb >> 3) * C::SBO2 + (rowb & 7) * 16);
-      // the traces of this thread's face columns (j = g4 and g4 + 4), both
-      // fetched before either is used
+      // this thread's two face columns (groups j = g4 and g4 + 4): traces
+      // fetched first, boundary ghosts next, then both Lax-Friedrichs fluxes
+      // as one straight-line computation
       static_assert(C::NFG <= 8, "two face column groups per warp");
-      float tM0[M], tP0[M], tM1[M], tP1[M];
-      auto fetch = [&](int j, float* tm, float* tp) {
-        const int col = 4 * j + f_me;
-        if (j < C::NFG && col < NF && evalid) {
-          const int fc = col / NG, g = col - fc * NG;
-          load_fields<M>(a.tr_in + ((size_t)k * 3 + fc) * TS + g * M, tm);
-          const int nb = CN[e_me * 6 + 2 * fc];
-          if (nb >= 0)
-            load_fields<M>(a.tr_in + ((size_t)nb * 3 + CN[e_me * 6 + 2 * fc + 1]) * TS + (NG - 1 - g) * M, tp);
+      float tM[2][M], tP[2][M];
+      int fcs[2], nbs[2];
+      bool val[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = g4 + 4 * h, col = 4 * j + f_me;
+        val[h] = j < C::NFG && col < NF && evalid;
+        const int fc = val[h] ? col / NG : 0, g = col - fc * NG;
+        fcs[h] = fc;
+        nbs[h] = CN[e_me * 6 + 2 * fc];
+#pragma unroll
+        for (int f = 0; f < M; ++f) { tM[h][f] = kQF[f]; tP[h][f] = kQF[f]; }  // a physical stand-in
+        if (val[h]) {
+          load_fields<M>(a.tr_in + ((size_t)k * 3 + fc) * TS + g * M, tM[h]);
+          if (nbs[h] >= 0)
+            load_fields<M>(a.tr_in + ((size_t)nbs[h] * 3 + CN[e_me * 6 + 2 * fc + 1]) * TS + (NG - 1 - g) * M,
+                           tP[h]);
         }
-      };
-      fetch(g4, tM0, tP0);
-      fetch(g4 + 4, tM1, tP1);
-      auto item = [&](int j, float* qM, float* qP) {
+      }
+      float nx[2], ny[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        nx[h] = GEO[(4 + fcs[h]) * E + e_me];
+        ny[h] = GEO[(7 + fcs[h]) * E + e_me];
+        if (val[h] && nbs[h] < 0) {
+          const int col = 4 * (g4 + 4 * h) + f_me, g = col - fcs[h] * NG;
+          const ElemGeo& geo = d.geo[k];
+          const double z = d.gz[g];
+          double rr, ss;
+          if (fcs[h] == 0) { rr = z; ss = -1.0; }
+          else if (fcs[h] == 1) { rr = -z; ss = z; }
+          else { rr = -1.0; ss = -z; }
+          const double bx = 0.5 * (-geo.vx[0] * (rr + ss) + geo.vx[1] * (1. + rr) + geo.vx[2] * (1. + ss));
+          const double by = 0.5 * (-geo.vy[0] * (rr + ss) + geo.vy[1] * (1. + rr) + geo.vy[2] * (1. + ss));
+          apply_bc<EQ, float>(d.bcs, -nbs[h], stage_t(k), bx, by, nx[h], ny[h], tM[h], tP[h]);
+        }
+      }
+      float nf[2][M], lam[2];
+      {
+        int e_ign = 0;  // stand-in columns report nothing
+        int* er0 = val[0] ? &err : &e_ign;
+        int* er1 = val[1] ? &err : &e_ign;
+        const typename Q::Side A0 = Q::side(d.eqp, tM[0], er0), B0 = Q::side(d.eqp, tP[0], er0);
+        const typename Q::Side A1 = Q::side(d.eqp, tM[1], er1), B1 = Q::side(d.eqp, tP[1], er1);
+        if (A0.clean && B0.clean && A1.clean && B1.clean) {
+          const float gamma = (float)d.eqp.p[0];
+          float FM0[M], FP0[M], FM1[M], FP1[M];
+          Q::along(A0, tM[0], nx[0], ny[0], FM0);
+          Q::along(B0, tP[0], nx[0], ny[0], FP0);
+          Q::along(A1, tM[1], nx[1], ny[1], FM1);
+          Q::along(B1, tP[1], nx[1], ny[1], FP1);
+          const float cM0 = sqrtf(A0.vx * A0.vx + A0.vy * A0.vy + A0.vz * A0.vz) + sqrtf(gamma * A0.p * A0.ir);
+          const float cP0 = sqrtf(B0.vx * B0.vx + B0.vy * B0.vy + B0.vz * B0.vz) + sqrtf(gamma * B0.p * B0.ir);
+          const float cM1 = sqrtf(A1.vx * A1.vx + A1.vy * A1.vy + A1.vz * A1.vz) + sqrtf(gamma * A1.p * A1.ir);
+          const float cP1 = sqrtf(B1.vx * B1.vx + B1.vy * B1.vy + B1.vz * B1.vz) + sqrtf(gamma * B1.p * B1.ir);
+          lam[0] = cM0 > cP0 ? cM0 : cP0;
+          lam[1] = cM1 > cP1 ? cM1 : cP1;
+#pragma unroll
+          for (int c = 0; c < M; ++c) {
+            nf[0][c] = 0.5f * (FM0[c] + FP0[c] + lam[0] * (tM[0][c] - tP[0][c]));
+            nf[1][c] = 0.5f * (FM1[c] + FP1[c] + lam[1] * (tM[1][c] - tP[1][c]));
+          }
+        } else {
+          // a clamp: each flux down the reference's own path
+          lam[0] = Q::lf(d.eqp, nx[0], ny[0], tM[0], tP[0], nf[0], er0);
+          lam[1] = Q::lf(d.eqp, nx[1], ny[1], tM[1], tP[1], nf[1], er1);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = g4 + 4 * h;
+        if (j >= C::NFG) continue;
         const int col = 4 * j + f_me;
         float dev[M];
-        if (col < NF && evalid) {
-          const int fc = col / NG, g = col - fc * NG;
-          const int nb = CN[e_me * 6 + 2 * fc];
-          float nf[M];
-          const float nx = GEO[(4 + fc) * E + e_me], ny = GEO[(7 + fc) * E + e_me];
-          if (nb < 0) {
-            const ElemGeo& geo = d.geo[k];
-            const double z = d.gz[g];
-            double rr, ss;
-            if (fc == 0) { rr = z; ss = -1.0; }
-            else if (fc == 1) { rr = -z; ss = z; }
-            else { rr = -1.0; ss = -z; }
-            const double bx = 0.5 * (-geo.vx[0] * (rr + ss) + geo.vx[1] * (1. + rr) + geo.vx[2] * (1. + ss));
-            const double by = 0.5 * (-geo.vy[0] * (rr + ss) + geo.vy[1] * (1. + rr) + geo.vy[2] * (1. + ss));
-            apply_bc<EQ, float>(d.bcs, -nb, stage_t(k), bx, by, nx, ny, qM, qP);
-          }
-          const float lam = Q::lf(d.eqp, nx, ny, qM, qP, nf, &err);
-          if (want_lambda) lam_acc.add(d.st, inst_of(d, k), fabs((double)lam));
-          const float w = GEO[(10 + fc) * E + e_me];
+        if (val[h]) {
+          if (want_lambda) lam_acc.add(d.st, inst_of(d, k), fabs((double)lam[h]));
+          const float w = GEO[(10 + fcs[h]) * E + e_me];
 #pragma unroll
-          for (int f = 0; f < M; ++f) dev[f] = w * (nf[f] - P0[((2 + fc) * M + f) * E + e_me]);
+          for (int f = 0; f < M; ++f) dev[f] = w * (nf[h][f] - P0[((2 + fcs[h]) * M + f) * E + e_me]);
         } else {
 #pragma unroll
           for (int f = 0; f < M; ++f) dev[f] = 0.f;
@@ -554,14 +599,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         const uint32_t oc = obase + (uint32_t)(((C::KV + col) >> 2) * umma::kLBO + (col & 3) * 4);
 #pragma unroll
         for (int f = 0; f < M; ++f) {
-          float h, l;
-          split_tf32(dev[f], h, l);
-          *(float*)(A2h + oc + 16 * f) = h;
-          *(float*)(A2l + oc + 16 * f) = l;
+          float hh, ll;
+          split_tf32(dev[f], hh, ll);
+          *(float*)(A2h + oc + 16 * f) = hh;
+          *(float*)(A2l + oc + 16 * f) = ll;
         }
-      };
-      if (g4 < C::NFG) item(g4, tM0, tP0);
-      if (g4 + 4 < C::NFG) item(g4 + 4, tM1, tP1);
+      }
       umma::fence_proxy_async();
       all_sync();
     }

@@ -87,6 +87,31 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
   return ok != 0;
 }
 
+// One poll without a suspend hint (returns at once).
+__device__ __forceinline__ bool mbar_test_wait(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded spin on an mbarrier phase for a single waiting warp whose wait is
+// short (the tensor core finishing a few MMAs): polls without suspending, so
+// the warp sees the phase complete at once; gives up after `limit` polls
+// (about 2^27 cycles at the default) and returns false.
+__device__ __forceinline__ bool mbar_spin_bounded(uint32_t mbar, uint32_t parity, uint32_t limit = (1u << 22)) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    if (mbar_test_wait(mbar, parity)) return true;
+    if (i > 64) __nanosleep(32);
+  }
+  return false;
+}
+
 // Bounded wait on an mbarrier phase: gives up after `limit` polls (each poll
 // suspends for at most kSuspendNs: about 2 s in all) and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, uint32_t limit = (1u << 22)) {
