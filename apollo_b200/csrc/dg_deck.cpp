@@ -287,6 +287,16 @@ const std::vector<KindSpec>& bc_kinds() {
   };
   return k;
 }
+const std::vector<KindSpec>& source_kinds() {
+  static const std::vector<KindSpec> k = {
+      {"tranverseMagneticSrc", {}},
+      {"pointCurrentSrc",
+       {{"xLocation", true, 0.0}, {"yLocation", true, 0.0}, {"radius", true, 0.0}, {"currentDensity", true, 0.0},
+        {"frequency", true, 0.0}, {"phase", true, 0.0}, {"charge", true, 0.0}, {"mass", true, 0.0},
+        {"epsilon0", true, 0.0}}},
+  };
+  return k;
+}
 const std::vector<KindSpec>& limiter_kinds() {
   static const std::vector<KindSpec> k = {
       {"eulerLimiterHW", {{"gas_gamma", true, 0.0}, {"min_pressure", true, 0.0}, {"min_density", true, 0.0}}},
@@ -481,6 +491,73 @@ apollo_status apollo_dg_deck_bc(const char* kind, const char* text, int index, i
   return APOLLO_OK;
 }
 
+apollo_status apollo_dg_deck_source(const char* kind, const char* text, int index, int* count, char* kind_out,
+                                    int kind_len, int* out_range, int* nout, double* params, int* nparams, char* err,
+                                    int err_len) {
+  if (!text || !count) return APOLLO_ERR_ARG;
+  Deck d;
+  if (!parse(text, d)) {
+    copy_err(d.err, err, err_len);
+    return APOLLO_ERR_CONFIG;
+  }
+  std::string e;
+  const Block* b = nullptr;
+  if (kind) {
+    *count = 1;
+    b = (d.root.sub.size() == 1 && d.root.kv.empty()) ? &d.root.sub[0] : &d.root;
+    if (index > 0) b = nullptr;
+  } else if (const Block* holder = find_with_key(d.root, "Equations")) {
+    // the sub-solver's Sources list (none: no sources)
+    const std::string* lst = holder->get("Sources");
+    const std::vector<std::string> items = lst ? list_items(*lst) : std::vector<std::string>();
+    *count = (int)items.size();
+    if (index < (int)items.size()) {
+      b = find_block(d.root, items[index]);
+      if (!b) e = "no block <" + items[index] + "> for Sources";
+    }
+  } else {
+    *count = 1;
+    if (d.root.get("Kind")) b = &d.root;
+    else if (d.root.sub.size() == 1) b = &d.root.sub[0];
+    else e = "no Equations list and no single source block";
+    if (index > 0) b = nullptr;
+  }
+  if (index >= *count) return APOLLO_OK;
+  if (!b) {
+    copy_err(e, err, err_len);
+    return APOLLO_ERR_CONFIG;
+  }
+  const std::string k = kind ? std::string(kind) : (b->get("Kind") ? unquote(*b->get("Kind")) : std::string());
+  std::vector<double> v;
+  if (!block_params(*b, k, source_kinds(), d, v, e)) {
+    copy_err(e, err, err_len);
+    return APOLLO_ERR_CONFIG;
+  }
+  const std::string* orng = b->get("OutRange");
+  const std::vector<std::string> outs = orng ? list_items(*orng) : std::vector<std::string>();
+  if (outs.empty()) {
+    copy_err(k + ": missing OutRange", err, err_len);
+    return APOLLO_ERR_CONFIG;
+  }
+  if (out_range && nout) {
+    int n = 0;
+    for (const std::string& o : outs) {
+      double x;
+      if (!eval_number(o, d.defs, &x) || x != std::floor(x) || x < 0) {
+        copy_err(k + ": OutRange entry " + o + " is not a field index", err, err_len);
+        return APOLLO_ERR_CONFIG;
+      }
+      if (n < 8) out_range[n++] = (int)x;
+    }
+    *nout = n;
+  }
+  if (params)
+    for (size_t i = 0; i < v.size(); ++i) params[i] = v[i];
+  if (nparams) *nparams = (int)v.size();
+  if (kind_out && kind_len > 0) copy_err(k, kind_out, kind_len);
+  return APOLLO_OK;
+}
+
 apollo_status apollo_dg_deck_limiter(const char* kind, const char* text, char* kind_out, int kind_len,
                                      double* params, int* nparams, char* err, int err_len) {
   if (!text || !params || !nparams) return APOLLO_ERR_ARG;
@@ -555,6 +632,29 @@ apollo_status apollo_dg_add_bc_text(apollo_dg* h, const char* kind, const char* 
       return r;
     }
     r = apollo_dg_add_bc(h, k, p, np);
+    if (r) return r;
+  }
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_add_source_text(apollo_dg* h, const char* kind, const char* text) {
+  if (!h || !text) return APOLLO_ERR_ARG;
+  char k[64], err[256];
+  double p[9];
+  int count = 0, np = 0, outs[8], nout = 0;
+  apollo_status r = apollo_dg_deck_source(kind, text, 0, &count, nullptr, 0, nullptr, nullptr, nullptr, nullptr, err,
+                                          sizeof err);
+  if (r) {
+    apollo::handle_set_error(h, err);
+    return r;
+  }
+  for (int i = 0; i < count; ++i) {
+    r = apollo_dg_deck_source(kind, text, i, &count, k, sizeof k, outs, &nout, p, &np, err, sizeof err);
+    if (r) {
+      apollo::handle_set_error(h, err);
+      return r;
+    }
+    r = apollo_dg_add_source(h, k, outs, nout, p, np);
     if (r) return r;
   }
   return APOLLO_OK;

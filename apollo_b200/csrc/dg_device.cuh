@@ -38,6 +38,20 @@ struct DevState {
   double sums[8];
 };
 
+// Source plugins (Apollo's WxHyperbolicSrc kinds whose value depends on time
+// and position only): kind SRC_TM tranverseMagneticSrc
+// (src/hyperapps/maxwell/wxtransversemagneticsrc.h:37-44), SRC_POINT
+// pointCurrentSrc (src/hyperapps/maxwell/wxpointcurrent.h); out: the field of
+// this handle's layout the source adds into; p: the plugin's parameters.
+constexpr int kMaxSrc = 4;
+enum SrcKind : int { SRC_TM = 1, SRC_POINT = 2 };
+struct SrcTable {
+  int n;
+  int kind[kMaxSrc];
+  int out[kMaxSrc];
+  double p[kMaxSrc][9];
+};
+
 // Operators of one order, float64, row-major, built on the host.
 //   V  [NC][NP]  nodal values -> cubature points (Vand_cub * V^-1)
 //   Dr [NP][NC]  VVT * Dr_cub^T * diag(w_cub)    (VVT = V V^T, reference-element M^-1)
@@ -61,6 +75,13 @@ struct DgDev {
   // first wait at a barrier nothing completes (apollo_dg_debug_set_waits)
   unsigned wait_limit;
   int debug_stall;
+  // source terms: the table, VS = VVT V^T diag(w) [NP][NC] (the source's
+  // contribution is VS S at the cubature points), the cubature points' reference
+  // coordinates [NC] each, and (mixed precision) a [K][NP][M] buffer holding
+  // the current stage's source contribution
+  SrcTable src;
+  const double *VS, *cub_r, *cub_s;
+  double* srcv;
   const double *V, *Dr, *Ds, *I, *L, *gz, *gw;
   double *vol, *trace, *flux;  // scratch: [K][NP][M], [K][NF][M], [K][NF][M]
   DevState* st;
@@ -174,6 +195,9 @@ cudaError_t launch_halo_blocks(const void* src, void* dst, const int* idx, int n
                                cudaStream_t s);
 cudaError_t launch_integrals(int eq, const DgDev& d, const double* u, const double* wJ, cudaStream_t s);
 cudaError_t launch_energy(int eq, const DgDev& d, const double* u, const double* mass, cudaStream_t s);
+// Source contribution VS S(t, x_c, y_c) of every element at the stage time of
+// `a`: added to dst (accumulate) or written to it (fields without a source: 0).
+cudaError_t launch_source(int eq, const DgDev& d, const StageArgs& a, double* dst, int accumulate, cudaStream_t s);
 int fp64_supported(int eq, int N);
 
 }  // namespace apollo

@@ -359,6 +359,80 @@ __global__ void k_energy(DgDev d, const double* __restrict__ u, const double* __
   }
 }
 
+// The source plugins at one point (Apollo adds each into its output field,
+// WxHyperbolicSrc::compSource, src/hyper/wxhyperbolicsrc.cc:64-80).
+__device__ __forceinline__ void source_terms(const SrcTable& T, double t, double x, double y, double* s) {
+  for (int i = 0; i < T.n; ++i) {
+    const double* p = T.p[i];
+    double v = 0.0;
+    if (T.kind[i] == SRC_TM) {
+      v = exp(t) * (x * (1 - x) * y * (1 - y) + 2. * x * (1 - x) + 2 * y * (1 - y));
+    } else if (T.kind[i] == SRC_POINT) {
+      const double qbyme = p[6] / (p[7] * p[8]);
+      if (sqrt((x - p[0]) * (x - p[0]) + (y - p[1]) * (y - p[1])) < p[2]) v = p[3] * qbyme * sin(p[4] * t + p[5]);
+    }
+    s[T.out[i]] += v;
+  }
+}
+
+// Source contribution of a block of kSrcE elements: the sources at every
+// cubature point (physical coordinates from the element's affine map), then
+// VS times them per (element, node, field).
+constexpr int kSrcE = 4;
+template <int EQ, int N>
+__global__ void __launch_bounds__(128) k_source(DgDev d, StageArgs a, double* __restrict__ dst, int accumulate) {
+  constexpr int M = Eq<EQ>::M, NP = Sizes<N>::NP, NC = Sizes<N>::NC;
+  __shared__ double S[kSrcE][NC][M];
+  const int k0 = blockIdx.x * kSrcE;
+  for (int i = threadIdx.x; i < kSrcE * NC; i += blockDim.x) {
+    const int e = i / NC, c = i - e * NC, k = k0 + e;
+    double sv[M];
+#pragma unroll
+    for (int f = 0; f < M; ++f) sv[f] = 0.0;
+    if (k < d.K) {
+      const ElemGeo& g = d.geo[k];
+      const double r = d.cub_r[c], q = d.cub_s[c];
+      const double x = 0.5 * (-g.vx[0] * (r + q) + g.vx[1] * (1. + r) + g.vx[2] * (1. + q));
+      const double y = 0.5 * (-g.vy[0] * (r + q) + g.vy[1] * (1. + r) + g.vy[2] * (1. + q));
+      const DevState& st = d.st[inst_of(d, k)];
+      const double t = a.time_from_state ? st.t + st.dt * a.frac : a.t_arg;
+      source_terms(d.src, t, x, y, sv);
+    }
+#pragma unroll
+    for (int f = 0; f < M; ++f) S[e][c][f] = sv[f];
+  }
+  __syncthreads();
+  unsigned fmask = 0;
+  for (int i = 0; i < d.src.n; ++i) fmask |= 1u << d.src.out[i];
+  for (int i = threadIdx.x; i < kSrcE * NP * M; i += blockDim.x) {
+    const int e = i / (NP * M), r = i - e * NP * M, n = r / M, f = r - n * M, k = k0 + e;
+    if (k >= d.K) continue;
+    double v = 0.0;
+    if (fmask & (1u << f))
+      for (int c = 0; c < NC; ++c) v += d.VS[n * NC + c] * S[e][c][f];
+    double* o = dst + ((size_t)k * NP + n) * M + f;
+    if (accumulate) {
+      if (fmask & (1u << f)) *o += v;
+    } else {
+      *o = v;
+    }
+  }
+}
+
+template <int EQ>
+cudaError_t source_dispatch(const DgDev& d, const StageArgs& a, double* dst, int acc, cudaStream_t s) {
+  const unsigned g = (unsigned)((d.K + kSrcE - 1) / kSrcE);
+  if (g == 0) return cudaSuccess;
+  switch (d.N) {
+    case 2: k_source<EQ, 2><<<g, 128, 0, s>>>(d, a, dst, acc); break;
+    case 3: k_source<EQ, 3><<<g, 128, 0, s>>>(d, a, dst, acc); break;
+    case 4: k_source<EQ, 4><<<g, 128, 0, s>>>(d, a, dst, acc); break;
+    case 5: k_source<EQ, 5><<<g, 128, 0, s>>>(d, a, dst, acc); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 int g_num_sms = 0;
 int num_sms() {
   if (g_num_sms == 0) {
@@ -395,6 +469,11 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
   if (a.phase != PHASE_FACE) {
     if (ev) cudaEventRecord(ev[0], s);
     k_volume<EQ, N><<<gv, kThreads, VT::BYTES, s>>>(d, a);
+    // sources enter the volume term (wxcubature2d.cc:297-325: VT (w J S))
+    if (d.src.n > 0) {
+      cudaError_t e = source_dispatch<EQ>(d, a, d.vol, 1, s);
+      if (e != cudaSuccess) return e;
+    }
     if (ev) cudaEventRecord(ev[1], s);
   }
   if (a.phase == PHASE_VOLUME) return cudaGetLastError();
@@ -473,6 +552,17 @@ cudaError_t launch_rhs_fp64(int eq, const DgDev& d, const StageArgs& a, cudaStre
     case EQ_MAXWELL: return dispatch_n<EQ_MAXWELL>(d, a, s, ev);
     case EQ_EULER2D: return dispatch_n<EQ_EULER2D>(d, a, s, ev);
     case EQ_MAXWELL_TM: return dispatch_n<EQ_MAXWELL_TM>(d, a, s, ev);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_source(int eq, const DgDev& d, const StageArgs& a, double* dst, int accumulate, cudaStream_t s) {
+  switch (eq) {
+    case EQ_ADVECTION: return source_dispatch<EQ_ADVECTION>(d, a, dst, accumulate, s);
+    case EQ_EULER: return source_dispatch<EQ_EULER>(d, a, dst, accumulate, s);
+    case EQ_MAXWELL: return source_dispatch<EQ_MAXWELL>(d, a, dst, accumulate, s);
+    case EQ_EULER2D: return source_dispatch<EQ_EULER2D>(d, a, dst, accumulate, s);
+    case EQ_MAXWELL_TM: return source_dispatch<EQ_MAXWELL_TM>(d, a, dst, accumulate, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -48,6 +48,10 @@ struct apollo_dg {
   int tile_shape = 0;  // mixed stage operand chunking picked by the batch autotuner
   unsigned wait_limit = 0;  // apollo_dg_debug_set_waits
   int debug_stall = 0;
+  // source plugins (apollo_dg_add_source): the table, VS = VVT V^T diag(w),
+  // the cubature points, and the mixed stages' source buffer
+  SrcTable src{};
+  double *VS_d = nullptr, *cubr_d = nullptr, *cubs_d = nullptr, *srcv_d = nullptr;
   double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
          *gw_d = nullptr, *wmass_d = nullptr, *mass_d = nullptr;
   double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
@@ -146,6 +150,7 @@ void free_mesh(apollo_dg* h) {
   dfree(h->geo_d); dfree(h->faces_d); dfree(h->conn_d); dfree(h->einst_d);
   dfree(h->V_d); dfree(h->Dr_d); dfree(h->Ds_d); dfree(h->I_d); dfree(h->L_d); dfree(h->gz_d); dfree(h->gw_d);
   dfree(h->wmass_d); dfree(h->mass_d);
+  dfree(h->VS_d); dfree(h->cubr_d); dfree(h->cubs_d); dfree(h->srcv_d);
   dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
   dfree(h->TU_d); dfree(h->T0_d); dfree(h->T1_d);
   h->tu_valid = false;
@@ -196,6 +201,11 @@ DgDev make_dev(const apollo_dg* h) {
   d.tile_shape = h->tile_shape;
   d.wait_limit = h->wait_limit;
   d.debug_stall = h->debug_stall;
+  d.src = h->src;
+  d.VS = h->VS_d;
+  d.cub_r = h->cubr_d;
+  d.cub_s = h->cubs_d;
+  d.srcv = h->src.n > 0 ? h->srcv_d : nullptr;
   d.eqp = h->eqp;
   d.bcs = h->bcs;
   d.dtfac = 2. / 3. * h->cfg.cfl * h->dtscale;
@@ -376,6 +386,7 @@ apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const doubl
   else if (k == "maxwellTM") eq = EQ_MAXWELL_TM;
   else return fail(h, APOLLO_ERR_CONFIG, "unknown equation kind " + k);
   if (nparams < 0 || nparams > 4 || (nparams > 0 && !params)) return fail(h, APOLLO_ERR_ARG, "bad parameter list");
+  h->src.n = 0;  // sources name fields of the equation they were added for
   // the Euler kinds take three parameters; p[3] holds their numerical flux
   if ((eq == EQ_EULER || eq == EQ_EULER2D) && nparams > 3) return fail(h, APOLLO_ERR_ARG, "eulerEqn takes 3 parameters");
   EqParams p{};
@@ -389,6 +400,51 @@ apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const doubl
   h->eq = eq;
   h->eqp = p;
   h->M = fields_of(eq);
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_add_source(apollo_dg* h, const char* kind, const int* out_range, int nout,
+                                   const double* params, int nparams) {
+  if (!h || !kind || !out_range || nout < 1) return APOLLO_ERR_ARG;
+  if (h->eq < 0) return fail(h, APOLLO_ERR_STATE, "set the equation before its sources");
+  if (h->src.n >= kMaxSrc) return fail(h, APOLLO_ERR_CONFIG, "too many sources");
+  if (nparams < 0 || nparams > 9 || (nparams > 0 && !params)) return fail(h, APOLLO_ERR_ARG, "bad parameter list");
+  const std::string k(kind);
+  int kd = 0;
+  if (k == "tranverseMagneticSrc") {
+    kd = SRC_TM;
+    if (nparams != 0) return fail(h, APOLLO_ERR_ARG, "tranverseMagneticSrc takes no parameters");
+  } else if (k == "pointCurrentSrc") {
+    kd = SRC_POINT;
+    if (nparams != 9)
+      return fail(h, APOLLO_ERR_ARG, "pointCurrentSrc takes xLocation, yLocation, radius, currentDensity, "
+                                     "frequency, phase, charge, mass, epsilon0");
+  } else {
+    return fail(h, APOLLO_ERR_CONFIG, "unknown source " + k);
+  }
+  // both plugins write their first output only: OutRange[0] is the field, in
+  // Apollo's numbering, mapped to this handle's layout
+  const int a = out_range[0];
+  int f = -1;
+  switch (h->eq) {
+    case EQ_ADVECTION: f = a == 0 ? 0 : -1; break;
+    case EQ_EULER: f = a >= 0 && a < 5 ? a : -1; break;
+    case EQ_MAXWELL: f = a >= 0 && a < 8 ? a : -1; break;
+    case EQ_EULER2D: f = a == 0 ? 0 : a == 1 ? 1 : a == 2 ? 2 : a == 4 ? 3 : -1; break;
+    case EQ_MAXWELL_TM: f = a == 2 ? 0 : a == 3 ? 1 : a == 4 ? 2 : -1; break;
+  }
+  if (f < 0) return fail(h, APOLLO_ERR_CONFIG, "source output field " + std::to_string(a) + " is not a field of this equation");
+  const int i = h->src.n;
+  h->src.kind[i] = kd;
+  h->src.out[i] = f;
+  for (int j = 0; j < 9; ++j) h->src.p[i][j] = j < nparams ? params[j] : 0.0;
+  h->src.n = i + 1;
+  if (h->K > 0 && h->mixed && !h->srcv_d) {
+    const size_t nU = (size_t)h->K * h->ops.Np * h->M;
+    CK(dev_malloc((void**)&h->srcv_d, nU * sizeof(double)), "source alloc");
+  }
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return APOLLO_OK;
 }
 
@@ -650,6 +706,21 @@ apollo_status set_mesh_body(apollo_dg* h, int nverts, const double* vx, const do
   CK(upload(&h->wmass_d, o.mass_colsum.data(), o.mass_colsum.size()), "op upload");
   const Mat mass = inverse(o.VVT);
   CK(upload(&h->mass_d, mass.a.data(), mass.a.size()), "op upload");
+  {
+    // VS = VVT V^T diag(w): the source's share of the right-hand side
+    // (wxcubature2d.cc:297-325 adds VT (w J S) to the volume term, which the
+    // step multiplies by VVT / J)
+    std::vector<double> vs((size_t)o.Np * o.Nc, 0.0);
+    for (int n = 0; n < o.Np; ++n)
+      for (int c = 0; c < o.Nc; ++c) {
+        double acc = 0.0;
+        for (int j = 0; j < o.Np; ++j) acc += o.VVT(n, j) * o.Vc(c, j);
+        vs[(size_t)n * o.Nc + c] = acc * o.cub_w[c];
+      }
+    CK(upload(&h->VS_d, vs.data(), vs.size()), "op upload");
+    CK(upload(&h->cubr_d, o.cub_r.data(), o.cub_r.size()), "op upload");
+    CK(upload(&h->cubs_d, o.cub_s.data(), o.cub_s.size()), "op upload");
+  }
   CK(dev_malloc((void**)&h->U_d, nU * sizeof(double)), "state alloc");
   CK(dev_malloc((void**)&h->W_d, nU * sizeof(double)), "state alloc");
   CK(dev_malloc((void**)&h->in_d, nU * sizeof(double)), "state alloc");
@@ -669,6 +740,7 @@ apollo_status set_mesh_body(apollo_dg* h, int nverts, const double* vx, const do
     CK(cudaMemset(h->TU_d, 0, nTr * sizeof(float)), "trace clear");
     CK(cudaMemset(h->T0_d, 0, nTr * sizeof(float)), "trace clear");
     CK(cudaMemset(h->T1_d, 0, nTr * sizeof(float)), "trace clear");
+    if (h->src.n > 0) CK(dev_malloc((void**)&h->srcv_d, nU * sizeof(double)), "source alloc");
   }
   // halo: face-block indices of the blocks sent (local) and received (ghost)
   h->partitioned = part != nullptr;

@@ -964,7 +964,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
             const int n = i0 + u;
             if (n >= NP) break;
             const double* rs = RSUM + n * 5;
-            const double r = (double)dv[n] + rs[0] * Rbar + rs[1] * Sbar + rs[2] * F0 + rs[3] * F1 + rs[4] * F2;
+            double r = (double)dv[n] + rs[0] * Rbar + rs[1] * Sbar + rs[2] * F0 + rs[3] * F1 + rs[4] * F2;
+            if (d.srcv) r += d.srcv[((size_t)k * NP + n) * M + rf];  // the stage's source terms
             if (!isfinite(r)) err |= ERRB_NAN;
             if (a.mode == MODE_RHS) o[n] = r;
             else if (a.mode == MODE_STAGE) o[n] = xr[u] + c_stage * r;
@@ -1149,6 +1150,10 @@ cudaError_t launch_mixed_sh(MixedPlan* p, const DgDev& d, const StageArgs& a0, c
       a.tr_out = nullptr;
     }
     if (!a.tr_in) return cudaErrorInvalidValue;
+    if (d.srcv) {  // this stage's source terms, added by the epilogue
+      cudaError_t e = launch_source(EQ, d, a, d.srcv, 0, s);
+      if (e != cudaSuccess) return e;
+    }
     if (ev) cudaEventRecord(ev[1], s);
     // bit 0: the state is bulk-copied (16-byte aligned); bit 1: warm L2 with u0
     const int flags = (((uintptr_t)a.x & 15) == 0 ? 1 : 0) |
@@ -1199,6 +1204,10 @@ cudaError_t launch_fused(MixedPlan* p, const DgDev& d, const StageArgs& a0, cuda
     if (!a.tr_in) return cudaErrorInvalidValue;
     // the trace bulk stores need a 16-byte aligned destination
     if (a.tr_out && ((uintptr_t)a.tr_out & 15)) return cudaErrorInvalidValue;
+    if (d.srcv) {  // this stage's source terms, added by the epilogue
+      cudaError_t e = launch_source(EQ, d, a, d.srcv, 0, s);
+      if (e != cudaSuccess) return e;
+    }
     if (ev) cudaEventRecord(ev[1], s);
     const int flags = (((uintptr_t)a.x & 15) == 0 ? 1 : 0) |
                       (a.mode == MODE_FINAL && ((uintptr_t)a.u0 & 15) == 0 ? 2 : 0);

@@ -654,7 +654,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           if (n >= NP) break;
           const double* rs = RSUM + n * 5;
           const double dv = (double)(vh[u] + vl[u]);
-          const double rr = dv + rs[0] * Rbar + rs[1] * Sbar + rs[2] * F0 + rs[3] * F1 + rs[4] * F2;
+          double rr = dv + rs[0] * Rbar + rs[1] * Sbar + rs[2] * F0 + rs[3] * F1 + rs[4] * F2;
+          if (d.srcv) rr += d.srcv[((size_t)k * NP + n) * M + f];  // the stage's source terms
           if (!isfinite(rr)) err |= ERRB_NAN;
           if (a.mode == MODE_RHS) o[u] = rr;
           else if (a.mode == MODE_STAGE) o[u] = xr[u] + c_stage * rr;

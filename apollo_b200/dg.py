@@ -66,6 +66,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_create": (C.c_int, [C.POINTER(_Config), C.POINTER(H)]),
         "apollo_dg_set_equation": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_add_bc": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
+        "apollo_dg_add_source": (C.c_int, [H, C.c_char_p, _ip, C.c_int, _dp, C.c_int]),
         "apollo_dg_set_numerical_flux": (C.c_int, [H, C.c_char_p]),
         "apollo_dg_set_limiter": (C.c_int, [H, C.c_char_p, _dp, C.c_int]),
         "apollo_dg_averaging_weights": (C.c_int, [H, _dp]),
@@ -138,6 +139,9 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_set_equation_text": (C.c_int, [H, C.c_char_p, C.c_char_p]),
         "apollo_dg_add_bc_text": (C.c_int, [H, C.c_char_p, C.c_char_p]),
         "apollo_dg_set_limiter_text": (C.c_int, [H, C.c_char_p, C.c_char_p]),
+        "apollo_dg_deck_source": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, _ip, C.c_char_p, C.c_int, _ip, _ip,
+                                            _dp, _ip, C.c_char_p, C.c_int]),
+        "apollo_dg_add_source_text": (C.c_int, [H, C.c_char_p, C.c_char_p]),
         "apollo_dg_last_error": (C.c_char_p, [H]),
         "apollo_dg_destroy": (C.c_int, [H]),
     }
@@ -173,13 +177,15 @@ class NodalDG2d:
 
     def __init__(self, N: int, cfl: float, equation: str | None, eq_params, mesh: Mesh, bcs=(), device: int = 0,
                  stream: int | None = None, part=None, rank: int = 0, numerical_flux: str = "LF",
-                 deck: str | None = None):
+                 deck: str | None = None, sources=()):
         """``part`` (int32 [K], optional): a partition of ``mesh``; the handle then
         holds the elements with ``part == rank`` (apollo_dg_set_mesh_partition)
         and steps through ``apollo_b200.distributed.DistNodalDG2d``.
         ``deck`` (with ``equation`` None): Apollo input-deck text whose
-        equation block and boundary-condition list configure the handle
-        (apollo_dg_set_equation_text, apollo_dg_add_bc_text)."""
+        equation block, boundary-condition list and sources configure the
+        handle (apollo_dg_set_equation_text, apollo_dg_add_bc_text,
+        apollo_dg_add_source_text).  ``sources``: (kind, out_range, params)
+        triples (apollo_dg_add_source)."""
         self.lib = load_library()
         cfg = _Config(N, cfl, device, C.c_void_p(stream) if stream else None)
         h = C.c_void_p()
@@ -188,6 +194,7 @@ class NodalDG2d:
         if equation is None:
             self._check(self.lib.apollo_dg_set_equation_text(h, None, deck.encode()))
             self._check(self.lib.apollo_dg_add_bc_text(h, None, deck.encode()))
+            self._check(self.lib.apollo_dg_add_source_text(h, None, deck.encode()))
         else:
             p = np.asarray(list(eq_params), dtype=np.float64)
             self._check(self.lib.apollo_dg_set_equation(h, equation.encode(), p.ctypes.data_as(_dp), len(p)))
@@ -195,6 +202,11 @@ class NodalDG2d:
         for kind, params in bcs:
             bp = np.asarray(list(params), dtype=np.float64)
             self._check(self.lib.apollo_dg_add_bc(h, kind.encode(), bp.ctypes.data_as(_dp), len(bp)))
+        for kind, out, params in sources:
+            o = np.asarray(list(out), dtype=np.int32)
+            sp = np.asarray(list(params) or [0.0], dtype=np.float64)
+            self._check(self.lib.apollo_dg_add_source(h, kind.encode(), o.ctypes.data_as(_ip), len(o),
+                                                      sp.ctypes.data_as(_dp), len(params)))
         self.mesh = mesh
         if part is None:
             self._check(self.lib.apollo_dg_set_mesh(

@@ -107,15 +107,24 @@ apollo_status apollo_dg_deck_equation(const char* kind, const char* text, char* 
  * *count) as apollo_dg_add_bc's kind and params. */
 apollo_status apollo_dg_deck_bc(const char* kind, const char* text, int index, int* count, char* kind_out,
                                 int kind_len, double* params, int* nparams, char* err, int err_len);
+/* Host only: *count receives the number of sources the deck lists (the
+ * Sources of the block holding Equations; a text without Equations is one
+ * source's block); entry `index` as apollo_dg_add_source's kind, out_range[nout]
+ * (at most 8) and params. */
+apollo_status apollo_dg_deck_source(const char* kind, const char* text, int index, int* count, char* kind_out,
+                                    int kind_len, int* out_range, int* nout, double* params, int* nparams, char* err,
+                                    int err_len);
 /* Host only: the first block of the deck's Limiter list as
  * apollo_dg_set_limiter's kind and params (kind_out "" when there is none). */
 apollo_status apollo_dg_deck_limiter(const char* kind, const char* text, char* kind_out, int kind_len,
                                      double* params, int* nparams, char* err, int err_len);
 /* The same, applied to a handle: apollo_dg_set_equation (+ the numerical
- * flux), apollo_dg_add_bc for every listed condition in order, and
- * apollo_dg_set_limiter (removed when the deck lists none). */
+ * flux), apollo_dg_add_bc for every listed condition in order,
+ * apollo_dg_add_source for every listed source, and apollo_dg_set_limiter
+ * (removed when the deck lists none). */
 apollo_status apollo_dg_set_equation_text(apollo_dg* h, const char* kind, const char* text);
 apollo_status apollo_dg_add_bc_text(apollo_dg* h, const char* kind, const char* text);
+apollo_status apollo_dg_add_source_text(apollo_dg* h, const char* kind, const char* text);
 apollo_status apollo_dg_set_limiter_text(apollo_dg* h, const char* kind, const char* text);
 
 /* Euler numerical flux by Apollo's "Numerical_Flux" name (WxEulerEqn::setup,
@@ -168,6 +177,26 @@ apollo_status apollo_dg_set_launch_shape(apollo_dg* h, int grid_share, int tile_
  * weights (half the column sums of the reference mass matrix, Apollo's
  * LimiterElementAVE, src/lib/wxnodaldggeometry2d.h:84-98). */
 apollo_status apollo_dg_averaging_weights(const apollo_dg* h, double* w);
+
+/* Source plugin, appended to the equation's source set (WxHyperbolicSrcSet,
+ * src/hyper/wxhyperbolicsrcset.cc:16-71; "Sources = [...]"), for the kinds
+ * whose value depends on time and position only:
+ *   "tranverseMagneticSrc"   (no params; Apollo's spelling)
+ *        s = exp(t) (x (1-x) y (1-y) + 2 x (1-x) + 2 y (1-y))
+ *        (src/hyperapps/maxwell/wxtransversemagneticsrc.h:37-44)
+ *   "pointCurrentSrc"        xLocation, yLocation, radius, currentDensity,
+ *        frequency, phase, charge, mass, epsilon0: s = j0 q/(m eps0)
+ *        sin(omega t + phase) within radius of (x, y), 0 elsewhere
+ *        (src/hyperapps/maxwell/wxpointcurrent.h)
+ * out_range[nout]: the plugin's OutRange; its first entry is the field (in
+ * Apollo's numbering of the full equation: Ez of phMaxwellEqn is 2, also for
+ * "maxwellTM") that the source adds into.  As in Apollo the source is
+ * evaluated at the cubature points at the stage time and enters the volume
+ * term as V^T (w J S); every form (float64, mixed precision, partitioned,
+ * derivatives, the no-allocation right-hand side) includes it.  Up to 4
+ * sources; apollo_dg_set_equation clears them. */
+apollo_status apollo_dg_add_source(apollo_dg* h, const char* kind, const int* out_range, int nout,
+                                   const double* params, int nparams);
 
 /* Boundary-condition plugin, appended to the list; a face tagged t uses the
  * t-th condition added (Apollo's boundaryConditions[t-1]).  Kinds and params:

@@ -241,7 +241,31 @@ struct Oracle {
   int lim_kind = 0;  // 0: eulerLimiterHW, 1: tuAliabadiLimiter
   double lim_gamma = 1.4, lim_minP = 0.0, lim_minD = 0.0;
   std::vector<double> lim_ave;
+  // source plugins (orc_add_source): kind, output field (Apollo's index), params
+  std::vector<int> src_kind, src_out;
+  std::vector<double> src_par;  // [nsrc][9]
 };
+
+// Source plugins, WxHyperbolicSrc::compSource (src/hyper/wxhyperbolicsrc.cc:64-80)
+// adding src() into the output field.  kind 1: tranverseMagneticSrc
+// (src/hyperapps/maxwell/wxtransversemagneticsrc.h:37-44); kind 2:
+// pointCurrentSrc (src/hyperapps/maxwell/wxpointcurrent.h: setup keys xLocation,
+// yLocation, radius, currentDensity, frequency, phase, charge, mass, epsilon0).
+// tx = [t, x, y].
+void add_sources(const Oracle& o, const double* tx, double* s) {
+  for (size_t i = 0; i < o.src_kind.size(); ++i) {
+    const double* p = &o.src_par[i * 9];
+    const double t = tx[0], x = tx[1], y = tx[2];
+    double v = 0.0;
+    if (o.src_kind[i] == 1) {
+      v = std::exp(t) * (x * (1 - x) * y * (1 - y) + 2. * x * (1 - x) + 2 * y * (1 - y));
+    } else if (o.src_kind[i] == 2) {
+      const double qbyme = p[6] / (p[7] * p[8]);
+      if (std::sqrt((x - p[0]) * (x - p[0]) + (y - p[1]) * (y - p[1])) < p[2]) v = p[3] * qbyme * std::sin(p[4] * t + p[5]);
+    }
+    s[o.src_out[i]] += v;
+  }
+}
 
 // ----------------------------------------------------------- plugins ----
 // Advection: wxadvectioneqn.cc:176-208
@@ -654,6 +678,25 @@ void* orc_create(int N, int eq, const double* eqp, int nverts, const double* vx,
 }
 
 void orc_destroy(void* h) { delete (Oracle*)h; }
+
+// A source plugin (kind 1 tranverseMagneticSrc, 2 pointCurrentSrc) adding into
+// field `out` (Apollo's field index); params[9] as add_sources reads them.
+int orc_add_source(void* h, int kind, int out, const double* params) {
+  Oracle& o = *(Oracle*)h;
+  if (kind < 1 || kind > 2 || out < 0 || out >= o.meqn) return 1;
+  o.src_kind.push_back(kind);
+  o.src_out.push_back(out);
+  for (int i = 0; i < 9; ++i) o.src_par.push_back(params ? params[i] : 0.0);
+  return 0;
+}
+
+// The source terms at (t, x, y) for a state q (the plugins' own value check).
+void orc_source_terms(void* h, double t, double x, double y, double* s) {
+  Oracle& o = *(Oracle*)h;
+  double tx[5] = {t, x, y, 0.0, 0.0};
+  for (int c = 0; c < o.meqn; ++c) s[c] = 0.0;
+  add_sources(o, tx, s);
+}
 int orc_meqn(void* h) { return ((Oracle*)h)->meqn; }
 int orc_np(void* h) { return ((Oracle*)h)->Np; }
 int orc_nc(void* h) { return ((Oracle*)h)->Nc; }
@@ -726,6 +769,8 @@ double orc_rhs(void* h, double t, double dt, const double* u, double* rhs) {
         eq_flux(o, 0, &Iq[p * m], F.data());
         eq_flux(o, 1, &Iq[p * m], G.data());
         for (int c = 0; c < m; ++c) { If[p * m + c] = F[c]; Ig[p * m + c] = G[c]; Isrc[p * m + c] = 0.0; }
+        // sourceTerms (src/hyper/wxhyperbolicsrcset.cc:59-71) at the cubature point
+        add_sources(o, xc5.data(), &Isrc[p * m]);
       }
       // evaluatedVolumeIntegrals + geometricFactors2D (wxcubature2d.cc:297-356)
       mat_vec(Nc, Np, 1, o.Drc.data(), xk, xr.data());

@@ -22,6 +22,8 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libapollo_ref.so")
 
 EQ_ADVECTION, EQ_EULER, EQ_MAXWELL = 0, 1, 2
+# source plugins (Apollo kind names tranverseMagneticSrc, pointCurrentSrc)
+SRC_TM, SRC_POINT = 1, 2
 BC_FIXED, BC_VORTEX, BC_TM, BC_PEC = 0, 1, 2, 3
 BC_EULER_WALL, BC_EULER_INFLOW, BC_EULER_ZEROGRAD, BC_EULER_DIRICHLET = 4, 5, 6, 7
 # Euler numerical fluxes (eqp[3]), Apollo's Numerical_Flux codes
@@ -87,6 +89,10 @@ def _lib():
     lib.orc_set_limiter.restype = C.c_int
     lib.orc_limit.argtypes = [C.c_void_p, _dp]
     lib.orc_limit.restype = None
+    lib.orc_add_source.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+    lib.orc_add_source.restype = C.c_int
+    lib.orc_source_terms.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _dp]
+    lib.orc_source_terms.restype = None
     lib.orc_set_limiter_ta.argtypes = [C.c_void_p]
     lib.orc_set_limiter_ta.restype = C.c_int
     lib.orc_ta_prim.argtypes = [C.c_void_p, _dp, _dp]
@@ -183,6 +189,20 @@ class Oracle:
         assert u.flags.c_contiguous and u.dtype == np.float64
         return self.lib.orc_ssp_step(self.h, _p(u), t0, dt)
 
+    def add_source(self, kind: int, out: int, params=()) -> None:
+        """A source plugin adding into Apollo field `out` (SRC_TM; SRC_POINT
+        with xLocation, yLocation, radius, currentDensity, frequency, phase,
+        charge, mass, epsilon0)."""
+        p = np.zeros(9)
+        p[:len(params)] = params
+        if self.lib.orc_add_source(self.h, kind, out, _p(p)) != 0:
+            raise ValueError("bad source")
+
+    def source_terms(self, t: float, x: float, y: float):
+        out = np.zeros(self.meqn)
+        self.lib.orc_source_terms(self.h, t, x, y, _p(out))
+        return out
+
     def set_limiter(self, gamma: float, min_pressure: float, min_density: float) -> None:
         """Apollo's eulerLimiterHW on every stage input (5 fields, N <= 4)."""
         if self.lib.orc_set_limiter(self.h, gamma, min_pressure, min_density) != 0:
@@ -249,6 +269,10 @@ class RefPlugins:
         lib.ref_exprfunc_destroy.argtypes = [C.c_void_p]
         lib.ref_primitive.argtypes = [C.c_void_p, _dp, _dp]
         lib.ref_ta_limit.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        lib.ref_src_create.restype = C.c_void_p
+        lib.ref_src_create.argtypes = [C.c_char_p, C.c_int]
+        lib.ref_src_eval.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _dp, _dp]
+        lib.ref_src_destroy.argtypes = [C.c_void_p]
         self.lib = lib
 
     @staticmethod
@@ -295,6 +319,22 @@ class RefPlugins:
     def speed2(self, h, q) -> float:
         q = np.ascontiguousarray(q, dtype=np.float64)
         return self.lib.ref_speed2(h, _p(q))
+
+    def sources(self, blocks: dict, meqn: int):
+        """Apollo's source set from {name: (kind, {key: value})}."""
+        body = "".join(f" <{n}>\n  Kind = {k}\n" + "".join(f"  {a} = {v}\n" for a, v in kv.items()) + f" </{n}>\n"
+                       for n, (k, kv) in blocks.items())
+        text = f"<top>\n Sources = [{', '.join(blocks)}]\n{body}</top>\n"
+        h = self.lib.ref_src_create(text.encode(), meqn)
+        if not h:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return h
+
+    def source_terms(self, h, meqn: int, t: float, x: float, y: float, q=None):
+        q = np.zeros(meqn) if q is None else np.array(q, dtype=np.float64)
+        s = np.zeros(meqn)
+        self.lib.ref_src_eval(h, t, x, y, _p(q), _p(s))
+        return s
 
     def exprfunc(self, text: str):
         h = self.lib.ref_exprfunc_create(text.encode())

@@ -9,6 +9,9 @@
 //   WxHyperbolicEqnSet<double>::setup/flux/DGnumericalFlux/riemann
 //     (src/hyper/wxhyperboliceqnset.cc:43-89, 163-204, 295-328)
 //   WxExprFunc::setup/func (src/lib/wxexprfunction.cc:4-59)
+//   WxHyperbolicSrcSet<double>::setup/sourceTerms (src/hyper/wxhyperbolicsrcset.cc:16-71)
+//     with the tranverseMagneticSrc and pointCurrentSrc plugins
+//     (src/hyperapps/maxwell/wxtransversemagneticsrc.h, wxpointcurrent.h)
 #include <sstream>
 #include <string>
 #include <vector>
@@ -22,12 +25,18 @@
 #include "advection/wxadvectioneqn.h"
 #include "euler/wxeulereqn.h"
 #include "maxwell/wxphmaxwelleqn.h"
+#include <wxhyperbolicsrcset.h>
+#include "maxwell/wxtransversemagneticsrc.h"
+#include "maxwell/wxpointcurrent.h"
 
 // Registration of the three equation kinds under their Apollo names, as
 // src/hyperapps/aphyperapps_register.cc does for the full build.
 static WxCreator<WxAdvectionEqn<double>, WxHyperbolicEqn<double> > reg_adv("advectionEqn");
 static WxCreator<WxEulerEqn<double>, WxHyperbolicEqn<double> > reg_euler("eulerEqn");
 static WxCreator<WxPHMaxwellEqn<double>, WxHyperbolicEqn<double> > reg_maxwell("phMaxwellEqn");
+// and the two closed-form source kinds (aphyperapps_register.cc:113-118)
+static WxCreator<WxTransverseMagneticSrc<double>, WxHyperbolicSrc<double> > reg_tmsrc("tranverseMagneticSrc");
+static WxCreator<WxpointCurrentSrc<double>, WxHyperbolicSrc<double> > reg_pcsrc("pointCurrentSrc");
 
 namespace {
 struct RefEqn {
@@ -149,5 +158,29 @@ void ref_exprfunc_eval(void* h, double t, double x, double y, double* out) {
 }
 
 void ref_exprfunc_destroy(void* h) { delete (WxExprFunc*)h; }
+
+// Source set of `meqn` fields from a cryptset holding `Sources = [...]` and
+// the sources' own sets under one top-level set.
+void* ref_src_create(const char* text, int meqn) {
+  try {
+    std::istringstream in(text);
+    WxCryptSet wxc(in);
+    WxHyperbolicSrcSet<double>* s = new WxHyperbolicSrcSet<double>();
+    s->setNumEqns((unsigned)meqn);
+    s->setup(wxc);
+    return s;
+  } catch (...) {
+    g_err = "source setup failed";
+    return nullptr;
+  }
+}
+
+// sourceTerms at tx = [t, x, y, 0, 0] for the state q (s receives meqn values).
+void ref_src_eval(void* h, double t, double x, double y, double* q, double* s) {
+  double tx[5] = {t, x, y, 0.0, 0.0};
+  ((WxHyperbolicSrcSet<double>*)h)->sourceTerms(tx, q, nullptr, s);
+}
+
+void ref_src_destroy(void* h) { delete (WxHyperbolicSrcSet<double>*)h; }
 
 }  // extern "C"

@@ -89,7 +89,16 @@ CASES = [
      "eulerEqn", dict(gas_gamma=1.4, Numerical_Flux="HLL", minPressure=1e-6, minDensity=1e-6), CHANNEL_BCS, 4),
     ("maxwell_talimiter_N3", problems.maxwell_tm, dict(n=6, N=3, fields=8, seed=7), orc.EQ_MAXWELL, (1.0, 0.0, 0.0),
      "phMaxwellEqn", dict(c0=1.0), ((orc.BC_TM, ()),), 3),
+    ("maxwell_src_N3", problems.maxwell_tm, dict(n=7, N=3, fields=8, seed=8), orc.EQ_MAXWELL, (1.0, 1.0, 1.0),
+     "phMaxwellEqn", dict(c0=1.0, gamma=1.0, chi=1.0), ((orc.BC_PEC, ()),), 4),
 ]
+
+# source plugins per case (kind, Apollo output field, params), Apollo's example
+# TM2DwithSource.pin (tranverseMagneticSrc into Ez, phMaxwellEqn with chi =
+# gamma = 1, conducting walls) plus a point current into Ez
+SOURCES = {"maxwell_src_N3": ((orc.SRC_TM, 2, ()),
+                              (orc.SRC_POINT, 2, (0.4, 0.6, 0.15, 2.0, 5.0, 0.2, 1.0, 1.0, 1.0)))}
+SRC_NAMES = {orc.SRC_TM: "tranverseMagneticSrc", orc.SRC_POINT: "pointCurrentSrc"}
 
 # the limiter per case: eulerLimiterHW with its own (gas_gamma, min_pressure,
 # min_density), or tuAliabadiLimiter, which takes the equation's parameters
@@ -110,6 +119,14 @@ def make_case(name, builder, kw, eq, eqp, ref_kind, ref_params, bcs, steps, ref)
     U0 = np.ascontiguousarray(prob.ic(x, y), dtype=np.float64)
     lim = LIMITERS.get(name)
     extra = {}
+    srcs = SOURCES.get(name, ())
+    for kind, out, params in srcs:
+        o.add_source(kind, out, params)
+    if srcs:
+        extra["src_kinds"] = np.asarray([SRC_NAMES[k] for k, _, _ in srcs])
+        extra["src_out"] = np.asarray([out for _, out, _ in srcs], dtype=np.int32)
+        extra["src_params"] = np.asarray([list(p) + [0.0] * (9 - len(p)) for _, _, p in srcs], dtype=np.float64)
+        extra["src_nparams"] = np.asarray([len(p) for _, _, p in srcs], dtype=np.int32)
     if lim is not None:
         # the limiter (restated in the oracle; Apollo's needs PETSc's DMPlex)
         # acts on every stage input, and on the input of a single right-hand side

@@ -25,6 +25,9 @@ def load(name):
     par = d.get("bc_params", np.zeros((len(d["bc_kinds"]), 8)))
     d["bcs"] = tuple((BC_NAMES[int(k)], tuple(par[i][:BC_NPARAMS[int(k)]])) for i, k in enumerate(d["bc_kinds"]))
     d["numflux"] = str(d["numflux"]) if "numflux" in d else "LF"
+    d["sources"] = tuple((str(k), (int(o),), tuple(p[:n])) for k, o, p, n in
+                         zip(d.get("src_kinds", ()), d.get("src_out", ()), d.get("src_params", ()),
+                             d.get("src_nparams", ())))
     return d
 
 

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 def _fixture_solver(g):
     return NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
-                     numerical_flux=g["numflux"])
+                     numerical_flux=g["numflux"], sources=g["sources"])
 
 
 @pytest.mark.parametrize("name", NAMES)

@@ -28,6 +28,13 @@ def deck_for(g):
         keys = "\n".join(f"    {k} = {float(v)!r}" for k, v in zip(BC_KEYS.get(bk, ()), bp))
         blocks.append(f"  <{nm}>\n    Type = ApSubSolver\n    Kind = {bk}\n{keys}\n  </{nm}>")
     flux = f"      Numerical_Flux = {g['numflux']}\n" if kind == "eulerEqn" else ""
+    SRC_KEYS = ("xLocation", "yLocation", "radius", "currentDensity", "frequency", "phase", "charge", "mass",
+                "epsilon0")
+    snames = [f"src{i}" for i in range(len(g["sources"]))]
+    for nm, (sk, out, sp) in zip(snames, g["sources"]):
+        keys = "".join(f"    {k} = {float(v)!r}\n" for k, v in zip(SRC_KEYS, sp))
+        blocks.append(f"  <{nm}>\n    Type = WxHyperbolicSrc\n    Kind = {sk}\n    OutRange = [{out[0]}]\n{keys}  </{nm}>")
+    srcline = f"Sources = [{', '.join(snames)}]" if snames else ""
     lim = ""
     if "limiter" in g:
         lk = str(g.get("limiter_kind", "eulerLimiterHW"))
@@ -43,6 +50,7 @@ ORDER = {int(g['N'])}
      Equations = [eq]
      boundaryConditions = [{', '.join(names)}]
      {'Limiter = [lim]' if lim else ''}
+     {srcline}
      polynomialOrder = ORDER
      cfl = {float(g['cfl'])!r}
      <eq>
@@ -57,13 +65,14 @@ ORDER = {int(g['N'])}
 """
 
 
-@pytest.mark.parametrize("name", ["euler_N4", "euler_hll_N3", "euler_hll_limiter_N3", "maxwell_N5", "adv_N3"])
+@pytest.mark.parametrize("name", ["euler_N4", "euler_hll_N3", "euler_hll_limiter_N3", "maxwell_N5", "adv_N3",
+                                  "maxwell_src_N3"])
 def test_deck_configured_handle_matches(name):
     g = load(name)
     text = deck_for(g)
     s = solver_from_deck(text, g["mesh"])
     ref = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
-                    numerical_flux=g["numflux"])
+                    numerical_flux=g["numflux"], sources=g["sources"])
     if "limiter" in g:
         ref.set_limiter(str(g.get("limiter_kind", "eulerLimiterHW")), g["limiter"])
     a, sa = s.step(0.0, 0.0, g["U0"])

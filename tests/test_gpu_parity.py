@@ -17,7 +17,7 @@ RHS_TOL_CANCELLING = 1e-11
 
 def _solver(g):
     s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
-                  numerical_flux=g["numflux"])
+                  numerical_flux=g["numflux"], sources=g["sources"])
     if "limiter" in g:
         s.set_limiter(str(g.get("limiter_kind", "eulerLimiterHW")), g["limiter"])
     return s

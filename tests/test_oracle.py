@@ -20,6 +20,8 @@ def test_oracle_port_reproduces_golden(oracle_lib, name):
     g = load(name)
     bcs = tuple((int(k), tuple(g["bc_params"][i]) if "bc_params" in g else ()) for i, k in enumerate(g["bc_kinds"]))
     o = orc.Oracle(g["mesh"], int(g["N"]), int(g["eq"]), g["eqp"], bcs=bcs, cfl=float(g["cfl"]))
+    for kind, out, params in g["sources"]:
+        o.add_source({"tranverseMagneticSrc": orc.SRC_TM, "pointCurrentSrc": orc.SRC_POINT}[kind], out[0], params)
     x, y = o.node_coords()
     np.testing.assert_array_equal(x, g["x"])
     if "limiter" in g:
@@ -38,6 +40,31 @@ def test_oracle_port_reproduces_golden(oracle_lib, name):
     assert n == int(g["steps"])
     assert rel_l2(U, g["U_end"]) <= 1e-14
     assert t == pytest.approx(float(g["t_end"]), rel=1e-15)
+
+
+def test_sources_bitexact_vs_reference(oracle_lib):
+    """The restated source plugins (tranverseMagneticSrc, pointCurrentSrc)
+    equal Apollo's own, compiled unmodified, through its source set
+    (WxHyperbolicSrcSet::sourceTerms with OutRange)."""
+    orc = oracle_lib
+    if not orc.RefPlugins.available():
+        pytest.skip("Apollo's plugins are not built on this machine")
+    ref = orc.RefPlugins()
+    wire = {"OutRange": "[2]", "xLocation": 0.3, "yLocation": 0.6, "radius": 0.2, "currentDensity": 1.5,
+            "frequency": 6.0, "phase": 0.3, "charge": 1.0, "mass": 2.0, "epsilon0": 0.5}
+    h = ref.sources({"current": ("tranverseMagneticSrc", {"OutRange": "[2]"}), "wire": ("pointCurrentSrc", wire)}, 8)
+    from apollo_b200.mesh import jittered_square
+    o = orc.Oracle(jittered_square(5, periodic=False), 3, orc.EQ_MAXWELL, (1.0, 1.0, 1.0), bcs=((orc.BC_PEC, ()),))
+    o.add_source(orc.SRC_TM, 2)
+    o.add_source(orc.SRC_POINT, 2, (0.3, 0.6, 0.2, 1.5, 6.0, 0.3, 1.0, 2.0, 0.5))
+    rng = np.random.default_rng(0)
+    hits = 0
+    for _ in range(2000):
+        t, x, y = rng.uniform(0, 2), rng.uniform(0, 1), rng.uniform(0, 1)
+        a = ref.source_terms(h, 8, t, x, y)
+        np.testing.assert_array_equal(o.source_terms(t, x, y), a)
+        hits += (x - 0.3) ** 2 + (y - 0.6) ** 2 < 0.04
+    assert hits > 50  # the point current's disc was sampled
 
 
 def test_plugins_bitexact_vs_reference(oracle_lib):

@@ -31,7 +31,7 @@ def test_noalloc_matches_rhs_twice(name):
     torch = pytest.importorskip("torch")
     g = load(name)
     s = NodalDG2d(int(g["N"]), float(g["cfl"]), g["equation"], g["eqp"][:3], g["mesh"], bcs=g["bcs"],
-                  numerical_flux=g["numflux"])
+                  numerical_flux=g["numflux"], sources=g["sources"])
     u = torch.from_numpy(g["U0"]).cuda()
     if "limiter" in g:
         # the limiter needs scratch of its own: such handles are refused
