@@ -18,6 +18,7 @@
 #include "dg_mixed.h"
 #include "dg_operators.h"
 #include "dg_partition.h"
+#include "dg_revolve.h"
 
 using namespace apollo;
 
@@ -66,6 +67,9 @@ struct apollo_dg {
   std::vector<double*> ckpt;
   double* seg_d = nullptr;
   int seg_steps = 0;
+  int tr_snapshots = 0;  // > 0: the last forward was apollo_dg_forward_revolve with this many slots
+  long long tr_forward_steps = 0;  // forward steps the last revolve backward sweep re-ran
+  RevolvePlan revolve;
   int tr_nsteps = 0, tr_every = 0;
   double tr_t0 = 0.0, tr_dt = 0.0;
   bool tr_valid = false;
@@ -1303,6 +1307,161 @@ apollo_status apollo_dg_debug_set_waits(apollo_dg* h, unsigned polls, int stall_
 
 const char* apollo_dg_last_error(const apollo_dg* h) { return h ? h->err.c_str() : "null handle"; }
 
+}  // extern "C"
+
+namespace {
+
+// exactly n checkpoint states (extra ones of an earlier schedule are freed, so
+// the derivative memory reported is the current schedule's)
+apollo_status size_checkpoints(apollo_dg* h, int n) {
+  const size_t nU = state_doubles(h);
+  while ((int)h->ckpt.size() > n) {
+    dfree(h->ckpt.back());
+    h->ckpt.pop_back();
+  }
+  while ((int)h->ckpt.size() < n) {
+    double* p = nullptr;
+    CK(dev_malloc((void**)&p, nU * sizeof(double)), "checkpoint alloc");
+    h->ckpt.push_back(p);
+  }
+  return APOLLO_OK;
+}
+
+// stage states of `steps` steps (5 each) for the backward sweep
+apollo_status size_segment(apollo_dg* h, int steps) {
+  if (h->seg_steps == steps) return APOLLO_OK;
+  dfree(h->seg_d);
+  h->seg_steps = 0;
+  const size_t nU = state_doubles(h);
+  CK(dev_malloc((void**)&h->seg_d, (size_t)5 * steps * nU * sizeof(double)), "segment alloc");
+  h->seg_steps = steps;
+  return APOLLO_OK;
+}
+
+// the five stage states of step n (time tn) from its input state in S0; the
+// stage outputs go to S1..S4 (each stage of the step reads only the previous)
+apollo_status record_step(apollo_dg* h, double* const S[5], double tn, double dt) {
+  for (int s = 0; s < 4; ++s) {
+    apollo_status r = fixed_stage(h, s, S[s], nullptr, S[s + 1], tn, dt);
+    if (r) return r;
+  }
+  return APOLLO_OK;
+}
+
+// the adjoint of one step from its recorded stage states: A0 holds the
+// adjoint of the step's result on entry and of its input on return
+apollo_status reverse_step(apollo_dg* h, double* const S[5], double tn, double dt) {
+  const double c = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
+  double *A0 = h->A_d[0], *A1 = h->A_d[1], *A2 = h->A_d[2];
+  apollo_status r = adjoint_stage(h, S[4], A0, nullptr, A1, c_al, c_be, 0.0, stage_time(4, tn, dt));
+  if (!r) r = adjoint_stage(h, S[3], A1, nullptr, A2, 1.0, c, 0.0, stage_time(3, tn, dt));
+  if (!r) r = adjoint_stage(h, S[2], A2, nullptr, A1, 1.0, c, 0.0, stage_time(2, tn, dt));
+  if (!r) r = adjoint_stage(h, S[1], A1, nullptr, A2, 1.0, c, 0.0, stage_time(1, tn, dt));
+  if (!r) r = adjoint_stage(h, S[0], A2, A0, A0, 1.0, c, c_ga, stage_time(0, tn, dt));
+  return r;
+}
+
+// The device executor of the binomial reversal: slots are h->ckpt, the work
+// buffer is the tangent's state buffer (free during a backward sweep), and a
+// step is recorded into the five stage states of the segment buffer.
+struct RevolveDevice {
+  apollo_dg* h;
+  double t0, dt;
+  double* S[5];
+  double* work;
+  long long forward_steps = 0;
+  double* buf(int slot) { return slot < 0 ? work : h->ckpt[slot]; }
+  int copy(int dst, int src) {
+    const size_t nU = state_doubles(h);
+    CK(cudaMemcpyAsync(buf(dst), buf(src), nU * sizeof(double), cudaMemcpyDeviceToDevice, h->stream), "snapshot");
+    return APOLLO_OK;
+  }
+  int advance(int slot, int from, int count) {
+    for (int n = 0; n < count; ++n) {
+      apollo_status r = fixed_step(h, buf(slot), t0 + (from + n) * dt, dt);
+      if (r) return r;
+      ++forward_steps;
+    }
+    return APOLLO_OK;
+  }
+  int leaf(int j, int slot) {
+    const size_t nU = state_doubles(h);
+    CK(cudaMemcpyAsync(S[0], buf(slot), nU * sizeof(double), cudaMemcpyDeviceToDevice, h->stream), "restore");
+    apollo_status r = record_step(h, S, t0 + j * dt, dt);
+    if (r) return r;
+    ++forward_steps;
+    return reverse_step(h, S, t0 + j * dt, dt);
+  }
+};
+
+// The host executor: follows the same schedule, checks that every slot holds
+// the step it is used for and that the steps are reversed last to first.
+struct RevolveCount {
+  std::vector<int> pos;
+  int work = -1, next;
+  long long forward_steps = 0;
+  bool ok = true;
+  int& at(int slot) { return slot < 0 ? work : pos[slot]; }
+  int copy(int dst, int src) {
+    at(dst) = at(src);
+    return 0;
+  }
+  int advance(int slot, int from, int count) {
+    if (at(slot) != from) ok = false;
+    at(slot) += count;
+    forward_steps += count;
+    return 0;
+  }
+  int leaf(int j, int slot) {
+    if (at(slot) != j || j != next) ok = false;
+    --next;
+    ++forward_steps;
+    return 0;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+apollo_status apollo_dg_forward_revolve(apollo_dg* h, int nsteps, double t0, double dt, int snapshots) {
+  apollo_status r = check_whole(h);
+  if (r) return r;
+  if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "the derivatives do not support the limiter");
+  if (nsteps < 1 || snapshots < 1 || !(dt > 0.0)) return fail(h, APOLLO_ERR_ARG, "nsteps, snapshots >= 1, dt > 0");
+  if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  r = ensure_deriv_buffers(h);
+  if (!r) r = size_checkpoints(h, snapshots);
+  if (!r) r = size_segment(h, 1);
+  if (r) return r;
+  const size_t nU = state_doubles(h);
+  h->tr_valid = false;
+  h->tu_valid = false;
+  r = clear_errors(h);
+  if (r) return r;
+  h->revolve.build(nsteps, snapshots);
+  const std::vector<int> spine = h->revolve.spine();
+  size_t next = 0;
+  for (int n = 0; n < nsteps; ++n) {
+    if (next < spine.size() && spine[next] == n) {
+      CK(cudaMemcpyAsync(h->ckpt[next], h->U_d, nU * sizeof(double), cudaMemcpyDeviceToDevice, h->stream),
+         "checkpoint");
+      ++next;
+    }
+    r = fixed_step(h, h->U_d, t0 + n * dt, dt);
+    if (r) return r;
+  }
+  r = finish(h);
+  if (r) return r;
+  h->tr_nsteps = nsteps;
+  h->tr_every = 0;
+  h->tr_snapshots = snapshots;
+  h->tr_t0 = t0;
+  h->tr_dt = dt;
+  h->tr_valid = true;
+  return APOLLO_OK;
+}
+
 apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, double dt, int checkpoint_every) {
   apollo_status r = check_whole(h);
   if (r) return r;
@@ -1313,11 +1472,9 @@ apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, doubl
   if (r) return r;
   const size_t nU = state_doubles(h);
   const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
-  while ((int)h->ckpt.size() < nck) {
-    double* p = nullptr;
-    CK(dev_malloc((void**)&p, nU * sizeof(double)), "checkpoint alloc");
-    h->ckpt.push_back(p);
-  }
+  r = size_checkpoints(h, nck);
+  if (!r) r = size_segment(h, checkpoint_every);
+  if (r) return r;
   h->tr_valid = false;
   h->tu_valid = false;
   r = clear_errors(h);
@@ -1333,6 +1490,7 @@ apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, doubl
   if (r) return r;
   h->tr_nsteps = nsteps;
   h->tr_every = checkpoint_every;
+  h->tr_snapshots = 0;
   h->tr_t0 = t0;
   h->tr_dt = dt;
   h->tr_valid = true;
@@ -1346,13 +1504,24 @@ apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* uba
   if (!ubar_T || !ubar_0) return APOLLO_ERR_ARG;
   if (!h->tr_valid) return fail(h, APOLLO_ERR_STATE, "no trajectory: call apollo_dg_forward_fixed first");
   const size_t nU = state_doubles(h);
+  if (h->tr_snapshots > 0) {
+    // binomial schedule from the spine the forward pass stored
+    RevolveDevice dev{h, h->tr_t0, h->tr_dt, {}, h->tU_d};
+    for (int s = 0; s < 5; ++s) dev.S[s] = h->seg_d + (size_t)s * nU;
+    RevolveRun<RevolveDevice> rv{h->revolve, dev};
+    r = clear_errors(h);
+    if (!r) r = copy_in(h, h->A_d[0], ubar_T, where);
+    if (!r) r = (apollo_status)rv.run();
+    if (!r) r = copy_out(h, ubar_0, h->A_d[0], where);
+    if (r) return r;
+    h->tr_forward_steps = dev.forward_steps;
+    return finish(h);
+  }
   const int C = h->tr_every, nsteps = h->tr_nsteps, nseg = (nsteps + C - 1) / C;
   const double dt = h->tr_dt, c = dt / 4.0, c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
   if (h->seg_steps < C) {
-    dfree(h->seg_d);
-    h->seg_steps = 0;
-    CK(dev_malloc((void**)&h->seg_d, (size_t)5 * C * nU * sizeof(double)), "segment alloc");
-    h->seg_steps = C;
+    r = size_segment(h, C);
+    if (r) return r;
   }
   auto S = [&](int j, int s) { return h->seg_d + ((size_t)j * 5 + s) * nU; };
   double *A0 = h->A_d[0], *A1 = h->A_d[1], *A2 = h->A_d[2];
@@ -1478,6 +1647,29 @@ apollo_status apollo_dg_rhs_vjp(apollo_dg* h, double t, const double* x, const d
     if (r) return r;
   }
   return finish(h);
+}
+
+apollo_status apollo_dg_revolve_schedule(int nsteps, int snapshots, long long* recomputed_steps, int* spine_states) {
+  if (nsteps < 1 || snapshots < 1 || !recomputed_steps) return APOLLO_ERR_ARG;
+  RevolvePlan plan;
+  plan.build(nsteps, snapshots);
+  const std::vector<int> spine = plan.spine();
+  RevolveCount cnt;
+  cnt.pos.assign(snapshots, -1);
+  for (size_t k = 0; k < spine.size(); ++k) cnt.pos[k] = spine[k];
+  cnt.next = nsteps - 1;
+  RevolveRun<RevolveCount> rv{plan, cnt};
+  rv.run();
+  if (!cnt.ok || cnt.next != -1) return APOLLO_ERR_STATE;
+  *recomputed_steps = cnt.forward_steps;
+  if (spine_states) *spine_states = (int)spine.size();
+  return APOLLO_OK;
+}
+
+apollo_status apollo_dg_adjoint_stats(const apollo_dg* h, long long* recomputed_steps) {
+  if (!h || !recomputed_steps) return APOLLO_ERR_ARG;
+  *recomputed_steps = h->tr_snapshots > 0 ? h->tr_forward_steps : (long long)h->tr_nsteps;
+  return APOLLO_OK;
 }
 
 apollo_status apollo_dg_adjoint_memory(const apollo_dg* h, size_t* bytes) {

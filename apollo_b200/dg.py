@@ -94,6 +94,9 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_rhs_noalloc": (C.c_int, [H, C.c_double, C.c_double, C.c_void_p, C.c_void_p, _dp, C.c_void_p]),
         "apollo_dg_forward_fixed": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_int]),
         "apollo_dg_backward": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_int]),
+        "apollo_dg_forward_revolve": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_int]),
+        "apollo_dg_adjoint_stats": (C.c_int, [H, C.POINTER(C.c_longlong)]),
+        "apollo_dg_revolve_schedule": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
         "apollo_dg_tangent": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_int]),
         "apollo_dg_rhs_jvp": (C.c_int, [H, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
         "apollo_dg_rhs_vjp": (C.c_int, [H, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
@@ -377,6 +380,28 @@ class NodalDG2d:
     def forward_fixed(self, nsteps: int, t0: float, dt: float, checkpoint_every: int):
         """Advance the resident state by nsteps fixed steps, keeping checkpoints for backward()."""
         self._check(self.lib.apollo_dg_forward_fixed(self.h, nsteps, t0, dt, checkpoint_every))
+
+    def forward_revolve(self, nsteps: int, t0: float, dt: float, snapshots: int):
+        """Advance the resident state by nsteps fixed steps with `snapshots`
+        state slots (the initial state's included) for backward(), which then
+        follows the binomial (revolve) schedule."""
+        self._check(self.lib.apollo_dg_forward_revolve(self.h, nsteps, t0, dt, snapshots))
+
+    @staticmethod
+    def revolve_schedule(nsteps: int, snapshots: int):
+        """(forward steps the revolve backward sweep runs, states the forward
+        pass stores) for a trajectory of nsteps steps; host only."""
+        lib = load_library()
+        n, k = C.c_longlong(), C.c_int()
+        rc = lib.apollo_dg_revolve_schedule(nsteps, snapshots, C.byref(n), C.byref(k))
+        if rc:
+            raise ApolloError(rc, "revolve schedule")
+        return n.value, k.value
+
+    def recomputed_steps(self) -> int:
+        n = C.c_longlong()
+        self._check(self.lib.apollo_dg_adjoint_stats(self.h, C.byref(n)))
+        return n.value
 
     def backward(self, ubar_T, out=None):
         """dJ/dU(0) of the last forward_fixed trajectory, given dJ/dU(T)."""

@@ -325,6 +325,28 @@ apollo_status apollo_dg_rhs_noalloc(apollo_dg* h, double t, double dt, const dou
  * states) for apollo_dg_backward. */
 apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, double dt, int checkpoint_every);
 
+/* The same trajectory with binomial checkpointing (Griewank's revolve):
+ * `snapshots` state slots, the initial state's included, of which the forward
+ * pass fills those of the schedule's first descent; apollo_dg_backward then
+ * re-runs the steps it needs from them, splitting each interval where the
+ * total of re-run steps is least (dynamic programming up to 4000 steps, the
+ * binomial rule beyond: beta(c, t) = C(c + t, c) steps need t passes with c
+ * free slots).  Derivative memory: `snapshots` states and the 5 stage states
+ * of one step (the two-level schedule of apollo_dg_forward_fixed holds
+ * nsteps / checkpoint_every states and 5 checkpoint_every stage states). */
+apollo_status apollo_dg_forward_revolve(apollo_dg* h, int nsteps, double t0, double dt, int snapshots);
+
+/* Host only: the forward steps the backward sweep after
+ * apollo_dg_forward_revolve(nsteps, snapshots) runs (each reversed step's
+ * own recording included), and how many states the forward pass stores
+ * (NULL: not wanted).  APOLLO_ERR_STATE if the schedule failed its own check
+ * (every slot holds the step it is used for, steps reversed last to first). */
+apollo_status apollo_dg_revolve_schedule(int nsteps, int snapshots, long long* recomputed_steps, int* spine_states);
+
+/* Steps the last apollo_dg_backward re-ran forward (with revolve: its
+ * schedule's count; with checkpoints every C steps: nsteps). */
+apollo_status apollo_dg_adjoint_stats(const apollo_dg* h, long long* recomputed_steps);
+
 /* Discrete adjoint of the last apollo_dg_forward_fixed trajectory: given
  * ubar_T = dJ/dU(T) (any terminal functional J), writes ubar_0 = dJ/dU(0).
  * Each checkpoint segment is re-run once, keeping its 5 x checkpoint_every

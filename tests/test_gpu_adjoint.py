@@ -183,3 +183,39 @@ def test_trajectory_adjoint_with_hll_flux():
         print(g_adj, g_tan, fd)
         assert abs(g_adj - g_tan) <= 1e-10 * abs(g_tan)
         assert abs(g_adj - fd) <= 1e-5 * abs(fd)
+
+
+@pytest.mark.parametrize("snapshots", [1, 3, 5, 20])
+def test_revolve_gradient_equals_two_level(snapshots):
+    """Binomial checkpointing re-runs the same steps with the same kernels, so
+    its gradient equals the two-level schedule's bit for bit; the re-run count
+    is the host schedule's."""
+    s, u0, target, dt, nsteps = _vortex_case(nsteps=23)
+    _, uT = _J(s, u0, target, nsteps, dt, 5)
+    g2 = s.backward(uT - target)
+    s.set_state(u0)
+    s.forward_revolve(nsteps, 0.0, dt, snapshots)
+    uR = s.get_state()
+    assert np.array_equal(uR, uT)
+    gr = s.backward(uR - target)
+    assert np.array_equal(gr, g2)
+    assert s.recomputed_steps() == NodalDG2d.revolve_schedule(nsteps, snapshots)[0]
+    # the backward sweep can be repeated on the same trajectory
+    assert np.array_equal(s.backward(uR - target), g2)
+
+
+def test_revolve_gradient_matches_finite_differences():
+    s, u0, target, dt, nsteps = _vortex_case(nsteps=12)
+
+    def J(u):
+        s.set_state(u)
+        s.forward_revolve(nsteps, 0.0, dt, 4)
+        v = s.get_state()
+        return 0.5 * float(np.sum((v - target) ** 2)), v
+
+    _, uT = J(u0)
+    grad = s.backward(uT - target)
+    d = np.random.default_rng(4).standard_normal(u0.shape)
+    eps = 1e-6
+    fd = (J(u0 + eps * d)[0] - J(u0 - eps * d)[0]) / (2 * eps)
+    assert abs(float(np.vdot(grad, d)) - fd) <= 1e-6 * abs(fd)
