@@ -70,6 +70,7 @@ struct apollo_dg {
   int tr_snapshots = 0;  // > 0: the last forward was apollo_dg_forward_revolve with this many slots
   long long tr_forward_steps = 0;  // forward steps the last revolve backward sweep re-ran
   RevolvePlan revolve;
+  bool tr_spine_valid = false;  // the slots still hold the first descent's states
   int tr_nsteps = 0, tr_every = 0;
   double tr_t0 = 0.0, tr_dt = 0.0;
   bool tr_valid = false;
@@ -1456,6 +1457,7 @@ apollo_status apollo_dg_forward_revolve(apollo_dg* h, int nsteps, double t0, dou
   h->tr_nsteps = nsteps;
   h->tr_every = 0;
   h->tr_snapshots = snapshots;
+  h->tr_spine_valid = true;
   h->tr_t0 = t0;
   h->tr_dt = dt;
   h->tr_valid = true;
@@ -1511,7 +1513,18 @@ apollo_status apollo_dg_backward(apollo_dg* h, const double* ubar_T, double* uba
     RevolveRun<RevolveDevice> rv{h->revolve, dev};
     r = clear_errors(h);
     if (!r) r = copy_in(h, h->A_d[0], ubar_T, where);
-    if (!r) r = (apollo_status)rv.run();
+    if (!r && !h->tr_spine_valid) {
+      // an earlier sweep reused the slots of the first descent: run it again
+      const std::vector<int> p = h->revolve.spine();
+      for (size_t k = 1; k < p.size() && !r; ++k) {
+        r = (apollo_status)dev.copy((int)k, (int)k - 1);
+        if (!r) r = (apollo_status)dev.advance((int)k, p[k - 1], p[k] - p[k - 1]);
+      }
+    }
+    if (!r) {
+      h->tr_spine_valid = false;
+      r = (apollo_status)rv.run();
+    }
     if (!r) r = copy_out(h, ubar_0, h->A_d[0], where);
     if (r) return r;
     h->tr_forward_steps = dev.forward_steps;

@@ -331,7 +331,8 @@ apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, doubl
  * re-runs the steps it needs from them, splitting each interval where the
  * total of re-run steps is least (dynamic programming up to 4000 steps, the
  * binomial rule beyond: beta(c, t) = C(c + t, c) steps need t passes with c
- * free slots).  Derivative memory: `snapshots` states and the 5 stage states
+ * free slots).  A second apollo_dg_backward of the same trajectory first
+ * re-runs the first descent, whose slots the first sweep reused.  Derivative memory: `snapshots` states and the 5 stage states
  * of one step (the two-level schedule of apollo_dg_forward_fixed holds
  * nsteps / checkpoint_every states and 5 checkpoint_every stage states). */
 apollo_status apollo_dg_forward_revolve(apollo_dg* h, int nsteps, double t0, double dt, int snapshots);

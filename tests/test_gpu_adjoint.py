@@ -200,8 +200,10 @@ def test_revolve_gradient_equals_two_level(snapshots):
     gr = s.backward(uR - target)
     assert np.array_equal(gr, g2)
     assert s.recomputed_steps() == NodalDG2d.revolve_schedule(nsteps, snapshots)[0]
-    # the backward sweep can be repeated on the same trajectory
+    # the backward sweep can be repeated on the same trajectory (the first
+    # descent is run again: its slots were reused)
     assert np.array_equal(s.backward(uR - target), g2)
+    assert s.recomputed_steps() >= NodalDG2d.revolve_schedule(nsteps, snapshots)[0]
 
 
 def test_revolve_gradient_matches_finite_differences():
