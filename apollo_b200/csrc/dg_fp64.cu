@@ -126,11 +126,232 @@ __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
     }
     __syncthreads();
     // volume term: [Dr | Ds] [R; S]
-    block_dgemm<T::NPR, T::COLS, T::K2, T::LDA2, LDB, NWARPS>(sD, sRS, [&](int r, int c, double v) {
+    block_dgemm<T::NPR, T::COLS, T::K2, T::LDA2, LDB, NWARPS, 4>(sD, sRS, [&](int r, int c, double v) {
       const int e = c / M, f = c - e * M;
       if (r < NP && e < ne) d.vol[((size_t)(k0 + e) * NP + r) * M + f] = v;
     });
   }
+  if (err) atomicOr(&d.st->err, err);
+}
+
+// Tile of the fused float64 stage: the volume and surface terms of E elements
+// and the stage update in one pass.  Shared memory (doubles):
+//   V  [NCR][LDA1]             nodal values -> cubature points
+//   DL [NPR][LDA2]             [Dr | Ds | L], K2 = 2 NC + NF (+ zero padding)
+//   I  [NFR][LDA1]             nodal values -> face Gauss points
+//   Q  [NPK][LDB]              the tile's states, column e M + f
+//   PB [NPK][LDP]              the neighbour across face j of element e, column (3 e + j) M + f
+//   T  [NFR][LDB]              the tile's face traces I q
+//   TP [E][3][NG][M]           the neighbours' traces on the shared faces, in this side's Gauss order
+//   RS [K2][LDB]               cubature values, then R (rows 0..NC-1), S (NC..2NC-1)
+//                              and -(1/J) sJ w_g times the numerical flux (2NC..)
+//   GS [E][16]                 rx, ry, sx, sy, 1/J, dt, nx[3], ny[3], sJ[3] of each element
+//   F2 [E][3] int              the neighbour's face index (-1: boundary)
+// E is the largest of a few candidates whose tile leaves two blocks per SM
+// (the smallest one otherwise).
+template <int N, int M> struct StageTile {
+  static constexpr int NP = Sizes<N>::NP, NC = Sizes<N>::NC, NF = Sizes<N>::NF, NG = Sizes<N>::NG;
+  static constexpr int NPM = NP * M;
+  static constexpr int NPK = round_up(NP, 4);
+  static constexpr int LDA1 = pad_ld(NPK);
+  static constexpr int NCR = round_up(NC, 8);
+  static constexpr int NFR = round_up(NF, 8);
+  static constexpr int NPR = round_up(NP, 8);
+  static constexpr int K2 = round_up(2 * NC + NF, 4);
+  static constexpr int LDA2 = pad_ld(K2);
+  static constexpr int RSR = K2 > NCR ? K2 : NCR;
+  static constexpr int doubles(int e) {
+    return NCR * LDA1 + NPR * LDA2 + NFR * LDA1 + NPK * pad_ld(round_up(e * M, 8)) +
+           NPK * pad_ld(round_up(3 * e * M, 8)) + NFR * pad_ld(round_up(e * M, 8)) + e * 3 * NG * M +
+           RSR * pad_ld(round_up(e * M, 8)) + e * 16 + (e * 3 + 1) / 2;
+  }
+  static constexpr int pick() {
+    const int c0 = M == 1 ? 64 : 16, c1 = M == 1 ? 32 : 8, c2 = M == 1 ? 16 : 4;
+    return doubles(c0) * 8 <= 110 * 1024 ? c0 : doubles(c1) * 8 <= 110 * 1024 ? c1 : c2;
+  }
+  static constexpr int E = pick();
+  static constexpr int COLS = round_up(E * M, 8);
+  static constexpr int LDB = pad_ld(COLS);
+  static constexpr int PCOLS = round_up(3 * E * M, 8);
+  static constexpr int LDP = pad_ld(PCOLS);
+  static constexpr int OFF_V = 0;
+  static constexpr int OFF_DL = OFF_V + NCR * LDA1;
+  static constexpr int OFF_I = OFF_DL + NPR * LDA2;
+  static constexpr int OFF_Q = OFF_I + NFR * LDA1;
+  static constexpr int OFF_PB = OFF_Q + NPK * LDB;
+  static constexpr int OFF_T = OFF_PB + NPK * LDP;
+  static constexpr int OFF_TP = OFF_T + NFR * LDB;
+  static constexpr int OFF_RS = OFF_TP + E * 3 * NG * M;
+  static constexpr int OFF_GS = OFF_RS + RSR * LDB;
+  static constexpr int OFF_F2 = OFF_GS + E * 16;
+  static constexpr int TOTAL = OFF_F2 + (E * 3 + 1) / 2;
+  static constexpr size_t BYTES = sizeof(double) * TOTAL;
+  static_assert(TOTAL == doubles(E), "layout");
+};
+
+// One SSPRK stage (or right-hand side) in float64, fused: per tile, the states
+// of its elements and of their face neighbours into shared memory; DMMA
+// contractions for the cubature values V q, the face traces I q of the tile
+// and of the neighbours (each element's trace comes out of the same
+// contraction on either side of a face, so both sides see the same values);
+// the physical flux at every cubature point and, on every face Gauss point,
+// the boundary hook and the numerical flux; one contraction
+// [Dr | Ds | L] [R; S; -(1/J) sJ w_g f*] for the right-hand side; the stage
+// update in its epilogue.  Every element evaluates its own faces, as Apollo
+// does (wxnodaldg2dmethod.cc:389-472), so no face buffer makes a round trip
+// through HBM.  Reads the neighbours of x: x and out must not overlap.
+template <int EQ, int N>
+__global__ void __launch_bounds__(kThreads) k_stage64(DgDev d, StageArgs a) {
+  using P = Eq<EQ>;
+  constexpr int M = P::M;
+  using T = StageTile<N, M>;
+  constexpr int NP = T::NP, NC = T::NC, NF = T::NF, NG = T::NG, NPM = T::NPM, E = T::E, LDB = T::LDB, LDP = T::LDP;
+  constexpr int NWARPS = kThreads / 32;
+  extern __shared__ double smem[];
+  double* sV = smem + T::OFF_V;
+  double* sDL = smem + T::OFF_DL;
+  double* sI = smem + T::OFF_I;
+  double* sQ = smem + T::OFF_Q;
+  double* sPB = smem + T::OFF_PB;
+  double* sT = smem + T::OFF_T;
+  double* sTP = smem + T::OFF_TP;
+  double* sRS = smem + T::OFF_RS;
+  double* sGS = smem + T::OFF_GS;
+  int* sF2 = (int*)(smem + T::OFF_F2);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < T::NCR * T::LDA1; i += kThreads) {
+    const int r = i / T::LDA1, c = i % T::LDA1;
+    sV[i] = (r < NC && c < NP) ? d.V[r * NP + c] : 0.0;
+  }
+  for (int i = tid; i < T::NPR * T::LDA2; i += kThreads) {
+    const int r = i / T::LDA2, c = i % T::LDA2;
+    double v = 0.0;
+    if (r < NP) {
+      if (c < NC) v = d.Dr[r * NC + c];
+      else if (c < 2 * NC) v = d.Ds[r * NC + c - NC];
+      else if (c < 2 * NC + NF) v = d.L[r * NF + c - 2 * NC];
+    }
+    sDL[i] = v;
+  }
+  for (int i = tid; i < T::NFR * T::LDA1; i += kThreads) {
+    const int r = i / T::LDA1, c = i % T::LDA1;
+    sI[i] = (r < NF && c < NP) ? d.I[r * NP + c] : 0.0;
+  }
+  // padding rows and columns of the contraction operands stay zero
+  for (int i = tid; i < T::NPK * LDB; i += kThreads) sQ[i] = 0.0;
+  for (int i = tid; i < T::NPK * LDP; i += kThreads) sPB[i] = 0.0;
+  for (int i = tid; i < T::RSR * LDB; i += kThreads) sRS[i] = 0.0;
+  int err = 0;
+  LamAcc lam_acc;
+  const int ntiles = (d.K + E - 1) / E;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int k0 = tile * E;
+    const int ne = min(E, d.K - k0);
+    __syncthreads();
+    const double* src = a.x + (size_t)k0 * NPM;
+    for (int i = tid; i < ne * NPM; i += kThreads) {
+      const int e = i / NPM, r = i - e * NPM, j = r / M, f = r - j * M;
+      sQ[j * LDB + e * M + f] = src[i];
+    }
+    for (int i = tid; i < ne * 3; i += kThreads) sF2[i] = d.conn[(size_t)k0 * 6 + 2 * i + 1];
+    for (int i = tid; i < ne * 16; i += kThreads) {
+      const int e = i >> 4, q = i & 15;
+      const ElemGeo& g = d.geo[k0 + e];
+      double v = 0.0;
+      if (q < 4) v = (&g.rx)[q];
+      else if (q == 4) v = g.invJ;
+      else if (q == 5) v = a.time_from_state ? d.st[inst_of(d, k0 + e)].dt : a.dt_arg;
+      else if (q < 9) v = g.nx[q - 6];
+      else if (q < 12) v = g.ny[q - 9];
+      else if (q < 15) v = g.sJ[q - 12];
+      sGS[i] = v;
+    }
+    for (int i = tid; i < ne * 3 * NPM; i += kThreads) {
+      const int p = i / NPM, r = i - p * NPM, n = r / M, f = r - n * M;
+      const int* cn = d.conn + (size_t)(k0 + p / 3) * 6 + 2 * (p % 3);
+      if (cn[1] >= 0) sPB[n * LDP + p * M + f] = a.x[(size_t)cn[0] * NPM + r];
+    }
+    __syncthreads();
+    // cubature values (into the R/S rows), the tile's traces and the
+    // neighbours' traces on the faces they share with the tile
+    block_dgemm<T::NCR, T::COLS, T::NPK, T::LDA1, LDB, NWARPS>(
+        sV, sQ, [&](int r, int c, double v) { sRS[r * LDB + c] = v; });
+    block_dgemm<T::NFR, T::COLS, T::NPK, T::LDA1, LDB, NWARPS>(
+        sI, sQ, [&](int r, int c, double v) { sT[r * LDB + c] = v; });
+    block_dgemm<T::NFR, T::PCOLS, T::NPK, T::LDA1, LDP, NWARPS>(sI, sPB, [&](int r, int c, double v) {
+      const int p = c / M;
+      if (p >= 3 * ne) return;
+      const int f2 = sF2[p], g2 = r - f2 * NG;
+      if (f2 >= 0 && g2 >= 0 && g2 < NG) sTP[(p * NG + (NG - 1 - g2)) * M + (c - p * M)] = v;
+    });
+    __syncthreads();
+    // physical flux at the cubature points: R into row c, S into row NC + c
+    for (int idx = tid; idx < ne * NC; idx += kThreads) {
+      const int e = idx / NC, c = idx - e * NC;
+      double qc[M], F[M], G[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) qc[f] = sRS[c * LDB + e * M + f];
+      P::flux2(d.eqp, qc, F, G, &err);
+      const double* gs = sGS + e * 16;
+      const double rx = gs[0], ry = gs[1], sx = gs[2], sy = gs[3];
+#pragma unroll
+      for (int f = 0; f < M; ++f) {
+        sRS[c * LDB + e * M + f] = rx * F[f] + ry * G[f];
+        sRS[(NC + c) * LDB + e * M + f] = sx * F[f] + sy * G[f];
+      }
+    }
+    // numerical flux at the face Gauss points into rows 2 NC + j NG + g
+    for (int idx = tid; idx < ne * NF; idx += kThreads) {
+      const int e = idx / NF, kk = idx - e * NF, j = kk / NG, gq = kk - j * NG;
+      const int k = k0 + e;
+      const double* gs = sGS + e * 16;
+      const double nx = gs[6 + j], ny = gs[9 + j];
+      double qM[M], qP[M], nf[M];
+#pragma unroll
+      for (int f = 0; f < M; ++f) qM[f] = sT[kk * LDB + e * M + f];
+      const int inst = inst_of(d, k);
+      if (sF2[e * 3 + j] >= 0) {
+#pragma unroll
+        for (int f = 0; f < M; ++f) qP[f] = sTP[((e * 3 + j) * NG + gq) * M + f];
+      } else {
+        const ElemGeo& g = d.geo[k];
+        const double t = a.time_from_state ? d.st[inst].t + d.st[inst].dt * a.frac : a.t_arg;
+        // Gauss point coordinates on face j (wxcubature2d.cc:118-124)
+        const double z = d.gz[gq];
+        double r, s;
+        if (j == 0) { r = z; s = -1.0; }
+        else if (j == 1) { r = -z; s = z; }
+        else { r = -1.0; s = -z; }
+        const double x = 0.5 * (-g.vx[0] * (r + s) + g.vx[1] * (1. + r) + g.vx[2] * (1. + s));
+        const double y = 0.5 * (-g.vy[0] * (r + s) + g.vy[1] * (1. + r) + g.vy[2] * (1. + s));
+        apply_bc<EQ, double>(d.bcs, -d.conn[(size_t)k * 6 + 2 * j], t, x, y, nx, ny, qM, qP);
+      }
+      const double lam = P::numflux(d.eqp, nx, ny, qM, qP, nf, &err);
+      lam_acc.add(d.st, inst, fabs(lam));
+      const double w = -(gs[4] * (d.gw[gq] * gs[12 + j]));
+#pragma unroll
+      for (int f = 0; f < M; ++f) sRS[(2 * NC + kk) * LDB + e * M + f] = nf[f] * w;
+    }
+    __syncthreads();
+    // right-hand side [Dr | Ds | L] [R; S; F] and the stage update
+    block_dgemm<T::NPR, T::COLS, T::K2, T::LDA2, LDB, NWARPS, 4>(sDL, sRS, [&](int i, int c, double r) {
+      const int e = c / M;
+      if (i >= NP || e >= ne) return;
+      const int k = k0 + e;
+      const size_t off = (size_t)k * NPM + i * M + (c - e * M);
+      const double dt = sGS[e * 16 + 5];
+      const double c_stage = dt / 4.0;  // dt/(s-1), s = 5
+      const double c_al = 4.0 / 5.0, c_be = dt / 5.0, c_ga = 1.0 / 5.0;
+      if (r != r) err |= ERRB_NAN;
+      const double xv = sQ[i * LDB + c];
+      double o;
+      if (a.mode == MODE_RHS) o = r;
+      else if (a.mode == MODE_STAGE) o = xv + c_stage * r;
+      else o = c_al * xv + c_be * r + c_ga * a.u0[off];
+      a.out[off] = o;
+    });
+  }
+  lam_acc.flush_warp(d.st);
   if (err) atomicOr(&d.st->err, err);
 }
 
@@ -460,6 +681,41 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
     configured |= 1u << (dev & 31);
   }
   const int sms = d.grid_div > 1 ? (num_sms() + d.grid_div - 1) / d.grid_div : num_sms();
+  // the fused stage where it applies: the whole mesh on this handle (no ghost
+  // elements), no sources, and an output that does not overlap the input (it
+  // reads the neighbours' states while other blocks write theirs)
+  const size_t nbytes = (size_t)d.K * Sizes<N>::NP * M * sizeof(double);
+  const char *xb = (const char*)a.x, *ob = (const char*)a.out;
+  const bool apart = ob + nbytes <= xb || xb + nbytes <= ob;
+  using ST = StageTile<N, M>;
+  const bool one_wave = (d.K + ST::E - 1) / ST::E <= sms * 2;  // launch-bound: one launch instead of three
+  const bool fuse = d.fp64_fused == 1 || (d.fp64_fused == 2 && one_wave);
+  if (fuse && d.nghost == 0 && a.phase == PHASE_ALL && d.src.n == 0 && apart) {
+    static unsigned fused_configured = 0;
+    static int resident = 1;  // blocks per SM (registers and shared memory)
+    if (!(fused_configured & (1u << (dev & 31)))) {
+      cudaError_t e = cudaFuncSetAttribute(k_stage64<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)ST::BYTES);
+      if (e != cudaSuccess) return e;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_stage64<EQ, N>, kThreads, ST::BYTES);
+      if (e != cudaSuccess) return e;
+      fused_configured |= 1u << (dev & 31);
+    }
+    const int st = (d.K + ST::E - 1) / ST::E;
+    // a persistent grid of the blocks that are resident at once
+    int per = resident < 1 ? 1 : resident;
+    int gs = sms * per;
+    if (gs > st) gs = st;
+    if (ev) cudaEventRecord(ev[0], s);
+    if (a.reset_lambda) launch_reset_lambda(d, s);
+    k_stage64<EQ, N><<<gs, kThreads, ST::BYTES, s>>>(d, a);
+    if (ev) {
+      cudaEventRecord(ev[1], s);
+      cudaEventRecord(ev[2], s);
+      cudaEventRecord(ev[3], s);
+    }
+    return cudaGetLastError();
+  }
   const int vt = (d.K + VT::E - 1) / VT::E;
   int per_sm = (int)((200 * 1024) / VT::BYTES);
   if (per_sm < 1) per_sm = 1;

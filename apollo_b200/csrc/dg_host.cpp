@@ -47,6 +47,7 @@ struct apollo_dg {
   int ninst = 1;
   int grid_div = 1;    // launch shape picked by the batch autotuner
   int tile_shape = 0;  // mixed stage operand chunking picked by the batch autotuner
+  int fp64_fused = 0;  // float64 stage kernels: 0 three, 1 fused, 2 fused on one-wave meshes
   unsigned wait_limit = 0;  // apollo_dg_debug_set_waits
   int debug_stall = 0;
   // source plugins (apollo_dg_add_source): the table, VS = VVT V^T diag(w),
@@ -55,7 +56,9 @@ struct apollo_dg {
   double *VS_d = nullptr, *cubr_d = nullptr, *cubs_d = nullptr, *srcv_d = nullptr;
   double *V_d = nullptr, *Dr_d = nullptr, *Ds_d = nullptr, *I_d = nullptr, *L_d = nullptr, *gz_d = nullptr,
          *gw_d = nullptr, *wmass_d = nullptr, *mass_d = nullptr;
-  double *U_d = nullptr, *W_d = nullptr, *in_d = nullptr, *out_d = nullptr;
+  // W_d, W2_d: stage states, alternating so that a stage's output never
+  // overlaps its input (the fused float64 stage reads neighbours' states)
+  double *U_d = nullptr, *W_d = nullptr, *W2_d = nullptr, *in_d = nullptr, *out_d = nullptr;
   // mixed precision: fp32 face traces of U (TU) and of the stage states (T0, T1)
   float *TU_d = nullptr, *T0_d = nullptr, *T1_d = nullptr;
   bool tu_valid = false;
@@ -156,7 +159,7 @@ void free_mesh(apollo_dg* h) {
   dfree(h->V_d); dfree(h->Dr_d); dfree(h->Ds_d); dfree(h->I_d); dfree(h->L_d); dfree(h->gz_d); dfree(h->gw_d);
   dfree(h->wmass_d); dfree(h->mass_d);
   dfree(h->VS_d); dfree(h->cubr_d); dfree(h->cubs_d); dfree(h->srcv_d);
-  dfree(h->U_d); dfree(h->W_d); dfree(h->in_d); dfree(h->out_d);
+  dfree(h->U_d); dfree(h->W_d); dfree(h->W2_d); dfree(h->in_d); dfree(h->out_d);
   dfree(h->TU_d); dfree(h->T0_d); dfree(h->T1_d);
   h->tu_valid = false;
   dfree(h->dvol_d); dfree(h->dtrace_d); dfree(h->dflux_d); dfree(h->sbar_d);
@@ -204,6 +207,8 @@ DgDev make_dev(const apollo_dg* h) {
   d.ninst = h->ninst;
   d.grid_div = h->grid_div;
   d.tile_shape = h->tile_shape;
+  d.fp64_fused = h->fp64_fused;
+  d.nghost = h->KG;
   d.wait_limit = h->wait_limit;
   d.debug_stall = h->debug_stall;
   d.src = h->src;
@@ -283,13 +288,14 @@ StageArgs stage_args(const apollo_dg* h, int i) {
   StageArgs a{};
   a.time_from_state = 1;
   a.reset_lambda = 1;
+  double* wb[2] = {h->W_d, h->W2_d};
   if (i < s - 1) {
-    a.x = i == 0 ? h->U_d : h->W_d;
-    a.out = h->W_d;
+    a.x = i == 0 ? h->U_d : wb[(i - 1) & 1];
+    a.out = wb[i & 1];
     a.mode = MODE_STAGE;
     a.frac = i / (s - 1.);
   } else {
-    a.x = h->W_d;
+    a.x = wb[(i - 1) & 1];
     a.u0 = h->U_d;
     a.out = h->U_d;
     a.mode = MODE_FINAL;
@@ -305,15 +311,17 @@ apollo_status enqueue_step(apollo_dg* h, apollo_precision prec) {
     StageArgs a = stage_args(h, i);
     if (h->lim_on) {
       // PETSc's SSP stepper hands the right-hand side its work vector, which
-      // Apollo's step limits in place: stage 0 limits a copy of U into W
-      apollo_status rl = enqueue_limiter(h, a.x, h->W_d);
+      // Apollo's step limits in place: stage 0 limits a copy of U (into the
+      // stage buffer stage 0 does not write), later stages their input
+      double* lim = i == 0 ? h->W2_d : const_cast<double*>(a.x);
+      apollo_status rl = enqueue_limiter(h, a.x, lim);
       if (rl) return rl;
-      a.x = h->W_d;
+      a.x = lim;
       if (prec == APOLLO_PREC_MIXED && h->mixed) {
         // the mixed stage reads the face traces of its input, which the
-        // previous stage wrote for the unlimited state: those of W instead
+        // previous stage wrote for the unlimited state: those of the limited one
         DgDev d = make_dev(h);
-        CK(mixed_launch_traces(h->mixed, d, h->W_d, (float*)a.tr_in, h->stream), "trace launch");
+        CK(mixed_launch_traces(h->mixed, d, lim, (float*)a.tr_in, h->stream), "trace launch");
       }
     }
     apollo_status r = enqueue_stage(h, a, prec);
@@ -525,6 +533,16 @@ apollo_status apollo_dg_set_launch_shape(apollo_dg* h, int grid_share, int tile_
   return APOLLO_OK;
 }
 
+apollo_status apollo_dg_set_fp64_kernels(apollo_dg* h, int fused) {
+  if (!h || fused < 0 || fused > 2) return APOLLO_ERR_ARG;
+  if (fused != h->fp64_fused) {
+    h->fp64_fused = fused;
+    for (auto& g : h->graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
+  return APOLLO_OK;
+}
+
 apollo_status apollo_dg_averaging_weights(const apollo_dg* h, double* w) {
   if (!h || !w || h->ops.Np == 0) return APOLLO_ERR_ARG;
   for (int k = 0; k < h->ops.Np; ++k) w[k] = 0.5 * h->ops.mass_colsum[k];
@@ -728,6 +746,7 @@ apollo_status set_mesh_body(apollo_dg* h, int nverts, const double* vx, const do
   }
   CK(dev_malloc((void**)&h->U_d, nU * sizeof(double)), "state alloc");
   CK(dev_malloc((void**)&h->W_d, nU * sizeof(double)), "state alloc");
+  CK(dev_malloc((void**)&h->W2_d, nU * sizeof(double)), "state alloc");
   CK(dev_malloc((void**)&h->in_d, nU * sizeof(double)), "state alloc");
   CK(dev_malloc((void**)&h->out_d, nU * sizeof(double)), "state alloc");
   CK(dev_malloc((void**)&h->vol_d, nU * sizeof(double)), "scratch alloc");
@@ -1096,10 +1115,11 @@ apollo_status fixed_stage(apollo_dg* h, int s, const double* x, const double* u0
   return APOLLO_OK;
 }
 
-// One fixed step in place on u (stages through W).
+// One fixed step in place on u (stages through W and W2 alternately).
 apollo_status fixed_step(apollo_dg* h, double* u, double tn, double dt) {
+  double* wb[2] = {h->W_d, h->W2_d};
   for (int s = 0; s < 5; ++s) {
-    apollo_status r = fixed_stage(h, s, s == 0 ? u : h->W_d, u, s < 4 ? h->W_d : u, tn, dt);
+    apollo_status r = fixed_stage(h, s, s == 0 ? u : wb[(s - 1) & 1], u, s < 4 ? wb[s & 1] : u, tn, dt);
     if (r) return r;
   }
   return APOLLO_OK;
@@ -1590,12 +1610,13 @@ apollo_status apollo_dg_tangent(apollo_dg* h, int nsteps, double t0, double dt, 
   for (int n = 0; n < nsteps; ++n) {
     const double tn = t0 + n * dt;
     for (int s = 0; s < 5; ++s) {
-      // the tangent stage reads the stage's input state before the value stage overwrites it
-      const double* x = s == 0 ? h->U_d : h->W_d;
+      // the tangent stage reads the stage's input state before the value stage replaces it
+      double* wb[2] = {h->W_d, h->W2_d};
+      const double* x = s == 0 ? h->U_d : wb[(s - 1) & 1];
       const double* dx = s == 0 ? h->tU_d : h->tW_d;
       double* dout = s < 4 ? h->tW_d : h->tU_d;
       r = tangent_stage(h, s, s < 4 ? MODE_STAGE : MODE_FINAL, x, dx, s < 4 ? nullptr : h->tU_d, dout, tn, dt);
-      if (!r) r = fixed_stage(h, s, x, h->U_d, s < 4 ? h->W_d : h->U_d, tn, dt);
+      if (!r) r = fixed_stage(h, s, x, h->U_d, s < 4 ? wb[s & 1] : h->U_d, tn, dt);
       if (r) return r;
     }
   }

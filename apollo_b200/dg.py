@@ -96,6 +96,7 @@ def load_library(path: str = LIB_PATH):
         "apollo_dg_backward": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_int]),
         "apollo_dg_forward_revolve": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_int]),
         "apollo_dg_adjoint_stats": (C.c_int, [H, C.POINTER(C.c_longlong)]),
+        "apollo_dg_set_fp64_kernels": (C.c_int, [H, C.c_int]),
         "apollo_dg_revolve_schedule": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
         "apollo_dg_tangent": (C.c_int, [H, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_int]),
         "apollo_dg_rhs_jvp": (C.c_int, [H, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
@@ -252,6 +253,12 @@ class NodalDG2d:
     def set_launch_shape(self, grid_share: int = 1, tile_shape: int = 0):
         """The persistent grids' share of the SMs and the mixed stage's operand chunking."""
         self._check(self.lib.apollo_dg_set_launch_shape(self.h, grid_share, tile_shape))
+
+    def set_fp64_kernels(self, fused=True):
+        """Float64 stage kernels: True (1) the fused stage kernel, False (0, the
+        default) the volume, face and LIFT kernels, 2 the fused one on meshes
+        of about one wave of tiles."""
+        self._check(self.lib.apollo_dg_set_fp64_kernels(self.h, int(fused)))
 
     def averaging_weights(self):
         """w[Np]: an element's average of a nodal field is sum_n w[n] u[n]."""

@@ -273,6 +273,14 @@ def advection_measure(args, device: int, cpu: bool):
         ends[prec] = s.get_state()
         out[prec] = {"value": dofs * steps / (ms / 1000.0), "ms_per_step": ms / steps, "t_end": t}
     out["l2_mixed_vs_fp64"] = float(np.linalg.norm(ends["mixed"] - ends["fp64"]) / np.linalg.norm(ends["fp64"]))
+    # the mesh is one wave of tiles: the fused float64 stage (one launch per
+    # stage instead of three) is the faster form here
+    s.set_fp64_kernels(1)
+    ms, (t, dt) = _device_run(s, stream, U0, dt0, "fp64", steps)
+    out["fp64_fused_stage"] = {"value": dofs * steps / (ms / 1000.0), "ms_per_step": ms / steps, "t_end": t,
+                               "l2_vs_fp64": float(np.linalg.norm(s.get_state() - ends["fp64"]) /
+                                                   np.linalg.norm(ends["fp64"]))}
+    s.set_fp64_kernels(0)
     if cpu:
         from oracle import oracle as orc
         threads = os.cpu_count() or 1
@@ -887,6 +895,20 @@ def ours_arm(args):
     if prec == "mixed":
         roofline["note"] = ("stage kernel: tf32x3 tcgen05 contractions; bounded in practice by shared-memory "
                             "bandwidth and issue latency, not HBM (see profiles/)")
+    # the whole stage (what one SSPRK stage must move at the least: read the
+    # stage state and the step's initial state, write the new stage state, plus
+    # 160 B of geometry per element), timed as a fifth of the measured step
+    stage_b = 8 * 3 * Np * M + 160
+    stage_ms = ms_step / 5.0
+    stage_ach = stage_b * K / (stage_ms / 1000.0) / 1e9
+    stage_traffic = (profile_traffic().get(f"mixed:stage:{workload_name(p.N, s.K)}") if prec == "mixed" else
+                     sum(profile_traffic().get(f"fp64:{k}:{workload_name(p.N, s.K)}") or 0
+                         for k in ("volume", "face", "lift_update")) or None)
+    roofline["stage_mode"] = {"bytes_per_element": stage_b, "bytes": stage_b * K, "stage_ms": stage_ms,
+                              "achieved": stage_ach, "frac": stage_ach / peaks["hbm_gbs"],
+                              "traffic": stage_traffic,
+                              "how": "compulsory bytes of one stage / (ms_per_step / 5); traffic: DRAM bytes of "
+                                     "one stage from one-pass ncu captures at this mesh"}
 
     e2e = None
     if not args.no_e2e:

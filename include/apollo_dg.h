@@ -173,6 +173,19 @@ apollo_status apollo_dg_set_limiter(apollo_dg* h, const char* kind, const double
  * in Apollo. */
 apollo_status apollo_dg_set_launch_shape(apollo_dg* h, int grid_share, int tile_shape);
 
+/* Float64 stage kernels of this handle.  0 (the default): the volume, face
+ * and LIFT kernels.  1: the fused stage kernel (the volume and surface terms
+ * and the stage update of a tile of elements in one pass, each element
+ * evaluating its own faces as Apollo does, DRAM traffic near the compulsory
+ * bytes) wherever it applies: a whole mesh, no source plugins, and a stage
+ * whose output does not overlap its input.  2: the fused kernel where the
+ * mesh's tiles fit about one wave of resident blocks (small meshes, where
+ * three launches cost more than the work), the three kernels elsewhere (the
+ * face kernel evaluates each face once, which a per-element pass cannot).
+ * The forms agree within float64 round-off, not bit for bit, so the default
+ * keeps every handle (whole, partitioned, batched) on the same arithmetic. */
+apollo_status apollo_dg_set_fp64_kernels(apollo_dg* h, int fused);
+
 /* The element average of a nodal field is sum_n w[n] u[n]: w[Np] receives the
  * weights (half the column sums of the reference mass matrix, Apollo's
  * LimiterElementAVE, src/lib/wxnodaldggeometry2d.h:84-98). */
