@@ -82,6 +82,7 @@ def test_fused_kernel_is_the_one_that_runs():
     s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh)
     x, y = s.node_coords()
     s.set_state(np.ascontiguousarray(p.ic(x, y)))
+    s.set_fp64_kernels(True)
     kt = s.kernel_times(3)
     assert kt[0] > 0 and kt[1] < 0.2 * kt[0] and kt[2] < 0.2 * kt[0]  # one kernel: no face or LIFT launch
     s.set_fp64_kernels(False)
