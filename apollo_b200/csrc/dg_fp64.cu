@@ -355,6 +355,34 @@ __global__ void __launch_bounds__(kThreads) k_stage64(DgDev d, StageArgs a) {
   if (err) atomicOr(&d.st->err, err);
 }
 
+// M consecutive doubles of one Gauss point (a trace or a face flux): 16-byte
+// vector accesses when M is even (every point's block then starts on a
+// 16-byte boundary), scalar ones otherwise.
+template <int M>
+__device__ __forceinline__ void load_point(const double* __restrict__ p, double* q) {
+  if constexpr (M % 2 == 0) {
+#pragma unroll
+    for (int f = 0; f < M; f += 2) {
+      const double2 v = __ldg(reinterpret_cast<const double2*>(p + f));
+      q[f] = v.x;
+      q[f + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < M; ++f) q[f] = __ldg(p + f);
+  }
+}
+template <int M>
+__device__ __forceinline__ void store_point(double* __restrict__ p, const double* q, double w) {
+  if constexpr (M % 2 == 0) {
+#pragma unroll
+    for (int f = 0; f < M; f += 2) *reinterpret_cast<double2*>(p + f) = make_double2(q[f] * w, q[f + 1] * w);
+  } else {
+#pragma unroll
+    for (int f = 0; f < M; ++f) p[f] = q[f] * w;
+  }
+}
+
 template <int EQ, int N>
 __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
   using P = Eq<EQ>;
@@ -377,12 +405,9 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
     const double nx = g.nx[fr.f1], ny = g.ny[fr.f1], sJ = g.sJ[fr.f1];
     double qM[M], qP[M], nf[M];
     const double* tm = d.trace + ((size_t)fr.k1 * NF + fr.f1 * NG + gq) * M;
-#pragma unroll
-    for (int f = 0; f < M; ++f) qM[f] = tm[f];
+    load_point<M>(tm, qM);
     if (fr.k2 >= 0) {
-      const double* tp = d.trace + ((size_t)fr.k2 * NF + fr.f2 * NG + (NG - 1 - gq)) * M;
-#pragma unroll
-      for (int f = 0; f < M; ++f) qP[f] = tp[f];
+      load_point<M>(d.trace + ((size_t)fr.k2 * NF + fr.f2 * NG + (NG - 1 - gq)) * M, qP);
     } else {
       // Gauss point coordinates on face f1: the affine map of the face
       // parametrisation (wxcubature2d.cc:118-124)
@@ -398,26 +423,20 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
     double lam = P::numflux(d.eqp, nx, ny, qM, qP, nf, &err);
     lam_acc.add(d.st, inst, fabs(lam));
     const double w = d.gw[gq] * sJ;
-    double* om = d.flux + ((size_t)fr.k1 * NF + fr.f1 * NG + gq) * M;
-#pragma unroll
-    for (int f = 0; f < M; ++f) om[f] = nf[f] * w;
+    store_point<M>(d.flux + ((size_t)fr.k1 * NF + fr.f1 * NG + gq) * M, nf, w);
     if (fr.k2 >= 0) {
       const int g2 = NG - 1 - gq;
       double* op = d.flux + ((size_t)fr.k2 * NF + fr.f2 * NG + g2) * M;
       if (two_sided) {
         // the partner's own evaluation: its normal, weight and trace as "-"
         const ElemGeo& h2 = d.geo[fr.k2];
-        const double* t2 = d.trace + ((size_t)fr.k2 * NF + fr.f2 * NG + g2) * M;
-#pragma unroll
-        for (int f = 0; f < M; ++f) { qM[f] = t2[f]; qP[f] = tm[f]; }
+        load_point<M>(d.trace + ((size_t)fr.k2 * NF + fr.f2 * NG + g2) * M, qM);
+        load_point<M>(tm, qP);
         const double lam2 = P::numflux(d.eqp, h2.nx[fr.f2], h2.ny[fr.f2], qM, qP, nf, &err);
         lam_acc.add(d.st, inst, fabs(lam2));
-        const double w2 = d.gw[g2] * h2.sJ[fr.f2];
-#pragma unroll
-        for (int f = 0; f < M; ++f) op[f] = nf[f] * w2;
+        store_point<M>(op, nf, d.gw[g2] * h2.sJ[fr.f2]);
       } else {
-#pragma unroll
-        for (int f = 0; f < M; ++f) op[f] = -(nf[f] * w);
+        store_point<M>(op, nf, -w);
       }
     }
   }
