@@ -506,6 +506,29 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def fp64_gemm_peak(device: int) -> float:
+    """Float64 dense GEMM throughput of this GPU (TFLOP/s): cuBLAS DGEMM through
+    torch.matmul on 4096^3 operands, best of 5 (CUDA events), the denominator of
+    the float64 path's roofline (the measured peaks file has no float64 entry)."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=f"cuda:{device}")
+    b = torch.randn(n, n, dtype=torch.float64, device=f"cuda:{device}")
+    c = torch.empty_like(a)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1000.0)
+    del a, b, c
+    return 2.0 * n ** 3 / best / 1e12
+
+
 def profile_traffic():
     """DRAM bytes per launch of the dominant kernels from the committed ncu summary."""
     try:
@@ -838,6 +861,18 @@ def ours_arm(args):
     if prec == "mixed":
         ms64 = timed("fp64", args.steps, args.warmup)
         extra["fp64"] = {"value": dofs * world * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps}
+        try:
+            # the float64 stepper against the float64 pipe: Survey-8d contraction
+            # FLOPs, 2 m (3 Nc Np + 2 Nf Np + Np^2) per element per stage
+            Nc, Nf = s.Nc, 3 * s.Ng
+            flops = 5 * s.K * 2 * s.m * (3 * Nc * s.Np + 2 * Nf * s.Np + s.Np * s.Np)
+            ach = flops / (ms64 / args.steps / 1000.0) / 1e12
+            pk = fp64_gemm_peak(local)
+            extra["fp64"]["roofline"] = {"bound": "fp64", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                                         "frac": ach / pk, "flops_per_step": flops,
+                                         "peak_source": "cuBLAS DGEMM 4096^3 on this GPU (torch.matmul, best of 5)"}
+        except Exception as exc:
+            extra["fp64"]["roofline"] = {"error": str(exc)}
         extra["speedup_vs_fp64"] = ms64 / ms
         if not args.no_l2_500:
             # the stated error: both forms over the configuration's 500 steps
