@@ -258,7 +258,10 @@ __global__ void __launch_bounds__(kThreads) k_stage64(DgDev d, StageArgs a) {
       const int e = i >> 4, q = i & 15;
       const ElemGeo& g = d.geo[k0 + e];
       double v = 0.0;
-      if (q < 4) v = (&g.rx)[q];
+      if (q == 0) v = g.rx;
+      else if (q == 1) v = g.ry;
+      else if (q == 2) v = g.sx;
+      else if (q == 3) v = g.sy;
       else if (q == 4) v = g.invJ;
       else if (q == 5) v = a.time_from_state ? d.st[inst_of(d, k0 + e)].dt : a.dt_arg;
       else if (q < 9) v = g.nx[q - 6];

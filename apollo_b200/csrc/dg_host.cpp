@@ -1451,6 +1451,8 @@ apollo_status apollo_dg_forward_revolve(apollo_dg* h, int nsteps, double t0, dou
   if (h->lim_on) return fail(h, APOLLO_ERR_CONFIG, "the derivatives do not support the limiter");
   if (nsteps < 1 || snapshots < 1 || !(dt > 0.0)) return fail(h, APOLLO_ERR_ARG, "nsteps, snapshots >= 1, dt > 0");
   if (!h->have_state) return fail(h, APOLLO_ERR_STATE, "no state set");
+  // a slot per step already stores every state the sweep needs
+  if (snapshots > nsteps) snapshots = nsteps;
   r = ensure_deriv_buffers(h);
   if (!r) r = size_checkpoints(h, snapshots);
   if (!r) r = size_segment(h, 1);
@@ -1685,6 +1687,7 @@ apollo_status apollo_dg_rhs_vjp(apollo_dg* h, double t, const double* x, const d
 
 apollo_status apollo_dg_revolve_schedule(int nsteps, int snapshots, long long* recomputed_steps, int* spine_states) {
   if (nsteps < 1 || snapshots < 1 || !recomputed_steps) return APOLLO_ERR_ARG;
+  if (snapshots > nsteps) snapshots = nsteps;
   RevolvePlan plan;
   plan.build(nsteps, snapshots);
   const std::vector<int> spine = plan.spine();

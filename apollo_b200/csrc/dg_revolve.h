@@ -12,8 +12,8 @@
 // minimises the forward steps of the whole reversal,
 //   F(1, c) = 1,  F(n, 0) = n (n + 1) / 2,
 //   F(n, c) = min_m  m + F(n - m, c - 1) + F(m, c),
-// by dynamic programming over n and c up to kRevolveDpSteps steps; longer
-// trajectories split by the binomial rule (beta(c, t) = C(c + t, c) steps
+// by dynamic programming over n and c while n^2 S / 2 stays under
+// kRevolveDpWork; longer trajectories split by the binomial rule (beta(c, t) = C(c + t, c) steps
 // need t passes with c free slots, and the right part takes beta(c - 1, t)).
 // The forward trajectory stores the states of the first descent (the spine)
 // as it passes them, so the reversal starts at the last of them; its splits
@@ -32,7 +32,7 @@ inline double revolve_beta(int c, int t) {
   return b;
 }
 
-constexpr int kRevolveDpSteps = 4000;
+constexpr double kRevolveDpWork = 1.5e8;  // split candidates the dynamic program may examine
 
 struct RevolvePlan {
   int n = 0;      // trajectory steps
@@ -53,7 +53,7 @@ struct RevolvePlan {
     S = snapshots;
     arg.clear();
     sarg.clear();
-    if (n > kRevolveDpSteps || S < 2) return;
+    if (S < 2 || 0.5 * (double)n * n * S > kRevolveDpWork) return;
     std::vector<long long> F((size_t)(n + 1) * S, 0), G((size_t)(n + 1) * S, 0);
     arg.assign((size_t)(n + 1) * S, 1);
     sarg.assign((size_t)(n + 1) * S, 1);

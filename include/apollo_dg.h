@@ -342,9 +342,10 @@ apollo_status apollo_dg_forward_fixed(apollo_dg* h, int nsteps, double t0, doubl
  * `snapshots` state slots, the initial state's included, of which the forward
  * pass fills those of the schedule's first descent; apollo_dg_backward then
  * re-runs the steps it needs from them, splitting each interval where the
- * total of re-run steps is least (dynamic programming up to 4000 steps, the
- * binomial rule beyond: beta(c, t) = C(c + t, c) steps need t passes with c
- * free slots).  A second apollo_dg_backward of the same trajectory first
+ * total of re-run steps is least (dynamic programming while nsteps^2
+ * snapshots / 2 stays under 1.5e8, the binomial rule beyond: beta(c, t) =
+ * C(c + t, c) steps need t passes with c free slots).  More snapshots than
+ * steps are not allocated.  A second apollo_dg_backward of the same trajectory first
  * re-runs the first descent, whose slots the first sweep reused.  Derivative memory: `snapshots` states and the 5 stage states
  * of one step (the two-level schedule of apollo_dg_forward_fixed holds
  * nsteps / checkpoint_every states and 5 checkpoint_every stage states). */
