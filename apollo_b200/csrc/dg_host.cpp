@@ -519,6 +519,10 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name) {
     else if (n == "Wave") kind = NF_WAVE;
     else if (n != "LF") h->err = "numerical flux " + n + " not recognised: Lax-Friedrichs used";
     h->eqp.p[3] = kind;
+  } else if (h->eq == EQ_ADVECTION) {
+    if (n == "upwind") kind = NF_UPWIND;
+    else if (n != "LF") h->err = "numerical flux " + n + " not recognised: Lax-Friedrichs used";
+    h->eqp.p[3] = kind;
   }
   // captured graphs hold the equation parameters
   for (auto& g : h->graph)

@@ -32,7 +32,10 @@ enum BcKind : int {
 
 // Euler numerical fluxes by Apollo's Numerical_Flux codes (wxeulereqn.cc:10-15);
 // stored in EqParams::p[3] of the Euler kinds
-enum NumFlux : int { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4 };
+// Numerical fluxes: Apollo's Euler Numerical_Flux codes (wxeulereqn.cc:10-15);
+// NF_UPWIND is an extension for advection (dissipation |n.u| instead of
+// Apollo's max(|ux|, |uy|)), held in the equation parameters' slot 3
+enum NumFlux : int { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4, NF_UPWIND = 8 };
 
 enum ErrBits : int { ERRB_NONPHYS = 1, ERRB_NAN = 2, ERRB_TIMEOUT = 4 };
 
@@ -78,7 +81,10 @@ template <> struct Eq<EQ_ADVECTION> {
     flux2(P, qM, fM, gM, err);
     flux2(P, qP, fP, gP, err);
     T lambda = T(dmax2(fabs(P.p[0]), fabs(P.p[1])));
-    nf[0] = T(0.5) * (nx * (fM[0] + fP[0]) + ny * (gM[0] + gP[0]) + lambda * (qM[0] - qP[0]));
+    // the upwind extension dissipates with the normal speed; the returned
+    // speed (the dt policy's) stays Apollo's
+    const T diss = (int)P.p[3] == NF_UPWIND ? fabs(nx * T(P.p[0]) + ny * T(P.p[1])) : lambda;
+    nf[0] = T(0.5) * (nx * (fM[0] + fP[0]) + ny * (gM[0] + gP[0]) + diss * (qM[0] - qP[0]));
     return lambda;
   }
   APOLLO_HD static double speed2(const EqParams& P, const double* q) {

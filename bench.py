@@ -281,6 +281,16 @@ def advection_measure(args, device: int, cpu: bool):
                                "l2_vs_fp64": float(np.linalg.norm(s.get_state() - ends["fp64"]) /
                                                    np.linalg.norm(ends["fp64"]))}
     s.set_fp64_kernels(0)
+    # the configuration names an upwind flux; Apollo's advection flux is
+    # Lax-Friedrichs with max(|ux|, |uy|) (the parity runs above), and the
+    # upwind flux (dissipation |n.u|) is this library's extension
+    su = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=device, stream=stream.cuda_stream,
+                   numerical_flux="upwind")
+    su.set_state(U0)
+    ms, (t, dt) = _device_run(su, stream, U0, dt0, "fp64", steps)
+    Uup = su.get_state()
+    out["fp64_upwind"] = {"value": dofs * steps / (ms / 1000.0), "ms_per_step": ms / steps, "t_end": t}
+    su.close()
     if cpu:
         from oracle import oracle as orc
         threads = os.cpu_count() or 1
@@ -289,6 +299,11 @@ def advection_measure(args, device: int, cpu: bool):
         n, el = _cpu_rate(o, Uc, steps, threads)
         out["cpu_all_cores"] = {"value": dofs * n / el, "cores": threads, "steps": n, "seconds": el}
         out["l2_fp64_gpu_vs_cpu_oracle"] = float(np.linalg.norm(ends["fp64"] - Uc) / np.linalg.norm(Uc))
+        ou = orc.Oracle(p.mesh, p.N, orc.EQ_ADVECTION, tuple(p.eq_params)[:3] + (orc.NF_UPWIND,), cfl=p.cfl)
+        ou.set_threads(threads)
+        Uu = U0.copy()
+        ou.run(Uu, steps, 0.0, dt0)
+        out["fp64_upwind"]["l2_vs_cpu_oracle"] = float(np.linalg.norm(Uup - Uu) / np.linalg.norm(Uu))
         n1, el1 = _cpu_rate(o, U0.copy(), 10, 1)
         out["cpu_1_thread"] = {"value": dofs * n1 / el1, "cores": 1, "steps": n1, "seconds": el1}
     s.close()

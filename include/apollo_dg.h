@@ -133,9 +133,12 @@ apollo_status apollo_dg_set_limiter_text(apollo_dg* h, const char* kind, const c
  * apollo_dg_last_error says so).  The fluxes reproduce Apollo's arithmetic,
  * including its HLL bound |S_R| truncated to an integer, its Roe flux's
  * y-momentum component of 0 and x-momentum component set from the rotated
- * y-momentum flux, and Wave's fall-through to LF on rotated traces.  Other
- * equations have only LF (the name is ignored).  Mixed precision and the
- * derivatives (tangent and adjoint) take every one of them. */
+ * y-momentum flux, and Wave's fall-through to LF on rotated traces.
+ * "advectionEqn" takes "LF" (Apollo's, dissipation max(|ux|, |uy|)) or the
+ * extension "upwind" (dissipation |n.u|, the exact upwind flux; the dt
+ * policy keeps Apollo's speed).  Maxwell has only LF (the name is ignored).
+ * Mixed precision and the derivatives (tangent and adjoint) take every one
+ * of them. */
 apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);
 
 /* Limiter applied to every stage input before its right-hand side, as

@@ -215,7 +215,8 @@ enum { EQ_ADVECTION = 0, EQ_EULER = 1, EQ_MAXWELL = 2 };
 enum { BC_FIXED = 0, BC_VORTEX = 1, BC_TM = 2, BC_PEC = 3, BC_EULER_WALL = 4, BC_EULER_INFLOW = 5,
        BC_EULER_ZEROGRAD = 6, BC_EULER_DIRICHLET = 7 };
 // Euler Numerical_Flux codes (wxeulereqn.cc:10-15), held in eqp[3]
-enum { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4 };
+// (NF_UPWIND: an extension for advection, dissipation |n.u|; not in Apollo)
+enum { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4, NF_UPWIND = 8 };
 enum { ERR_NONPHYS = 1, ERR_NAN = 2, ERR_JAC = 4 };
 
 typedef void (*flux_fn)(void* ctx, int d, const double* q, double* f);
@@ -445,6 +446,17 @@ void euler_wave_prelude(Oracle& o, const double* n, double* qM, double* qP) {
 // DGnumericalFlux (qM/qP may be modified by the Euler primitive clamp, as in
 // the reference).
 void eq_numflux(Oracle& o, const double* n, double* qM, double* qP, double* nf, double* lam) {
+  if (o.eq == EQ_ADVECTION && (int)o.eqp[3] == NF_UPWIND) {
+    // the upwind extension: 1/2 [n.u (qM + qP) + |n.u| (qM - qP)] written as
+    // the Lax-Friedrichs form with the normal speed as its dissipation; the
+    // returned speed (the dt policy's) is Apollo's
+    double fM[1], fP[1], gM[1], gP[1];
+    adv_flux(o, 0, qM, fM); adv_flux(o, 0, qP, fP); adv_flux(o, 1, qM, gM); adv_flux(o, 1, qP, gP);
+    const double diss = std::fabs(n[0] * o.eqp[0] + n[1] * o.eqp[1]);
+    nf[0] = 0.5 * (n[0] * (fM[0] + fP[0]) + n[1] * (gM[0] + gP[0]) + diss * (qM[0] - qP[0]));
+    *lam = dmax2(std::fabs(o.eqp[0]), std::fabs(o.eqp[1]));
+    return;
+  }
   if (o.ref_numflux) { o.ref_numflux(o.ref_ctx, n, qM, qP, nf, lam); return; }
   double fM[8], fP[8], gM[8], gP[8], lambda;
   int m = o.meqn;
