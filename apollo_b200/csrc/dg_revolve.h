@@ -112,25 +112,29 @@ struct RevolveRun {
   const RevolvePlan& plan;
   Exec& x;
 
+  // The left part [l, l + m) is reversed by the same loop (a tail call), so
+  // the recursion is only as deep as the free slots.
   int rev(int l, int r, int c, int slot) {
-    const int len = r - l;
-    if (len == 1) return x.leaf(l, slot);
-    if (c == 0) {
-      for (int j = r - 1; j >= l; --j) {
-        int st = x.copy(-1, slot);
-        if (!st) st = x.advance(-1, l, j - l);
-        if (!st) st = x.leaf(j, -1);
-        if (st) return st;
+    for (;;) {
+      const int len = r - l;
+      if (len == 1) return x.leaf(l, slot);
+      if (c == 0) {
+        for (int j = r - 1; j >= l; --j) {
+          int st = x.copy(-1, slot);
+          if (!st) st = x.advance(-1, l, j - l);
+          if (!st) st = x.leaf(j, -1);
+          if (st) return st;
+        }
+        return 0;
       }
-      return 0;
+      const int m = plan.split(len, c);
+      const int ns = plan.S - c;  // slots fill and free last in, first out
+      int st = x.copy(ns, slot);
+      if (!st) st = x.advance(ns, l, m);
+      if (!st) st = rev(l + m, r, c - 1, ns);
+      if (st) return st;
+      r = l + m;
     }
-    const int m = plan.split(len, c);
-    const int ns = plan.S - c;  // slots fill and free last in, first out
-    int st = x.copy(ns, slot);
-    if (!st) st = x.advance(ns, l, m);
-    if (!st) st = rev(l + m, r, c - 1, ns);
-    if (!st) st = rev(l, l + m, c, slot);
-    return st;
   }
 
   int run() {

@@ -50,6 +50,10 @@ def test_schedule_limits():
     # beyond the dynamic-programming range the binomial rule still passes its check
     big, stored = NodalDG2d.revolve_schedule(6000, 20)
     assert stored == 20 and big < 6 * 6000
+    # one free slot over a long trajectory: a deep schedule that the sweep
+    # walks without deep recursion
+    deep, stored = NodalDG2d.revolve_schedule(20000, 2)
+    assert stored == 2 and deep > 20000
 
 
 def test_schedule_arguments():
