@@ -90,16 +90,23 @@ __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
   for (int i = tid; i < T::RSR * LDB; i += kThreads) sRS[i] = 0.0;
   int err = 0;
   const int ntiles = (d.K + E - 1) / E;
+  // q tile, [e][node][field] -> Q[node][e*M + field]: the first tile here, each
+  // next one loaded into registers while this one's fluxes are evaluated and
+  // stored after them (Q is read only by the first two contractions)
+  constexpr int NQ = E * NP * M, QPT = (NQ + kThreads - 1) / kThreads;
+  auto put_q = [&](int i, double v) {
+    const int e = i / (NP * M), r = i - e * NP * M, j = r / M, f = r - j * M;
+    sQ[j * LDB + e * M + f] = v;
+  };
+  __syncthreads();  // the zero padding above is written before the first tile
+  if ((int)blockIdx.x < ntiles) {
+    const int k0 = blockIdx.x * E, nq = min(E, d.K - k0) * NP * M;
+    const double* src = a.x + (size_t)k0 * NP * M;
+    for (int i = tid; i < nq; i += kThreads) put_q(i, src[i]);
+  }
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int k0 = tile * E;
     const int ne = min(E, d.K - k0);
-    __syncthreads();
-    // q tile, [e][node][field] -> Q[node][e*M + field]
-    const double* src = a.x + (size_t)k0 * NP * M;
-    for (int i = tid; i < ne * NP * M; i += kThreads) {
-      const int e = i / (NP * M), r = i - e * NP * M, j = r / M, f = r - j * M;
-      sQ[j * LDB + e * M + f] = src[i];
-    }
     __syncthreads();
     // cubature values Qc = V Q (into the R/S buffer) and face traces I Q (to HBM)
     block_dgemm<T::NCR, T::COLS, T::NPK, T::LDA1, LDB, NWARPS>(
@@ -109,6 +116,15 @@ __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
       if (r < NF && e < ne) d.trace[((size_t)(k0 + e) * NF + r) * M + f] = v;
     });
     __syncthreads();
+    // the next tile's states, in flight during the flux evaluation
+    const int nxt = tile + (int)gridDim.x;
+    const int nq_next = nxt < ntiles ? min(E, d.K - nxt * E) * NP * M : 0;
+    double qn[QPT];
+#pragma unroll
+    for (int u = 0; u < QPT; ++u) {
+      const int i = tid + u * kThreads;
+      qn[u] = i < nq_next ? a.x[(size_t)nxt * E * NP * M + i] : 0.0;
+    }
     // physical flux at every cubature point; R = rx F + ry G into row c,
     // S = sx F + sy G into row NC + c (row c is overwritten by its reader only)
     for (int idx = tid; idx < ne * NC; idx += kThreads) {
@@ -123,6 +139,11 @@ __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
         sRS[c * LDB + e * M + f] = g.rx * F[f] + g.ry * G[f];
         sRS[(NC + c) * LDB + e * M + f] = g.sx * F[f] + g.sy * G[f];
       }
+    }
+#pragma unroll
+    for (int u = 0; u < QPT; ++u) {
+      const int i = tid + u * kThreads;
+      if (i < nq_next) put_q(i, qn[u]);
     }
     __syncthreads();
     // volume term: [Dr | Ds] [R; S]
@@ -693,12 +714,19 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
   using VT = VolTile<N, M>;
   using LT = LiftTile<N, M>;
   static unsigned configured = 0;  // bit per device
+  static int vol_res = 1, lift_res = 1;  // resident blocks per SM
   int dev = 0;
   cudaGetDevice(&dev);
   if (!(configured & (1u << (dev & 31)))) {
     cudaError_t e = cudaFuncSetAttribute(k_volume<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VT::BYTES);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_lift<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LT::BYTES);
+    if (e != cudaSuccess) return e;
+    // persistent grids of the blocks that are resident at once (registers
+    // and shared memory): a block beyond them would start a late second wave
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&vol_res, k_volume<EQ, N>, kThreads, VT::BYTES);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lift_res, k_lift<EQ, N>, kThreads, LT::BYTES);
     if (e != cudaSuccess) return e;
     configured |= 1u << (dev & 31);
   }
@@ -739,9 +767,7 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
     return cudaGetLastError();
   }
   const int vt = (d.K + VT::E - 1) / VT::E;
-  int per_sm = (int)((200 * 1024) / VT::BYTES);
-  if (per_sm < 1) per_sm = 1;
-  if (per_sm > 8) per_sm = 8;
+  int per_sm = vol_res < 1 ? 1 : (vol_res > 8 ? 8 : vol_res);
   int gv = sms * per_sm;
   if (gv > vt) gv = vt;
   if (a.phase != PHASE_FACE) {
@@ -762,9 +788,7 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
   k_face<EQ, N><<<gf, kThreads, 0, s>>>(d, a);
   if (ev) cudaEventRecord(ev[2], s);
   const int lt = (d.K + LT::E - 1) / LT::E;
-  int lper = (int)((200 * 1024) / LT::BYTES);
-  if (lper < 1) lper = 1;
-  if (lper > 8) lper = 8;
+  int lper = lift_res < 1 ? 1 : (lift_res > 8 ? 8 : lift_res);
   int gl = sms * lper;
   if (gl > lt) gl = lt;
   k_lift<EQ, N><<<gl, kThreads, LT::BYTES, s>>>(d, a);
@@ -780,17 +804,18 @@ cudaError_t launch_lift_t(const DgDev& d, const StageArgs& a, cudaStream_t s) {
   constexpr int M = Eq<EQ>::M;
   using LT = LiftTile<N, M>;
   static unsigned configured = 0;  // bit per device
+  static int lift_res = 1;          // resident blocks per SM
   int dev = 0;
   cudaGetDevice(&dev);
   if (!(configured & (1u << (dev & 31)))) {
     cudaError_t e = cudaFuncSetAttribute(k_lift<EQ, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LT::BYTES);
     if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lift_res, k_lift<EQ, N>, kThreads, LT::BYTES);
+    if (e != cudaSuccess) return e;
     configured |= 1u << (dev & 31);
   }
   const int lt = (d.K + LT::E - 1) / LT::E;
-  int lper = (int)((200 * 1024) / LT::BYTES);
-  if (lper < 1) lper = 1;
-  if (lper > 8) lper = 8;
+  int lper = lift_res < 1 ? 1 : (lift_res > 8 ? 8 : lift_res);
   int gl = num_sms() * lper;
   if (gl > lt) gl = lt;
   k_lift<EQ, N><<<gl, kThreads, LT::BYTES, s>>>(d, a);

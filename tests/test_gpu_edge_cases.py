@@ -28,11 +28,11 @@ def _cut(mesh, K):
 
 
 def _gas_at_rest(x, y):
-    """A density bump in a gas at rest (p = 1): the walls reflect sound waves,
-    no flow runs into them."""
+    """Density and pressure bumps in a gas at rest: sound waves start from the
+    pressure gradient and the walls reflect them; no flow runs into a wall."""
     U = np.zeros(x.shape + (4,))
     U[..., 0] = 1.0 + 0.2 * np.sin(1.3 * x + 0.4) * np.cos(0.9 * y)
-    U[..., 3] = 1.0 / 0.4
+    U[..., 3] = (1.0 + 0.2 * np.cos(1.1 * x - 0.3) * np.sin(0.7 * y + 0.5)) / 0.4
     return U
 
 
