@@ -693,20 +693,23 @@ __global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
   (void)err;
 }
 
+// Shared-memory size of a tile kernel and, once per device, how many of its
+// blocks are resident per SM (registers and shared memory): the persistent
+// grids launch that many, since a block beyond them would start a late
+// second wave.
 template <class Kern>
-cudaError_t set_smem(Kern k, size_t bytes, unsigned& configured) {
+cudaError_t set_smem(Kern k, size_t bytes, unsigned& configured, int& resident) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (configured & (1u << (dev & 31))) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k, kDThreads, bytes);
   if (e == cudaSuccess) configured |= 1u << (dev & 31);
   return e;
 }
 
-int tile_grid(int K, int E, size_t bytes) {
-  int per = (int)((200 * 1024) / bytes);
-  if (per < 1) per = 1;
-  if (per > 8) per = 8;
+int tile_grid(int K, int E, int resident) {
+  const int per = resident < 1 ? 1 : (resident > 8 ? 8 : resident);
   const int tiles = (K + E - 1) / E;
   const int g = sm_count() * per;
   return g < tiles ? g : tiles;
@@ -717,9 +720,10 @@ cudaError_t tangent_t(const DgDev& d, const TanArgs& a, cudaStream_t s) {
   constexpr int M = Eq<EQ>::M;
   using T = TanTile<N, M>;
   static unsigned configured = 0;
-  cudaError_t e = set_smem(k_tan_volume<EQ, N>, T::BYTES, configured);
+  static int resident = 1;
+  cudaError_t e = set_smem(k_tan_volume<EQ, N>, T::BYTES, configured, resident);
   if (e != cudaSuccess) return e;
-  k_tan_volume<EQ, N><<<tile_grid(d.K, T::E, T::BYTES), kDThreads, T::BYTES, s>>>(d, a.x, a.dx, a.dtrace, a.dvol);
+  k_tan_volume<EQ, N><<<tile_grid(d.K, T::E, resident), kDThreads, T::BYTES, s>>>(d, a.x, a.dx, a.dtrace, a.dvol);
   const int fthreads = d.nfaces * Sizes<N>::NG;
   int gf = (fthreads + kDThreads - 1) / kDThreads;
   if (gf > sm_count() * 8) gf = sm_count() * 8;
@@ -747,12 +751,13 @@ cudaError_t adjoint_t(const DgDev& d, const AdjArgs& a, cudaStream_t s) {
   constexpr int M = Eq<EQ>::M;
   using T = AdjTile<N, M>;
   static unsigned cpre = 0, cmain = 0;
-  cudaError_t e = set_smem(k_adj_pre<EQ, N>, T::PRE_BYTES, cpre);
+  static int rpre = 1, rmain = 1;
+  cudaError_t e = set_smem(k_adj_pre<EQ, N>, T::PRE_BYTES, cpre, rpre);
   if (e != cudaSuccess) return e;
-  e = set_smem(k_adj_main<EQ, N>, T::MAIN_BYTES, cmain);
+  e = set_smem(k_adj_main<EQ, N>, T::MAIN_BYTES, cmain, rmain);
   if (e != cudaSuccess) return e;
-  k_adj_pre<EQ, N><<<tile_grid(d.K, T::E, T::PRE_BYTES), kDThreads, T::PRE_BYTES, s>>>(d, a.x, a.wbar, a.sbar);
-  k_adj_main<EQ, N><<<tile_grid(d.K, T::E, T::MAIN_BYTES), kDThreads, T::MAIN_BYTES, s>>>(d, a);
+  k_adj_pre<EQ, N><<<tile_grid(d.K, T::E, rpre), kDThreads, T::PRE_BYTES, s>>>(d, a.x, a.wbar, a.sbar);
+  k_adj_main<EQ, N><<<tile_grid(d.K, T::E, rmain), kDThreads, T::MAIN_BYTES, s>>>(d, a);
   return cudaGetLastError();
 }
 
