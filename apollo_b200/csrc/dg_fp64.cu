@@ -26,6 +26,96 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Euler fluxes in float64 with one reciprocal of the density per state and
+// the flux formed along a direction directly (a n.F + b n.G in one pass): the
+// same quantities as WxEulerEqn's flux and Lax-Friedrichs flux
+// (wxeulereqn.cc:809-871, :1097-1117) to round-off, for states that need none
+// of the reference's clamps; a state that does (density below its floor or
+// not positive, pressure not positive) takes the equation's own code, which
+// applies them and raises its error flags.
+template <int MF> struct EulerFast64 {
+  static constexpr int IE = MF - 1;
+  struct Side {
+    double rho, ir, vx, vy, vz, p;
+    bool clean;
+  };
+  __device__ __forceinline__ static Side side(const EqParams& P, const double* q) {
+    const double g1 = P.p[0] - 1.0, minD = P.p[2];
+    Side s;
+    s.rho = q[0];
+    s.ir = 1.0 / s.rho;
+    s.vx = q[1] * s.ir;
+    s.vy = q[2] * s.ir;
+    s.vz = MF == 5 ? q[3] * s.ir : 0.0;
+    s.p = g1 * (q[IE] - 0.5 * s.rho * (s.vx * s.vx + s.vy * s.vy + s.vz * s.vz));
+    s.clean = s.rho > 0.0 && s.rho >= minD && s.p > 0.0;
+    return s;
+  }
+  // the flux along (ax, ay): ax F + ay G
+  __device__ __forceinline__ static void along(const Side& s, const double* q, double ax, double ay, double* R) {
+    const double ua = s.vx * ax + s.vy * ay;
+    R[0] = s.rho * ua;
+    R[1] = s.rho * s.vx * ua + s.p * ax;
+    R[2] = s.rho * s.vy * ua + s.p * ay;
+    if (MF == 5) R[3] = s.rho * s.vz * ua;
+    R[IE] = (q[IE] + s.p) * ua;
+  }
+};
+
+template <int EQ> constexpr bool kEulerEq = EQ == EQ_EULER || EQ == EQ_EULER2D;
+
+// R = rx F + ry G, S = sx F + sy G of one state
+template <int EQ>
+__device__ __forceinline__ void volume_flux(const EqParams& P, const double* q, double rx, double ry, double sx,
+                                            double sy, double* R, double* S, int* err) {
+  constexpr int M = Eq<EQ>::M;
+  if constexpr (kEulerEq<EQ>) {
+    using X = EulerFast64<M>;
+    const typename X::Side sd = X::side(P, q);
+    if (sd.clean) {
+      X::along(sd, q, rx, ry, R);
+      X::along(sd, q, sx, sy, S);
+      return;
+    }
+  }
+  double F[M], G[M];
+  Eq<EQ>::flux2(P, q, F, G, err);
+#pragma unroll
+  for (int f = 0; f < M; ++f) {
+    R[f] = rx * F[f] + ry * G[f];
+    S[f] = sx * F[f] + sy * G[f];
+  }
+}
+
+// The numerical flux of one face point (qM, qP may be modified as the
+// reference modifies them); the Euler Lax-Friedrichs flux of two clean states
+// through EulerFast64
+template <int EQ>
+__device__ __forceinline__ double face_flux(const EqParams& P, double nx, double ny, double* qM, double* qP,
+                                            double* nf, int* err) {
+  constexpr int M = Eq<EQ>::M;
+  if constexpr (kEulerEq<EQ>) {
+    const int kind = (int)P.p[3];
+    if (kind != NF_HLL && kind != NF_ROE && kind != NF_WAVE) {
+      using X = EulerFast64<M>;
+      const typename X::Side a = X::side(P, qM), b = X::side(P, qP);
+      if (a.clean && b.clean) {
+        double FM[M], FP[M];
+        X::along(a, qM, nx, ny, FM);
+        X::along(b, qP, nx, ny, FP);
+        const double gamma = P.p[0];
+        const double cM = sqrt(a.vx * a.vx + a.vy * a.vy + a.vz * a.vz) + sqrt(gamma * a.p * a.ir);
+        const double cP = sqrt(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) + sqrt(gamma * b.p * b.ir);
+        const double lam = cM > cP ? cM : cP;
+#pragma unroll
+        for (int c = 0; c < M; ++c) nf[c] = 0.5 * (FM[c] + FP[c] + lam * (qM[c] - qP[c]));
+        return lam;
+      }
+    }
+  }
+  return Eq<EQ>::numflux(P, nx, ny, qM, qP, nf, err);
+}
+
 
 // Tile of elements for the float64 volume kernel.  Columns of every GEMM are
 // (element, field) pairs; rows are cubature points, Gauss points or nodes.
@@ -129,15 +219,15 @@ __global__ void __launch_bounds__(kThreads) k_volume(DgDev d, StageArgs a) {
     // S = sx F + sy G into row NC + c (row c is overwritten by its reader only)
     for (int idx = tid; idx < ne * NC; idx += kThreads) {
       const int e = idx / NC, c = idx - e * NC;
-      double qc[M], F[M], G[M];
+      double qc[M], R[M], S[M];
 #pragma unroll
       for (int f = 0; f < M; ++f) qc[f] = sRS[c * LDB + e * M + f];
-      P::flux2(d.eqp, qc, F, G, &err);
       const ElemGeo& g = d.geo[k0 + e];
+      volume_flux<EQ>(d.eqp, qc, g.rx, g.ry, g.sx, g.sy, R, S, &err);
 #pragma unroll
       for (int f = 0; f < M; ++f) {
-        sRS[c * LDB + e * M + f] = g.rx * F[f] + g.ry * G[f];
-        sRS[(NC + c) * LDB + e * M + f] = g.sx * F[f] + g.sy * G[f];
+        sRS[c * LDB + e * M + f] = R[f];
+        sRS[(NC + c) * LDB + e * M + f] = S[f];
       }
     }
 #pragma unroll
@@ -312,16 +402,15 @@ __global__ void __launch_bounds__(kThreads) k_stage64(DgDev d, StageArgs a) {
     // physical flux at the cubature points: R into row c, S into row NC + c
     for (int idx = tid; idx < ne * NC; idx += kThreads) {
       const int e = idx / NC, c = idx - e * NC;
-      double qc[M], F[M], G[M];
+      double qc[M], R[M], S[M];
 #pragma unroll
       for (int f = 0; f < M; ++f) qc[f] = sRS[c * LDB + e * M + f];
-      P::flux2(d.eqp, qc, F, G, &err);
       const double* gs = sGS + e * 16;
-      const double rx = gs[0], ry = gs[1], sx = gs[2], sy = gs[3];
+      volume_flux<EQ>(d.eqp, qc, gs[0], gs[1], gs[2], gs[3], R, S, &err);
 #pragma unroll
       for (int f = 0; f < M; ++f) {
-        sRS[c * LDB + e * M + f] = rx * F[f] + ry * G[f];
-        sRS[(NC + c) * LDB + e * M + f] = sx * F[f] + sy * G[f];
+        sRS[c * LDB + e * M + f] = R[f];
+        sRS[(NC + c) * LDB + e * M + f] = S[f];
       }
     }
     // numerical flux at the face Gauss points into rows 2 NC + j NG + g
@@ -350,7 +439,7 @@ __global__ void __launch_bounds__(kThreads) k_stage64(DgDev d, StageArgs a) {
         const double y = 0.5 * (-g.vy[0] * (r + s) + g.vy[1] * (1. + r) + g.vy[2] * (1. + s));
         apply_bc<EQ, double>(d.bcs, -d.conn[(size_t)k * 6 + 2 * j], t, x, y, nx, ny, qM, qP);
       }
-      const double lam = P::numflux(d.eqp, nx, ny, qM, qP, nf, &err);
+      const double lam = face_flux<EQ>(d.eqp, nx, ny, qM, qP, nf, &err);
       lam_acc.add(d.st, inst, fabs(lam));
       const double w = -(gs[4] * (d.gw[gq] * gs[12 + j]));
 #pragma unroll
@@ -444,7 +533,7 @@ __global__ void __launch_bounds__(kThreads) k_face(DgDev d, StageArgs a) {
       const double y = 0.5 * (-g.vy[0] * (r + s) + g.vy[1] * (1. + r) + g.vy[2] * (1. + s));
       apply_bc<EQ, double>(d.bcs, -fr.k2, t, x, y, nx, ny, qM, qP);
     }
-    double lam = P::numflux(d.eqp, nx, ny, qM, qP, nf, &err);
+    double lam = face_flux<EQ>(d.eqp, nx, ny, qM, qP, nf, &err);
     lam_acc.add(d.st, inst, fabs(lam));
     const double w = d.gw[gq] * sJ;
     store_point<M>(d.flux + ((size_t)fr.k1 * NF + fr.f1 * NG + gq) * M, nf, w);
