@@ -320,7 +320,9 @@ template <int EQ> struct AdjPhys {
     }
     return r;
   }
-  // (d f*(n, a, b) / d a)^T dv and (d f* / d b)^T dv
+  // (d f*(n, a, b) / d a)^T dv and (d f* / d b)^T dv (LF_ONLY: the caller
+  // knows the flux is Lax-Friedrichs; nothing to drop here)
+  template <bool LF_ONLY = false>
   __device__ __forceinline__ static void face(const EqParams& P, double nx, double ny, const DVec<M>& a,
                                               const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
                                               bool want_b, int* err) {
@@ -415,13 +417,16 @@ template <int MF> struct EulerAdjPhys {
   // f* = 1/2 [Fn(a) + Fn(b) + lambda (a - b)], lambda = max(c(a), c(b)):
   // abar = 1/2 [ (dFn(a)/da)^T dv + lambda dv + (dv . (a - b)) grad c(a) [a wins] ]
   // bbar = 1/2 [ (dFn(b)/db)^T dv - lambda dv + (dv . (a - b)) grad c(b) [b wins] ]
+  template <bool LF_ONLY = false>
   __device__ __forceinline__ static void face(const EqParams& P, double nx, double ny, const DVec<M>& a,
                                               const DVec<M>& b, const DVec<M>& dv, DVec<M>& abar, DVec<M>& bbar,
                                               bool want_b, int* err) {
-    if ((int)P.p[3] != NF_LF) {
-      // HLL, Roe, Wave: the derivative of Apollo's own flux, quirks included
-      dual1_face<MF == 5 ? EQ_EULER : EQ_EULER2D, M>(P, nx, ny, a, b, dv, abar, bbar, want_b, err);
-      return;
+    if constexpr (!LF_ONLY) {
+      if ((int)P.p[3] != NF_LF) {
+        // HLL, Roe, Wave: the derivative of Apollo's own flux, quirks included
+        dual1_face<MF == 5 ? EQ_EULER : EQ_EULER2D, M>(P, nx, ny, a, b, dv, abar, bbar, want_b, err);
+        return;
+      }
     }
     double ga[M], gb[M];
     const double ca = EulerAdj<MF>::speed(P, a.v, ga, err), cb = EulerAdj<MF>::speed(P, b.v, gb, err);
@@ -527,7 +532,11 @@ __global__ void __launch_bounds__(kDThreads) k_adj_pre(DgDev d, const double* __
   }
 }
 
-template <int EQ, int N>
+// GEN: the general face code (boundary faces, and the Euler fluxes other
+// than Lax-Friedrichs); without it, the kernel for meshes with no boundary
+// face and a Lax-Friedrichs (or linear) flux, whose smaller code keeps more
+// of its state in registers.
+template <int EQ, int N, bool GEN>
 __global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
   using P = Eq<EQ>;
   constexpr int M = P::M;
@@ -595,7 +604,7 @@ __global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
       for (int j = 0; j < M; ++j) sQC[c * LDB + e * M + j] = gbar.v[j];
     }
     // faces: w_g (s_own - s_partner) d f*(n_own, a, b) / d a at every Gauss point
-    const bool two_sided = flux_two_sided<EQ>(d.eqp);
+    const bool two_sided = GEN && flux_two_sided<EQ>(d.eqp);
     for (int idx = tid; idx < ne * NF; idx += kDThreads) {
       const int e = idx / NF, fg = idx - e * NF, fc = fg / NG, gq = fg - fc * NG;
       const int k = k0 + e;
@@ -636,8 +645,12 @@ __global__ void __launch_bounds__(kDThreads, 2) k_adj_main(DgDev d, AdjArgs a) {
           dvec.v[f] = w * (a.sbar[own + f] - a.sbar[par + f]);
         }
         DVec<M> unused;
-        AdjPhys<EQ>::face(d.eqp, g.nx[fc], g.ny[fc], qa, qb, dvec, abar, unused, false, &err);
+        AdjPhys<EQ>::template face<!GEN>(d.eqp, g.nx[fc], g.ny[fc], qa, qb, dvec, abar, unused, false, &err);
         }
+      } else if constexpr (!GEN) {
+        // (the host launches this form only for meshes without boundary faces)
+#pragma unroll
+        for (int j = 0; j < M; ++j) abar.v[j] = 0.0;
       } else {
         // boundary: ghost state b = A a + c (every supported boundary hook is
         // affine in the trace); abar = (df*/da)^T dv + A^T (df*/db)^T dv
@@ -754,10 +767,18 @@ cudaError_t adjoint_t(const DgDev& d, const AdjArgs& a, cudaStream_t s) {
   static int rpre = 1, rmain = 1;
   cudaError_t e = set_smem(k_adj_pre<EQ, N>, T::PRE_BYTES, cpre, rpre);
   if (e != cudaSuccess) return e;
-  e = set_smem(k_adj_main<EQ, N>, T::MAIN_BYTES, cmain, rmain);
+  static unsigned clean = 0;
+  static int rlean = 1;
+  e = set_smem(k_adj_main<EQ, N, true>, T::MAIN_BYTES, cmain, rmain);
+  if (e != cudaSuccess) return e;
+  e = set_smem(k_adj_main<EQ, N, false>, T::MAIN_BYTES, clean, rlean);
   if (e != cudaSuccess) return e;
   k_adj_pre<EQ, N><<<tile_grid(d.K, T::E, rpre), kDThreads, T::PRE_BYTES, s>>>(d, a.x, a.wbar, a.sbar);
-  k_adj_main<EQ, N><<<tile_grid(d.K, T::E, rmain), kDThreads, T::MAIN_BYTES, s>>>(d, a);
+  const bool lf = !(EQ == EQ_EULER || EQ == EQ_EULER2D) || (int)d.eqp.p[3] == NF_LF;
+  if (d.nbound == 0 && lf)
+    k_adj_main<EQ, N, false><<<tile_grid(d.K, T::E, rlean), kDThreads, T::MAIN_BYTES, s>>>(d, a);
+  else
+    k_adj_main<EQ, N, true><<<tile_grid(d.K, T::E, rmain), kDThreads, T::MAIN_BYTES, s>>>(d, a);
   return cudaGetLastError();
 }
 

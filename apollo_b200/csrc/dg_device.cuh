@@ -73,6 +73,7 @@ struct DgDev {
   int fp64_fused;  // float64 stages: 0 the three kernels, 1 the fused stage kernel where it applies,
                    // 2 the fused kernel where its tiles fit one resident wave (launch-bound meshes)
   int nghost;      // ghost element slots of a partitioned mesh (their faces' traces come from peers)
+  int nbound;      // boundary faces of the local mesh
   // bounded device waits of the mixed stage kernel: polls before a wait gives
   // up (0: the default, about 2 s), and a test switch that points the kernel's
   // first wait at a barrier nothing completes (apollo_dg_debug_set_waits)

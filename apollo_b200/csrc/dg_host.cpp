@@ -89,6 +89,7 @@ struct apollo_dg {
   // blocks of hrecv unpacked to halo_dst (ghost face blocks)
   bool partitioned = false;
   int KG = 0;
+  int nbound = 0;  // boundary faces of the local mesh
   std::vector<int> peers, send_count, recv_count;
   int n_send = 0, n_recv = 0;
   int *halo_src_d = nullptr, *halo_dst_d = nullptr;
@@ -209,6 +210,7 @@ DgDev make_dev(const apollo_dg* h) {
   d.tile_shape = h->tile_shape;
   d.fp64_fused = h->fp64_fused;
   d.nghost = h->KG;
+  d.nbound = h->nbound;
   d.wait_limit = h->wait_limit;
   d.debug_stall = h->debug_stall;
   d.src = h->src;
@@ -716,6 +718,9 @@ apollo_status set_mesh_body(apollo_dg* h, int nverts, const double* vx, const do
       }
     }
   }
+  h->nbound = 0;
+  for (const FaceRec& fr : h->faces_h)
+    if (fr.k2 < 0) ++h->nbound;
   // device buffers: state-sized ones for the local elements, geometry and
   // trace/flux scratch with the ghost slots
   const size_t nU = (size_t)K * Np * M, nT = (size_t)(K + G) * o.Nf * M;
