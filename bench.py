@@ -68,6 +68,8 @@ def parse():
                     help="profiling driver: set up the workload, run this many RHS evaluations, exit")
     ap.add_argument("--steps-only", type=int, default=0,
                     help="profiling driver: set up the workload, advance this many SSPRK steps, exit")
+    ap.add_argument("--fp64-kernels", type=int, default=0, choices=[0, 1, 2],
+                    help="profiling drivers: the float64 stage form (0 three kernels, 1 fused, 2 by mesh size)")
     return ap.parse_args()
 
 
@@ -77,6 +79,7 @@ def rhs_only(args):
     from apollo_b200 import NodalDG2d, problems
     p = problems.euler_vortex(n=args.n, N=args.order, fields=4)
     s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=0)
+    s.set_fp64_kernels(args.fp64_kernels)
     x, y = s.node_coords()
     u = torch.from_numpy(np.ascontiguousarray(p.ic(x, y))).cuda()
     out = torch.empty_like(u)
@@ -97,6 +100,7 @@ def steps_only(args):
     from apollo_b200 import NodalDG2d, problems
     p = problems.euler_vortex(n=args.n, N=args.order, fields=4)
     s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=0)
+    s.set_fp64_kernels(args.fp64_kernels)
     x, y = s.node_coords()
     s.set_state(np.ascontiguousarray(p.ic(x, y)))
     prec = "fp64" if args.precision == "auto" else args.precision
