@@ -521,7 +521,7 @@ apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name) {
     else if (n == "Wave") kind = NF_WAVE;
     else if (n != "LF") h->err = "numerical flux " + n + " not recognised: Lax-Friedrichs used";
     h->eqp.p[3] = kind;
-  } else if (h->eq == EQ_ADVECTION) {
+  } else if (h->eq == EQ_ADVECTION || h->eq == EQ_MAXWELL_TM) {
     if (n == "upwind") kind = NF_UPWIND;
     else if (n != "LF") h->err = "numerical flux " + n + " not recognised: Lax-Friedrichs used";
     h->eqp.p[3] = kind;

@@ -34,7 +34,9 @@ enum BcKind : int {
 // stored in EqParams::p[3] of the Euler kinds
 // Numerical fluxes: Apollo's Euler Numerical_Flux codes (wxeulereqn.cc:10-15);
 // NF_UPWIND is an extension for advection (dissipation |n.u| instead of
-// Apollo's max(|ux|, |uy|)), held in the equation parameters' slot 3
+// Apollo's max(|ux|, |uy|)) and for the planar Maxwell TM form (no
+// dissipation on the normal magnetic field, whose wave speed is 0), held in
+// the equation parameters' slot 3
 enum NumFlux : int { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4, NF_UPWIND = 8 };
 
 enum ErrBits : int { ERRB_NONPHYS = 1, ERRB_NAN = 2, ERRB_TIMEOUT = 4 };
@@ -423,6 +425,14 @@ template <> struct Eq<EQ_MAXWELL_TM> {
 #pragma unroll
     for (int c = 0; c < 3; ++c)
       nf[c] = T(0.5) * (nx * (fM[c] + fP[c]) + ny * (gM[c] + gP[c]) + lambda * (qM[c] - qP[c]));
+    if ((int)P.p[3] == NF_UPWIND) {
+      // the upwind extension: n.B travels at speed 0 (the flux along n maps
+      // (Ez, B) to c^2 (n x B)_z and Ez (n_y, -n_x), with eigenvalues +-c on
+      // (Ez, tangential B) and 0 on n.B), so its jump is not dissipated
+      const T dBn = nx * (qM[1] - qP[1]) + ny * (qM[2] - qP[2]);
+      nf[1] = nf[1] - T(0.5) * lambda * dBn * nx;
+      nf[2] = nf[2] - T(0.5) * lambda * dBn * ny;
+    }
     return lambda;
   }
   APOLLO_HD static double lf_lambda(const EqParams& P, const double* qM, const double* qP) {

@@ -353,6 +353,20 @@ def maxwell_measure(args, device: int, cpu: bool):
                      "l2_vs_exact_mode": float(np.linalg.norm(U - ex) / np.linalg.norm(ex))}
     out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     out["l2_mixed_vs_fp64"] = float(np.linalg.norm(ends["mixed"] - ends["fp64"]) / np.linalg.norm(ends["fp64"]))
+    # the configuration names an upwind flux; Apollo's Maxwell flux is
+    # Lax-Friedrichs (the runs above), the exact upwind flux (no dissipation
+    # on the normal magnetic field) is this library's extension
+    su = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, bcs=p.bcs, device=device,
+                   stream=stream.cuda_stream, numerical_flux="upwind")
+    su.set_state(U0)
+    ms, (t, dt) = _device_run(su, stream, U0, dt0, "fp64", steps, warmup=2)
+    U = su.get_state()
+    ex = p.exact(x, y, t)
+    e1 = 0.5 * float(np.sum(su.square_integrals(U)))
+    out["fp64_upwind"] = {"value": dofs * steps / (ms / 1000.0), "ms_per_step": ms / steps, "t_end": t,
+                          "energy_drift_rel": (e1 - e0) / e0,
+                          "l2_vs_exact_mode": float(np.linalg.norm(U - ex) / np.linalg.norm(ex))}
+    su.close()
     if cpu:
         from oracle import oracle as orc
         threads = os.cpu_count() or 1

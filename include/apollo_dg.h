@@ -136,7 +136,10 @@ apollo_status apollo_dg_set_limiter_text(apollo_dg* h, const char* kind, const c
  * y-momentum flux, and Wave's fall-through to LF on rotated traces.
  * "advectionEqn" takes "LF" (Apollo's, dissipation max(|ux|, |uy|)) or the
  * extension "upwind" (dissipation |n.u|, the exact upwind flux; the dt
- * policy keeps Apollo's speed).  Maxwell has only LF (the name is ignored).
+ * policy keeps Apollo's speed).  "maxwellTM" takes "LF" (Apollo's,
+ * dissipation c0 on every field) or the extension "upwind" (the exact upwind
+ * flux: no dissipation on the normal magnetic field, whose wave speed is 0).
+ * "phMaxwellEqn" has only LF (the name is ignored).
  * Mixed precision and the derivatives (tangent and adjoint) take every one
  * of them. */
 apollo_status apollo_dg_set_numerical_flux(apollo_dg* h, const char* name);

@@ -215,7 +215,8 @@ enum { EQ_ADVECTION = 0, EQ_EULER = 1, EQ_MAXWELL = 2 };
 enum { BC_FIXED = 0, BC_VORTEX = 1, BC_TM = 2, BC_PEC = 3, BC_EULER_WALL = 4, BC_EULER_INFLOW = 5,
        BC_EULER_ZEROGRAD = 6, BC_EULER_DIRICHLET = 7 };
 // Euler Numerical_Flux codes (wxeulereqn.cc:10-15), held in eqp[3]
-// (NF_UPWIND: an extension for advection, dissipation |n.u|; not in Apollo)
+// (NF_UPWIND: an extension, not in Apollo: advection with dissipation |n.u|;
+// the Maxwell TM fields without dissipation of the normal magnetic field)
 enum { NF_LF = 0, NF_HLL = 1, NF_ROE = 2, NF_WAVE = 4, NF_UPWIND = 8 };
 enum { ERR_NONPHYS = 1, ERR_NAN = 2, ERR_JAC = 4 };
 
@@ -455,6 +456,21 @@ void eq_numflux(Oracle& o, const double* n, double* qM, double* qP, double* nf, 
     const double diss = std::fabs(n[0] * o.eqp[0] + n[1] * o.eqp[1]);
     nf[0] = 0.5 * (n[0] * (fM[0] + fP[0]) + n[1] * (gM[0] + gP[0]) + diss * (qM[0] - qP[0]));
     *lam = dmax2(std::fabs(o.eqp[0]), std::fabs(o.eqp[1]));
+    return;
+  }
+  if (o.eq == EQ_MAXWELL && (int)o.eqp[3] == NF_UPWIND) {
+    // the upwind extension for the TM fields (Ez, Bx, By = 2, 3, 4) with
+    // chi = gamma = 0: Apollo's Lax-Friedrichs flux without the dissipation
+    // of the normal magnetic field, whose wave speed is 0
+    double fM[8], fP[8], gM[8], gP[8];
+    maxwell_flux(o, 0, qM, fM); maxwell_flux(o, 0, qP, fP); maxwell_flux(o, 1, qM, gM); maxwell_flux(o, 1, qP, gP);
+    const double lambda = dmax3(o.eqp[2] * o.eqp[0], o.eqp[1] * o.eqp[0], o.eqp[0]);
+    for (int c = 0; c < o.meqn; ++c)
+      nf[c] = 0.5 * (n[0] * (fM[c] + fP[c]) + n[1] * (gM[c] + gP[c]) + lambda * (qM[c] - qP[c]));
+    const double dBn = n[0] * (qM[3] - qP[3]) + n[1] * (qM[4] - qP[4]);
+    nf[3] -= 0.5 * lambda * dBn * n[0];
+    nf[4] -= 0.5 * lambda * dBn * n[1];
+    *lam = lambda;
     return;
   }
   if (o.ref_numflux) { o.ref_numflux(o.ref_ctx, n, qM, qP, nf, lam); return; }

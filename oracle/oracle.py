@@ -28,7 +28,7 @@ BC_FIXED, BC_VORTEX, BC_TM, BC_PEC = 0, 1, 2, 3
 BC_EULER_WALL, BC_EULER_INFLOW, BC_EULER_ZEROGRAD, BC_EULER_DIRICHLET = 4, 5, 6, 7
 # Euler numerical fluxes (eqp[3]), Apollo's Numerical_Flux codes
 NF_LF, NF_HLL, NF_ROE, NF_WAVE = 0, 1, 2, 4
-NF_UPWIND = 8  # advection only: an extension (not in Apollo)
+NF_UPWIND = 8  # an extension (not in Apollo): advection, and the Maxwell TM fields with chi = gamma = 0
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
