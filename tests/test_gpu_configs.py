@@ -8,7 +8,8 @@ grids.
   (K = 130,050), 5 steps (the oracle takes about a second per step on 16
   threads);
 * Maxwell TM with the mirror (PEC) boundary condition at N = 5 on a reduced
-  48 x 48 vertex grid (K = 4,418), 60 steps.
+  48 x 48 vertex grid (K = 4,418), 60 steps, and on the configuration's own
+  512 x 512 vertex grid (K = 522,242), 2 steps.
 
 States after the steps agree with the oracle to 1e-12 relative L2, the time
 reached and the next dt to 1e-13.  The mixed form is held against the float64
@@ -103,5 +104,26 @@ def test_maxwell_tm_config_order5_walls(oracle_lib):
     assert rel_l2(U, Uc[..., 2:5]) <= TOL
     s.set_state(U3)
     s.advance(60, 0.0, dt0, precision="mixed")
+    assert rel_l2(s.get_state(), U) <= MIXED_TOL
+    s.close()
+
+
+def test_maxwell_tm_config_full_mesh(oracle_lib):
+    """The Maxwell TM configuration's own mesh (512 x 512 vertices, K = 522,242),
+    N = 5, mirror walls: 2 steps against the oracle (about 7 s per step on 16
+    threads), the mixed form on the same steps."""
+    orc = oracle_lib
+    p = problems.maxwell_tm(n=512, N=5)
+    assert p.mesh.K == 522242
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, bcs=p.bcs)
+    o = _oracle(orc, p, orc.EQ_MAXWELL, (1.0, 0.0, 0.0), bcs=((orc.BC_TM, ()),))
+    x, y = s.node_coords()
+    U3 = np.ascontiguousarray(p.ic(x, y))
+    U8 = np.zeros(U3.shape[:2] + (8,))
+    U8[..., 2:5] = U3
+    U, Uc, dt0 = _run_both(s, o, U3, U8, 2)
+    assert rel_l2(U, Uc[..., 2:5]) <= TOL
+    s.set_state(U3)
+    s.advance(2, 0.0, dt0, precision="mixed")
     assert rel_l2(s.get_state(), U) <= MIXED_TOL
     s.close()
