@@ -144,8 +144,18 @@ __global__ void __launch_bounds__(128) k_limiter_grad(DgDev d, LimArgs L, const 
     double qm[M], qp[M];
     for (int f = 0; f < M; ++f) qm[f] = qv(q, node, f);
     if (nb[edge] < 0) {
+      // Apollo reads the patch neighbours through the pointer that held this
+      // element's nodes and never points it back, so the condition sees the
+      // nodes of the last neighbour read before this face (faces in order;
+      // this element's own where none): wxhesthavenwarburtoneulerlimiter.cc
+      // :158, 221, aptualiabadilimiter.cc:170, 233
+      const double* qs = q;
+      for (int j = 0; j < edge; ++j)
+        if (nb[j] >= 0) qs = x + (size_t)nb[j] * NP * M;
+      double qin[M];
+      for (int f = 0; f < M; ++f) qin[f] = qv(qs, node, f);
       apply_bc<EQ, double>(d.bcs, -nb[edge], xn[(size_t)e * NP + node], yn[(size_t)e * NP + node], 0.0, g.nx[edge],
-                           g.ny[edge], qm, qp);
+                           g.ny[edge], qin, qp);
     } else {
       const double* qn = x + (size_t)nb[edge] * NP * M;
       const int pn = L.fmask[nf[edge] * NPF + NPF - 1 - nd];

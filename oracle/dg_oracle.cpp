@@ -746,11 +746,28 @@ void orc_connectivity(void* h, int* conn) {
   Oracle* o = (Oracle*)h;
   std::memcpy(conn, o->conn.data(), o->conn.size() * sizeof(int));
 }
-// Operator export for tests: which = 0 Vc, 1 Drc, 2 Dsc, 3 interp, 4 VVT, 5 cub w, 6 gauss w
+// Operator export for tests: which = 0 Vc, 1 Drc, 2 Dsc, 3 interp, 4 VVT, 5 cub w, 6 gauss w,
+// 7 the mass matrix inv(V V^T) that the limiters average with
 void orc_operator(void* h, int which, double* out) {
   Oracle* o = (Oracle*)h;
+  if (which == 7) {
+    std::vector<double> mass = invert(o->VVT, o->Np);
+    std::memcpy(out, mass.data(), mass.size() * sizeof(double));
+    return;
+  }
   const std::vector<double>* v[] = {&o->Vc, &o->Drc, &o->Dsc, &o->interp, &o->VVT, &o->cw, &o->gw};
   std::memcpy(out, v[which]->data(), v[which]->size() * sizeof(double));
+}
+
+// Face node masks [3][N + 1] (the limiters' face and vertex nodes).
+void orc_fmask(void* h, int* out) {
+  Oracle* o = (Oracle*)h;
+  std::memcpy(out, o->fmask.data(), o->fmask.size() * sizeof(int));
+}
+// Boundary condition `tag` (1-based, in bcs order) at one point, for tests:
+// xc = [t, x, y, 0, 0], nx the unit outward normal.
+void orc_apply_bc(void* h, int tag, const double* xc, const double* nx, const double* q, double* qb) {
+  apply_bc(*(Oracle*)h, tag, xc, nx, q, qb);
 }
 
 // One right-hand-side evaluation, WxNodalDG2dMethod::step
@@ -1088,6 +1105,12 @@ static void apply_limiter(Oracle& o, double* u) {
     for (int edge = 0; edge < 3; ++edge)
       for (int n = 0; n < NpF; ++n)
         for (int c = 0; c < meqn; ++c) QM[(edge * NpF + n) * meqn + c] = qIn[o.fmask[edge * NpF + n] * meqn + c];
+    // Apollo reads the patch neighbours through the same pointer as the
+    // element's own nodes and never points it back
+    // (wxhesthavenwarburtoneulerlimiter.cc:158, 221; aptualiabadilimiter.cc:
+    // 170, 233): a boundary face listed after an interior face takes its
+    // ghost nodes from that neighbour's nodes at this face's node ids.
+    const double* qsrc = qIn;
     for (int el = 0; el < 3; ++el) {
       if (connect[2 * el] < 0) {
         double NX[2] = {normals[3 * el], normals[3 * el + 1]};
@@ -1100,12 +1123,13 @@ static void apply_limiter(Oracle& o, double* u) {
         }
         for (int n = 0; n < NpF; ++n) {
           int node = o.fmask[el * NpF + n];
-          for (int c = 0; c < meqn; ++c) qCons[c] = qIn[node * meqn + c];
+          for (int c = 0; c < meqn; ++c) qCons[c] = qsrc[node * meqn + c];
           bc(-connect[2 * el], X(e, node), Y(e, node), NX, qCons, qBC);
           for (int c = 0; c < meqn; ++c) QP[(el * NpF + n) * meqn + c] = qBC[c];
         }
       } else {
         const double* qn = &u[(size_t)connect[2 * el] * Np * meqn];
+        qsrc = qn;
         averages(qn, qCons, qPrim);
         for (int c = 0; c < meqn; ++c) {
           ConsAve[c][el + 1] = qCons[c];

@@ -5,6 +5,9 @@
 * ``RefPlugins``  — Apollo's own equation plugins and exprFunc compiled
                     unmodified (ref_adapter.cpp, built to _ref/libapollo_ref.so
                     where the Apollo source tree exists).
+* ``RefLimiter``  — Apollo's own eulerLimiterHW and grid boundary conditions
+                    compiled unmodified (ref_limiter.cpp, built to
+                    _ref/libapollo_reflim.so where the Apollo source tree exists).
 
 Only tests, ``__graft_entry__.smoke`` and the CPU-baseline leg of ``bench.py``
 import this module.
@@ -20,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libapollo_ref.so")
+REFLIM_PATH = os.path.join(HERE, "_ref", "libapollo_reflim.so")
 
 EQ_ADVECTION, EQ_EULER, EQ_MAXWELL = 0, 1, 2
 # source plugins (Apollo kind names tranverseMagneticSrc, pointCurrentSrc)
@@ -55,7 +59,7 @@ def build(with_ref: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     src = reference_src()
     if with_ref and os.path.isdir(src):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"APOLLO_SRC={src}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "reflim", f"APOLLO_SRC={src}"], check=True)
 
 
 def _lib():
@@ -78,6 +82,8 @@ def _lib():
     lib.orc_node_coords.argtypes = [C.c_void_p, _dp, _dp]
     lib.orc_connectivity.argtypes = [C.c_void_p, _ip]
     lib.orc_operator.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.orc_fmask.argtypes = [C.c_void_p, _ip]
+    lib.orc_apply_bc.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
     lib.orc_rhs.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, _dp]
     lib.orc_rhs.restype = C.c_double
     lib.orc_init_dt.argtypes = [C.c_void_p, _dp]
@@ -159,10 +165,24 @@ class Oracle:
 
     def operator(self, which: int):
         shapes = {0: (self.Nc, self.Np), 1: (self.Nc, self.Np), 2: (self.Nc, self.Np), 3: (3 * self.Ng, self.Np),
-                  4: (self.Np, self.Np), 5: (self.Nc,), 6: (self.Ng,)}
+                  4: (self.Np, self.Np), 5: (self.Nc,), 6: (self.Ng,), 7: (self.Np, self.Np)}
         out = np.empty(shapes[which])
         self.lib.orc_operator(self.h, which, _p(out))
         return out
+
+    def fmask(self):
+        out = np.empty(3 * (self.N + 1), dtype=np.int32)
+        self.lib.orc_fmask(self.h, _p(out, _ip))
+        return out
+
+    def apply_bc(self, tag: int, xc, nx, q):
+        """Boundary condition `tag` (1-based, in bcs order) at one point."""
+        xc5 = np.zeros(5)
+        xc5[:len(xc)] = xc
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        qb = np.zeros(max(len(q), 8))
+        self.lib.orc_apply_bc(self.h, int(tag), _p(xc5), _p(np.array(nx, dtype=np.float64)), _p(q), _p(qb))
+        return qb[:len(q)]
 
     @property
     def error(self) -> int:
@@ -346,4 +366,78 @@ class RefPlugins:
     def exprfunc_eval(self, h, t: float, x: float, y: float):
         out = np.zeros(self.lib.ref_exprfunc_size(h))
         self.lib.ref_exprfunc_eval(h, t, x, y, _p(out))
+        return out
+
+
+class RefLimiter:
+    """Apollo's own eulerLimiterHW and grid boundary-condition plugins
+    (compiled unmodified) on the oracle's geometry: node coordinates, face
+    masks, mass matrix and element-to-element-to-face table of an Oracle."""
+
+    def __init__(self, o: "Oracle"):
+        if not os.path.exists(REFLIM_PATH):
+            raise FileNotFoundError(REFLIM_PATH)
+        lib = C.CDLL(REFLIM_PATH)
+        lib.reflim_last_error.restype = C.c_char_p
+        lib.reflim_create.restype = C.c_void_p
+        lib.reflim_create.argtypes = [C.c_int, C.c_int, _dp, _dp, _ip, _ip, _dp]
+        lib.reflim_destroy.argtypes = [C.c_void_p]
+        lib.reflim_add_bc.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
+        lib.reflim_add_bc.restype = C.c_int
+        lib.reflim_apply_bc.argtypes = [C.c_void_p, C.c_char_p, _dp, _dp, _dp, C.c_int, _dp]
+        lib.reflim_apply_bc.restype = C.c_int
+        lib.reflim_set_limiter.argtypes = [C.c_void_p, C.c_char_p]
+        lib.reflim_set_limiter.restype = C.c_int
+        lib.reflim_limit.argtypes = [C.c_void_p, _dp, _dp]
+        lib.reflim_limit.restype = C.c_int
+        self.lib = lib
+        x, y = o.node_coords()
+        self._keep = (np.ascontiguousarray(x), np.ascontiguousarray(y),
+                      np.ascontiguousarray(o.connectivity(), dtype=np.int32), o.fmask(), o.operator(7))
+        x, y, conn, fm, mass = self._keep
+        self.K, self.Np = x.shape
+        self.h = lib.reflim_create(int(self.K), int(o.N), _p(x), _p(y), _p(conn, _ip), _p(fm, _ip), _p(mass))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.reflim_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REFLIM_PATH)
+
+    @staticmethod
+    def _block(name: str, params: dict) -> bytes:
+        body = "".join(f"  {k} = {v}\n" for k, v in params.items())
+        return f"<{name}>\n{body}</{name}>\n".encode()
+
+    def add_bc(self, name: str, kind: str, **params) -> None:
+        """Register Apollo's boundary condition of `kind` under `name`."""
+        if self.lib.reflim_add_bc(self.h, kind.encode(), self._block(name, params)) != 0:
+            raise RuntimeError(self.lib.reflim_last_error().decode())
+
+    def apply_bc(self, name: str, xc, nx, q):
+        xc5 = np.zeros(5)
+        xc5[:len(xc)] = xc
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        qb = np.zeros(max(len(q), 8))
+        if self.lib.reflim_apply_bc(self.h, name.encode(), _p(xc5), _p(np.array(nx, dtype=np.float64)), _p(q),
+                                    len(q), _p(qb)) != 0:
+            raise RuntimeError(self.lib.reflim_last_error().decode())
+        return qb[:len(q)]
+
+    def set_limiter(self, boundary_conditions, gas_gamma: float, min_pressure: float, min_density: float) -> None:
+        """eulerLimiterHW with the named boundary conditions in tag order."""
+        text = self._block("eulerLimit", {"Kind": "eulerLimiterHW", "gas_gamma": gas_gamma,
+                                          "min_pressure": min_pressure, "min_density": min_density,
+                                          "boundaryConditions": "[" + ", ".join(boundary_conditions) + "]"})
+        if self.lib.reflim_set_limiter(self.h, text) != 0:
+            raise RuntimeError(self.lib.reflim_last_error().decode())
+
+    def limit(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.empty_like(u)
+        if self.lib.reflim_limit(self.h, _p(u), _p(out)) != 0:
+            raise RuntimeError(self.lib.reflim_last_error().decode())
         return out

@@ -46,3 +46,49 @@ def is_lf(name):
 
 
 LF_NAMES = [n for n in NAMES if is_lf(n)]
+
+
+def channel_mesh(n, seed, rotate_seed=None):
+    """[0,2] x [0,1] channel: bottom wall (tag 1), right outflow (2), top
+    inflow (3), left Dirichlet (4).  With ``rotate_seed`` each element's
+    vertex list is rotated by a random shift (orientation kept, face tags
+    follow), so boundary faces sit in every face slot, after interior faces
+    too."""
+    from apollo_b200.mesh import jittered_square
+    mesh = jittered_square(n, (0.0, 0.0), (2.0, 1.0), seed=seed, periodic=False, wall_tag=1)
+    for f, (i, j) in enumerate(((0, 1), (1, 2), (2, 0))):
+        xa, ya = mesh.vx[mesh.etov[:, i]], mesh.vy[mesh.etov[:, i]]
+        xb, yb = mesh.vx[mesh.etov[:, j]], mesh.vy[mesh.etov[:, j]]
+        mesh.face_tag[:, f] = np.select([(ya == 0) & (yb == 0), (xa == 2) & (xb == 2), (ya == 1) & (yb == 1),
+                                         (xa == 0) & (xb == 0)], [1, 2, 3, 4], 0)
+    if rotate_seed is not None:
+        shift = np.random.default_rng(rotate_seed).integers(0, 3, mesh.K)
+        idx = (np.arange(3)[None, :] + shift[:, None]) % 3
+        mesh.etov = np.ascontiguousarray(np.take_along_axis(mesh.etov, idx, axis=1))
+        mesh.face_tag = np.ascontiguousarray(np.take_along_axis(mesh.face_tag, idx, axis=1))
+    return mesh
+
+
+CHANNEL_INFLOW = (0.4, -60.0, 1.4, 1.0, 1.0)      # Mach_number, Flow_angle, gas_gamma, Pressure, density
+CHANNEL_DIRICHLET = (1.0, 0.5, 0.0, 0.0, 1.4, 1.0)  # density, x/y/zvelocity, gas_gamma, pressure
+
+
+def channel_state(x, y, rough=0.0, seed=0):
+    """Euler channel state (5 fields): density bump, transverse velocity wave,
+    pressure variation, with a relative random perturbation ``rough``."""
+    rho = 1.0 + 0.3 * np.exp(-((x - 1.0) ** 2 + (y - 0.5) ** 2) / 0.05)
+    u, v, p = 0.5 + 0 * x, 0.2 * np.sin(np.pi * x), 1.0 + 0.5 * np.cos(2 * np.pi * y)
+    U = np.stack([rho, rho * u, rho * v, 0 * x, p / 0.4 + 0.5 * rho * (u * u + v * v)], axis=-1)
+    if rough:
+        rng = np.random.default_rng(seed)
+        U = U * (1.0 + rough * rng.standard_normal(U.shape))
+        U[..., 3] = 0.3 * rough * rng.standard_normal(x.shape)
+    return np.ascontiguousarray(U)
+
+
+def boundary_after_interior(conn, N):
+    """Elements whose boundary face at a position the Euler limiters read
+    comes after an interior face (the faces whose ghost nodes Apollo takes
+    from the last neighbour read): face 1 at order 2, face 2 at orders 3-4."""
+    used = 1 if N == 2 else 2
+    return int(sum(1 for c in conn if c[2 * used] < 0 and any(c[2 * j] >= 0 for j in range(used))))

@@ -304,3 +304,38 @@ def test_averaging_weights_and_vtu(tmp_path):
     s.write_vtu(str(tmp_path / "s.vtu"), time=0.0)
     a = read_vtu(str(tmp_path / "s.vtu"))
     np.testing.assert_array_equal(a["solution"], g["U0"].reshape(g["U0"].shape[0], -1))
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+@pytest.mark.parametrize("kind", ["eulerLimiterHW", "tuAliabadiLimiter"])
+def test_limiter_boundary_face_after_interior_face(N, kind):
+    """Apollo's Euler limiters give a boundary face listed after an interior
+    face the ghost nodes of the neighbour they read last.  On a channel whose
+    elements list their faces in every order (every boundary kind), the B200
+    limiter does the same: the right-hand side of the limited state equals the
+    oracle's to 1e-12, for smooth and rough states."""
+    from oracle import oracle as orc
+    from golden_cases import (CHANNEL_DIRICHLET, CHANNEL_INFLOW, boundary_after_interior, channel_mesh,
+                              channel_state)
+    mesh = channel_mesh(7, seed=N, rotate_seed=10 + N)
+    floors = (1e-6, 1e-6)
+    bcs = (("eulerWallBC", ()), ("eulerZeroGradientBC", ()), ("eulerInflowBC", CHANNEL_INFLOW),
+           ("eulerDirichletBC", CHANNEL_DIRICHLET))
+    obcs = ((orc.BC_EULER_WALL, ()), (orc.BC_EULER_ZEROGRAD, ()), (orc.BC_EULER_INFLOW, CHANNEL_INFLOW),
+            (orc.BC_EULER_DIRICHLET, CHANNEL_DIRICHLET))
+    eqp = (1.4,) + (floors if kind == "tuAliabadiLimiter" else (0.0, 0.0))
+    s = NodalDG2d(N, 0.5, "eulerEqn", eqp, mesh, bcs=bcs, numerical_flux="HLL")
+    o = orc.Oracle(mesh, N, orc.EQ_EULER, eqp + (orc.NF_HLL,), bcs=obcs)
+    assert boundary_after_interior(o.connectivity(), N) > 0
+    if kind == "eulerLimiterHW":
+        s.set_limiter(kind, (1.4,) + floors)
+        o.set_limiter(1.4, *floors)
+    else:
+        s.set_limiter(kind)
+        o.set_limiter_ta()
+    x, y = o.node_coords()
+    for U in (channel_state(x, y), channel_state(x, y, rough=0.15, seed=N)):
+        got, _ = s.step(0.2, 0.0, U)
+        want, _ = o.rhs(o.limit(U), 0.2, 0.0)
+        assert o.error == 0
+        assert rel_l2(got, want) <= 1e-12

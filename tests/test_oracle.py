@@ -4,7 +4,8 @@ import pytest
 
 from apollo_b200 import problems
 from apollo_b200.mesh import jittered_square
-from golden_cases import NAMES, load, rel_l2
+from golden_cases import (CHANNEL_DIRICHLET, CHANNEL_INFLOW, NAMES, boundary_after_interior, channel_mesh,
+                          channel_state, load, rel_l2)
 
 
 def _ref(orc):
@@ -293,3 +294,91 @@ def test_tu_aliabadi_equals_hw_without_floors(oracle_lib):
     la, lb = a.limit(g["U0"]), b.limit(g["U0"])
     assert not np.array_equal(la, g["U0"])
     np.testing.assert_array_equal(la, lb)
+
+
+def _reflim(orc, o):
+    if not orc.RefLimiter.available():
+        pytest.skip("Apollo reference limiter not built here")
+    return orc.RefLimiter(o)
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+def test_euler_limiter_hw_bitexact_vs_reference(oracle_lib, N):
+    """The oracle's eulerLimiterHW restatement equals Apollo's limiter code
+    (wxhesthavenwarburtoneulerlimiter.cc, compiled unmodified with its four
+    Euler boundary-condition plugins) bit for bit, on a channel with every
+    boundary kind whose elements list their faces in every order (a boundary
+    face after an interior one takes its ghost nodes from the neighbour Apollo
+    read last), for smooth and rough states and with floors high enough that
+    the density and pressure fix-ups run."""
+    orc = oracle_lib
+    mesh = channel_mesh(7, seed=N, rotate_seed=10 + N)
+    bcs = ((orc.BC_EULER_WALL, ()), (orc.BC_EULER_ZEROGRAD, ()), (orc.BC_EULER_INFLOW, CHANNEL_INFLOW),
+           (orc.BC_EULER_DIRICHLET, CHANNEL_DIRICHLET))
+    o = orc.Oracle(mesh, N, orc.EQ_EULER, (1.4, 0.0, 0.0, orc.NF_HLL), bcs=bcs)
+    assert boundary_after_interior(o.connectivity(), N) > 0
+    r = _reflim(orc, o)
+    r.add_bc("wall", "eulerWallBC")
+    r.add_bc("outflow", "eulerZeroGradientBC")
+    r.add_bc("inflow", "eulerInflowBC", **dict(zip(("Mach_number", "Flow_angle", "gas_gamma", "Pressure", "density"),
+                                                  CHANNEL_INFLOW)))
+    r.add_bc("left", "eulerDirichletBC", **dict(zip(("density", "xvelocity", "yvelocity", "zvelocity", "gas_gamma",
+                                                     "pressure"), CHANNEL_DIRICHLET)))
+    x, y = o.node_coords()
+    smooth, rough = channel_state(x, y), channel_state(x, y, rough=0.15, seed=40 + N)
+    fired = False
+    for floors in ((1e-6, 1e-6), (1.2, 1.05)):
+        o.set_limiter(1.4, *floors)
+        r.set_limiter(["wall", "outflow", "inflow", "left"], 1.4, *floors)
+        for U in (smooth, rough):
+            a, b = o.limit(U), r.limit(U)
+            np.testing.assert_array_equal(a, b)
+            if floors[0] > 1:
+                o.set_limiter(1.4, 1e-6, 1e-6)
+                fired |= not np.array_equal(a, o.limit(U))
+                o.set_limiter(1.4, *floors)
+    assert fired  # the high floors changed the reconstruction
+
+
+def test_boundary_conditions_bitexact_vs_reference(oracle_lib):
+    """Each boundary condition restated in the oracle equals Apollo's plugin
+    (compiled unmodified) at random points, times, normals and states:
+    gridFixedBC, isentropicVortexBC, the four Euler conditions,
+    maxwellTransverseMagneticBC and phmConductingWallBC."""
+    orc = oracle_lib
+    rng = np.random.default_rng(77)
+    mesh = jittered_square(5, periodic=False)
+    vortex = (1.0, 0.3, 5.0, 4.0, 1.4, 5.0)
+    inflow = (0.8, 30.0, 1.4, 1.0, 1.2)
+    dirichlet = (0.9, 0.5, -0.2, 0.1, 1.4, 0.8)
+    cases = [  # oracle equation, its bcs, Apollo kind per tag with its keys
+        (orc.EQ_ADVECTION, (1.0, 0.5, 0.0), ((orc.BC_FIXED, (0.75,)),), [("gridFixedBC", dict(value=0.75))], 1),
+        (orc.EQ_EULER, (1.4, 0.0, 0.0),
+         ((orc.BC_VORTEX, vortex), (orc.BC_EULER_WALL, ()), (orc.BC_EULER_INFLOW, inflow),
+          (orc.BC_EULER_ZEROGRAD, ()), (orc.BC_EULER_DIRICHLET, dirichlet)),
+         [("isentropicVortexBC", dict(zip(("u0", "v0", "x0", "y0", "gas_gamma", "beta"), vortex))),
+          ("eulerWallBC", {}),
+          ("eulerInflowBC", dict(zip(("Mach_number", "Flow_angle", "gas_gamma", "Pressure", "density"), inflow))),
+          ("eulerZeroGradientBC", {}),
+          ("eulerDirichletBC", dict(zip(("density", "xvelocity", "yvelocity", "zvelocity", "gas_gamma", "pressure"),
+                                        dirichlet)))], 5),
+        (orc.EQ_MAXWELL, (1.0, 1.0, 1.0), ((orc.BC_TM, ()), (orc.BC_PEC, ())),
+         [("maxwellTransverseMagneticBC", {}), ("phmConductingWallBC", {})], 8),
+    ]
+    for eq, eqp, bcs, kinds, m in cases:
+        o = orc.Oracle(mesh, 3, eq, eqp, bcs=bcs)
+        r = _reflim(orc, o)
+        for tag, (kind, keys) in enumerate(kinds, start=1):
+            r.add_bc(f"bc{tag}", kind, **keys)
+            for _ in range(50):
+                xc = (rng.uniform(0, 2), rng.uniform(0, 10), rng.uniform(0, 10))
+                th = rng.uniform(0, 2 * np.pi)
+                nx = (np.cos(th), np.sin(th))
+                q = rng.uniform(-1, 1, m)
+                if m == 5:
+                    q[0] = rng.uniform(0.5, 2.0)
+                    q[4] = 0.5 * (q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0] + rng.uniform(1.0, 3.0)
+                a, b = o.apply_bc(tag, xc, nx, q), r.apply_bc(f"bc{tag}", xc, nx, q)
+                if kind == "gridFixedBC":  # Apollo writes the one advected field only
+                    a, b = a[:1], b[:1]
+                np.testing.assert_array_equal(a, b, err_msg=kind)
