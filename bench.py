@@ -68,6 +68,8 @@ def parse():
                     help="profiling driver: set up the workload, run this many RHS evaluations, exit")
     ap.add_argument("--steps-only", type=int, default=0,
                     help="profiling driver: set up the workload, advance this many SSPRK steps, exit")
+    ap.add_argument("--vjp-only", type=int, default=0,
+                    help="profiling driver: set up the workload, evaluate this many adjoint right-hand sides, exit")
     ap.add_argument("--fp64-kernels", type=int, default=0, choices=[0, 1, 2],
                     help="profiling drivers: the float64 stage form (0 three kernels, 1 fused, 2 by mesh size)")
     return ap.parse_args()
@@ -89,6 +91,25 @@ def rhs_only(args):
     torch.cuda.synchronize()
     print(json.dumps({"rhs_only": args.rhs_only, "K": s.K, "precision": prec,
                       "checksum": float(out.abs().sum().item())}))
+    s.close()
+    return 0
+
+
+def vjp_only(args):
+    """Set up the benchmark workload and evaluate the adjoint of its right-hand
+    side a few times (for ncu: the discrete adjoint's stage kernels)."""
+    import torch
+    from apollo_b200 import NodalDG2d, problems
+    p = problems.euler_vortex(n=args.n, N=args.order, fields=4)
+    s = NodalDG2d(p.N, p.cfl, p.equation, p.eq_params, p.mesh, device=0)
+    x, y = s.node_coords()
+    u = torch.from_numpy(np.ascontiguousarray(p.ic(x, y))).cuda()
+    w = torch.from_numpy(np.random.default_rng(0).standard_normal(u.shape)).cuda()
+    out = torch.empty_like(u)
+    for _ in range(args.vjp_only):
+        s.rhs_vjp(0.0, u, w, out)
+    torch.cuda.synchronize()
+    print(json.dumps({"vjp_only": args.vjp_only, "K": s.K, "checksum": float(out.abs().sum().item())}))
     s.close()
     return 0
 
@@ -1081,6 +1102,8 @@ def main():
     args = parse()
     if args.rhs_only:
         return rhs_only(args)
+    if args.vjp_only:
+        return vjp_only(args)
     if args.steps_only:
         return steps_only(args)
     if args.impl == "reference":
