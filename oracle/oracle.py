@@ -380,13 +380,13 @@ class RefLimiter:
         lib = C.CDLL(REFLIM_PATH)
         lib.reflim_last_error.restype = C.c_char_p
         lib.reflim_create.restype = C.c_void_p
-        lib.reflim_create.argtypes = [C.c_int, C.c_int, _dp, _dp, _ip, _ip, _dp]
+        lib.reflim_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _ip, _ip, _dp]
         lib.reflim_destroy.argtypes = [C.c_void_p]
         lib.reflim_add_bc.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
         lib.reflim_add_bc.restype = C.c_int
         lib.reflim_apply_bc.argtypes = [C.c_void_p, C.c_char_p, _dp, _dp, _dp, C.c_int, _dp]
         lib.reflim_apply_bc.restype = C.c_int
-        lib.reflim_set_limiter.argtypes = [C.c_void_p, C.c_char_p]
+        lib.reflim_set_limiter.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
         lib.reflim_set_limiter.restype = C.c_int
         lib.reflim_limit.argtypes = [C.c_void_p, _dp, _dp]
         lib.reflim_limit.restype = C.c_int
@@ -396,7 +396,8 @@ class RefLimiter:
                       np.ascontiguousarray(o.connectivity(), dtype=np.int32), o.fmask(), o.operator(7))
         x, y, conn, fm, mass = self._keep
         self.K, self.Np = x.shape
-        self.h = lib.reflim_create(int(self.K), int(o.N), _p(x), _p(y), _p(conn, _ip), _p(fm, _ip), _p(mass))
+        self.h = lib.reflim_create(int(self.K), int(o.N), int(o.lib.orc_meqn(o.h)), _p(x), _p(y), _p(conn, _ip),
+                                   _p(fm, _ip), _p(mass))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -432,7 +433,16 @@ class RefLimiter:
         text = self._block("eulerLimit", {"Kind": "eulerLimiterHW", "gas_gamma": gas_gamma,
                                           "min_pressure": min_pressure, "min_density": min_density,
                                           "boundaryConditions": "[" + ", ".join(boundary_conditions) + "]"})
-        if self.lib.reflim_set_limiter(self.h, text) != 0:
+        if self.lib.reflim_set_limiter(self.h, 0, text) != 0:
+            raise RuntimeError(self.lib.reflim_last_error().decode())
+
+    def set_limiter_ta(self, boundary_conditions, equation: str, **params) -> None:
+        """tuAliabadiLimiter with the named boundary conditions in tag order,
+        over Apollo's equation `equation` with its own keys."""
+        eq = "".join(f"  {k} = {v}\n" for k, v in params.items())
+        text = (f"<taLimit>\n  Kind = tuAliabadiLimiter\n  boundaryConditions = [{', '.join(boundary_conditions)}]\n"
+                f"  Equations = [eq]\n <eq>\n  Kind = {equation}\n{eq} </eq>\n</taLimit>\n").encode()
+        if self.lib.reflim_set_limiter(self.h, 1, text) != 0:
             raise RuntimeError(self.lib.reflim_last_error().decode())
 
     def limit(self, u):

@@ -1,10 +1,11 @@
-// ORACLE — test infrastructure only.  Runs Apollo's own Euler limiter
-// `eulerLimiterHW` (src/hyperapps/euler/wxhesthavenwarburtoneulerlimiter.cc)
-// and its grid boundary-condition plugins, compiled unmodified from the Apollo
-// source tree by `oracle/Makefile reflim` into oracle/_ref/libapollo_reflim.so,
-// so that tests can check the oracle's restatements of both against Apollo's
-// code:
-//   eulerLimiterHW                 wxhesthavenwarburtoneulerlimiter.cc:62-485
+// ORACLE — test infrastructure only.  Runs Apollo's own limiters and grid
+// boundary-condition plugins, compiled unmodified from the Apollo source tree
+// by `oracle/Makefile reflim` into oracle/_ref/libapollo_reflim.so, so that
+// tests can check the oracle's restatements against Apollo's code:
+//   eulerLimiterHW                 src/hyperapps/euler/wxhesthavenwarburtoneulerlimiter.cc:62-485
+//   tuAliabadiLimiter              src/hyperapps/multifluid/aptualiabadilimiter.cc:75-425
+//     (with the eulerEqn and phMaxwellEqn plugins it takes its primitive
+//     variables and reconstruction from)
 //   gridFixedBC                    src/hyperapps/advection/wxgridfixedbc.cc
 //   isentropicVortexBC             src/hyperapps/euler/wxisentropicvortexbc.cc
 //   eulerWallBC, eulerInflowBC, eulerZeroGradientBC, eulerDirichletBC
@@ -16,7 +17,7 @@
 //
 // What this file supplies in place of PETSc and of Apollo's PETSc-bound code:
 //   * the DM and Vec calls the limiter makes (declared in solver_stub/petsc.h),
-//     over one array of K elements x Np nodes x 5 fields with no ghost cells
+//     over one array of K elements x Np nodes x the fields, with no ghost cells
 //     (DMPlexGetHybridBounds returns K, where Apollo's ghost cells start);
 //   * the out-of-line members of wxNodalDGgeometry2D that the limiter calls.
 //     Apollo builds that object from a DMPlex with PETSc matrices
@@ -28,7 +29,8 @@
 //     Apollo's header code;
 //   * the members of ApSolver that the limiter reaches through getParent():
 //     getSubSolver (the same lookup as apsolver.cc:160-169) over the boundary
-//     conditions this harness registered.
+//     conditions this harness registered;
+//   * the PETSc vector norm that tuAliabadiLimiter's unused NaN check names.
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -51,10 +53,21 @@
 #include "euler/wxisentropicvortexbc.h"
 #include "maxwell/wxmaxwelltranversemagneticbc.h"
 #include "maxwell/wxphmaxwellconductingwallbc.h"
+#include "multifluid/aptualiabadilimiter.h"
+#include <wxcreator.h>
+#include "advection/wxadvectioneqn.h"
+#include "euler/wxeulereqn.h"
+#include "maxwell/wxphmaxwelleqn.h"
+
+// The equation kinds under their Apollo names, as aphyperapps_register.cc
+// registers them, for tuAliabadiLimiter's equation set.
+static WxCreator<WxAdvectionEqn<double>, WxHyperbolicEqn<double> > reg_adv("advectionEqn");
+static WxCreator<WxEulerEqn<double>, WxHyperbolicEqn<double> > reg_euler("eulerEqn");
+static WxCreator<WxPHMaxwellEqn<double>, WxHyperbolicEqn<double> > reg_maxwell("phMaxwellEqn");
 
 // ---------------------------------------------------------------- DM, Vec ----
 struct _p_DM {
-  int K = 0, N = 0, Np = 0, dof = 0;  // dof per element: Np nodes x 5 fields
+  int K = 0, N = 0, Np = 0, dof = 0;  // dof per element: Np nodes x the fields
   std::vector<double> x, y, mass;      // [K][Np], [K][Np], [Np][Np]
   std::vector<int> conn, fmask;        // [K][6], [3 (N+1)]
 };
@@ -117,6 +130,14 @@ PetscErrorCode VecDestroy(Vec* v) {
   *v = nullptr;
   return 0;
 }
+PetscErrorCode VecNormBegin(Vec v, NormType type, PetscReal* norm) {
+  double acc = 0.0;
+  for (size_t i = 0; i < v->a.size(); ++i) acc += type == NORM_1 ? std::fabs(v->a[i]) : v->a[i] * v->a[i];
+  *norm = type == NORM_1 ? acc : std::sqrt(acc);
+  return 0;
+}
+PetscErrorCode VecNormEnd(Vec, NormType, PetscReal*) { return 0; }
+int PetscIsInfOrNanReal(PetscReal v) { return std::isnan(v) || std::isinf(v); }
 // The harness owns its DM; the limiter's destructor only lets go of it.
 PetscErrorCode DMDestroy(DM* dm) {
   *dm = nullptr;
@@ -281,25 +302,26 @@ ApSubSolver<double>* make_bc(const std::string& kind) {
 extern "C" {
 const char* reflim_last_error() { return g_err.c_str(); }
 
-// A mesh of K elements at order N: node coordinates x, y [K][Np], the
-// element-to-element-to-face table conn [K][6] in Apollo's _ETETF convention
-// (neighbour and its face, or -tag twice on a boundary face), the face masks
-// fmask [3 (N+1)] and the reference element's mass matrix [Np][Np].
-void* reflim_create(int K, int N, const double* x, const double* y, const int* conn, const int* fmask,
+// A mesh of K elements at order N with meqn fields per node: node coordinates
+// x, y [K][Np], the element-to-element-to-face table conn [K][6] in Apollo's
+// _ETETF convention (neighbour and its face, or -tag twice on a boundary
+// face), the face masks fmask [3 (N+1)] and the reference element's mass
+// matrix [Np][Np].
+void* reflim_create(int K, int N, int meqn, const double* x, const double* y, const int* conn, const int* fmask,
                     const double* mass) {
   Harness* h = new Harness();
   const int Np = (N + 1) * (N + 2) / 2;
   h->dm.K = K;
   h->dm.N = N;
   h->dm.Np = Np;
-  h->dm.dof = Np * 5;
+  h->dm.dof = Np * meqn;
   h->dm.x.assign(x, x + (size_t)K * Np);
   h->dm.y.assign(y, y + (size_t)K * Np);
   h->dm.conn.assign(conn, conn + (size_t)K * 6);
   h->dm.fmask.assign(fmask, fmask + 3 * (N + 1));
   h->dm.mass.assign(mass, mass + (size_t)Np * Np);
   h->solver = new ApSolver<double>("harness");
-  h->geom = new wxNodalDGgeometry2D<double>(&h->dm, 5, (unsigned)N);
+  h->geom = new wxNodalDGgeometry2D<double>(&h->dm, (unsigned)meqn, (unsigned)N);
   return h;
 }
 
@@ -347,14 +369,18 @@ int reflim_apply_bc(void* p, const char* name, const double* xc, const double* n
   return 0;
 }
 
-// eulerLimiterHW set up from its cryptset block (gas_gamma, min_pressure,
-// min_density, boundaryConditions naming registered conditions in tag order).
-int reflim_set_limiter(void* p, const char* text) {
+// A limiter set up from its cryptset block: kind 0 eulerLimiterHW
+// (gas_gamma, min_pressure, min_density, boundaryConditions naming registered
+// conditions in tag order), kind 1 tuAliabadiLimiter (boundaryConditions and
+// the `Equations` list with the equations' own sets).
+int reflim_set_limiter(void* p, int kind, const char* text) {
   Harness* h = (Harness*)p;
   try {
     std::istringstream in(text);
     WxCryptSet wxc(in);
-    WxHestavenWarburtonEulerLimiter<double>* lim = new WxHestavenWarburtonEulerLimiter<double>();
+    WxNodalDGLimiter<double>* lim;
+    if (kind == 0) lim = new WxHestavenWarburtonEulerLimiter<double>();
+    else lim = new WxTuAliabadiLimiter<double>();
     ApSubSolver<double>* base = lim;
     base->setup(wxc, &h->dm);
     lim->setParent(h->solver);
@@ -367,7 +393,7 @@ int reflim_set_limiter(void* p, const char* text) {
   return 0;
 }
 
-// Apollo's limiter on u [K][Np][5] into out (WxNodalDGLimiter::applyToVector).
+// Apollo's limiter on u [K][Np][meqn] into out (WxNodalDGLimiter::applyToVector).
 int reflim_limit(void* p, const double* u, double* out) {
   Harness* h = (Harness*)p;
   if (!h->limiter) return -1;

@@ -25,4 +25,8 @@ PetscErrorCode VecGetArray(Vec, PetscScalar**);
 PetscErrorCode VecRestoreArray(Vec, PetscScalar**);
 PetscErrorCode VecDestroy(Vec*);
 PetscErrorCode DMDestroy(DM*);
+typedef enum { NORM_1 = 0, NORM_2 = 1 } NormType;
+PetscErrorCode VecNormBegin(Vec, NormType, PetscReal*);
+PetscErrorCode VecNormEnd(Vec, NormType, PetscReal*);
+int PetscIsInfOrNanReal(PetscReal);
 #endif

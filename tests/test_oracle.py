@@ -382,3 +382,41 @@ def test_boundary_conditions_bitexact_vs_reference(oracle_lib):
                 if kind == "gridFixedBC":  # Apollo writes the one advected field only
                     a, b = a[:1], b[:1]
                 np.testing.assert_array_equal(a, b, err_msg=kind)
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+def test_tu_aliabadi_limiter_bitexact_vs_reference(oracle_lib, N):
+    """The oracle's tuAliabadiLimiter restatement equals Apollo's limiter code
+    (aptualiabadilimiter.cc over the eulerEqn and phMaxwellEqn plugins,
+    compiled unmodified) bit for bit: the Euler channel with every boundary
+    kind and faces in every order, with the equation's floors low and high,
+    and the Maxwell TM cavity with its walls."""
+    orc = oracle_lib
+    mesh = channel_mesh(7, seed=N, rotate_seed=20 + N)
+    bcs = ((orc.BC_EULER_WALL, ()), (orc.BC_EULER_ZEROGRAD, ()), (orc.BC_EULER_INFLOW, CHANNEL_INFLOW),
+           (orc.BC_EULER_DIRICHLET, CHANNEL_DIRICHLET))
+    names = ["wall", "outflow", "inflow", "left"]
+    for floors in ((1e-6, 1e-6), (1.2, 1.05)):
+        o = orc.Oracle(mesh, N, orc.EQ_EULER, (1.4,) + floors + (orc.NF_HLL,), bcs=bcs)
+        assert boundary_after_interior(o.connectivity(), N) > 0
+        o.set_limiter_ta()
+        r = _reflim(orc, o)
+        r.add_bc("wall", "eulerWallBC")
+        r.add_bc("outflow", "eulerZeroGradientBC")
+        r.add_bc("inflow", "eulerInflowBC", **dict(zip(("Mach_number", "Flow_angle", "gas_gamma", "Pressure",
+                                                        "density"), CHANNEL_INFLOW)))
+        r.add_bc("left", "eulerDirichletBC", **dict(zip(("density", "xvelocity", "yvelocity", "zvelocity",
+                                                         "gas_gamma", "pressure"), CHANNEL_DIRICHLET)))
+        r.set_limiter_ta(names, "eulerEqn", gas_gamma=1.4, minPressure=floors[0], minDensity=floors[1])
+        x, y = o.node_coords()
+        for U in (channel_state(x, y), channel_state(x, y, rough=0.15, seed=50 + N)):
+            np.testing.assert_array_equal(o.limit(U), r.limit(U))
+    p = problems.maxwell_tm(n=6, N=N, fields=8, seed=N)
+    o = orc.Oracle(p.mesh, N, orc.EQ_MAXWELL, (1.0, 0.0, 0.0), bcs=((orc.BC_TM, ()),))
+    o.set_limiter_ta()
+    r = _reflim(orc, o)
+    r.add_bc("walls", "maxwellTransverseMagneticBC")
+    r.set_limiter_ta(["walls"], "phMaxwellEqn", c0=1.0)
+    x, y = o.node_coords()
+    U = np.ascontiguousarray(p.ic(x, y)) + 0.1 * np.random.default_rng(N).standard_normal((p.mesh.K, x.shape[1], 8))
+    np.testing.assert_array_equal(o.limit(U), r.limit(U))
