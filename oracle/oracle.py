@@ -8,6 +8,10 @@
 * ``RefLimiter``  — Apollo's own eulerLimiterHW and grid boundary conditions
                     compiled unmodified (ref_limiter.cpp, built to
                     _ref/libapollo_reflim.so where the Apollo source tree exists).
+* ``RefDriver``   — Apollo's own nodal-DG right-hand side with its geometry
+                    and cubature code compiled unmodified (ref_driver.cpp, built
+                    to _ref/libapollo_refdrv.so where the Apollo source tree
+                    exists).
 
 Only tests, ``__graft_entry__.smoke`` and the CPU-baseline leg of ``bench.py``
 import this module.
@@ -24,6 +28,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libapollo_ref.so")
 REFLIM_PATH = os.path.join(HERE, "_ref", "libapollo_reflim.so")
+REFDRV_PATH = os.path.join(HERE, "_ref", "libapollo_refdrv.so")
 
 EQ_ADVECTION, EQ_EULER, EQ_MAXWELL = 0, 1, 2
 # source plugins (Apollo kind names tranverseMagneticSrc, pointCurrentSrc)
@@ -59,7 +64,7 @@ def build(with_ref: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     src = reference_src()
     if with_ref and os.path.isdir(src):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "reflim", f"APOLLO_SRC={src}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "reflim", "refdrv", f"APOLLO_SRC={src}"], check=True)
 
 
 def _lib():
@@ -451,3 +456,91 @@ class RefLimiter:
         if self.lib.reflim_limit(self.h, _p(u), _p(out)) != 0:
             raise RuntimeError(self.lib.reflim_last_error().decode())
         return out
+
+
+class RefDriver:
+    """Apollo's own nodal-DG right-hand side (WxNodalDG2dMethod with its
+    geometry, cubature, equation, source and boundary-condition code,
+    compiled unmodified) on a triangle mesh through a minimal stand-in for
+    PETSc's mesh, vector and dense-matrix calls."""
+
+    def __init__(self, mesh):
+        if not os.path.exists(REFDRV_PATH):
+            raise FileNotFoundError(REFDRV_PATH)
+        lib = C.CDLL(REFDRV_PATH)
+        lib.refdrv_last_error.restype = C.c_char_p
+        lib.refdrv_create.restype = C.c_void_p
+        lib.refdrv_create.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, _ip]
+        lib.refdrv_destroy.argtypes = [C.c_void_p]
+        lib.refdrv_add_bc.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
+        lib.refdrv_add_bc.restype = C.c_int
+        lib.refdrv_add_limiter.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+        lib.refdrv_add_limiter.restype = C.c_int
+        lib.refdrv_setup.argtypes = [C.c_void_p, C.c_char_p]
+        lib.refdrv_setup.restype = C.c_int
+        for name in ("refdrv_np", "refdrv_meqn"):
+            getattr(lib, name).argtypes = [C.c_void_p]
+            getattr(lib, name).restype = C.c_int
+        lib.refdrv_init.argtypes = [C.c_void_p, C.c_double, _dp, _dp]
+        lib.refdrv_init.restype = C.c_int
+        lib.refdrv_rhs.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, _dp, _dp]
+        lib.refdrv_rhs.restype = C.c_int
+        self.lib = lib
+        self._keep = (np.ascontiguousarray(mesh.vx, dtype=np.float64), np.ascontiguousarray(mesh.vy, dtype=np.float64),
+                      np.ascontiguousarray(mesh.etov, dtype=np.int32),
+                      np.ascontiguousarray(mesh.face_tag, dtype=np.int32))
+        vx, vy, etov, tags = self._keep
+        self.K = etov.shape[0]
+        self.h = lib.refdrv_create(len(vx), _p(vx), _p(vy), self.K, _p(etov, _ip), _p(tags, _ip))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.refdrv_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REFDRV_PATH)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.refdrv_last_error().decode())
+
+    def add_bc(self, name: str, kind: str, **params) -> None:
+        body = "".join(f"  {k} = {v}\n" for k, v in params.items())
+        self._check(self.lib.refdrv_add_bc(self.h, kind.encode(), f"<{name}>\n{body}</{name}>\n".encode()))
+
+    def add_limiter(self, name: str, kind: str, boundary_conditions, **params) -> None:
+        """A limiter sub-solver (eulerLimiterHW with gas_gamma, min_pressure,
+        min_density; or tuAliabadiLimiter with an `equation` kind and its keys)
+        for the method's `Limiter = [name]`."""
+        bcs = f"  boundaryConditions = [{', '.join(boundary_conditions)}]\n"
+        if kind == "eulerLimiterHW":
+            body = bcs + "".join(f"  {k} = {v}\n" for k, v in params.items())
+            code = 0
+        else:
+            eq = params.pop("equation")
+            body = bcs + f"  Equations = [eq]\n <eq>\n  Kind = {eq}\n" + "".join(
+                f"  {k} = {v}\n" for k, v in params.items()) + " </eq>\n"
+            code = 1
+        self._check(self.lib.refdrv_add_limiter(self.h, code, f"<{name}>\n  Kind = {kind}\n{body}</{name}>\n".encode()))
+
+    def setup(self, text: str) -> None:
+        """The nodalDG2d sub-solver's cryptset block, as in an Apollo input
+        (keys before sub-sets: Apollo's cryptset reader does not see a key
+        written after a sub-set)."""
+        self._check(self.lib.refdrv_setup(self.h, text.encode()))
+        self.Np, self.meqn = self.lib.refdrv_np(self.h), self.lib.refdrv_meqn(self.h)
+
+    def init(self, t: float = 0.0):
+        u = np.zeros((self.K, self.Np, self.meqn))
+        dt = C.c_double()
+        self._check(self.lib.refdrv_init(self.h, t, _p(u), C.byref(dt)))
+        return u, dt.value
+
+    def rhs(self, u, t: float = 0.0, dt: float = 0.0):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.zeros_like(u)
+        s = C.c_double()
+        self._check(self.lib.refdrv_rhs(self.h, t, dt, _p(u), _p(out), C.byref(s)))
+        return out, s.value

@@ -27,9 +27,9 @@
 //     Normals2d / GeometricFactors2d restate wxnodaldggeometry2d.cc:384-438.
 //     The inline members (LimiterElementAVE, returnFmask, the accessors) are
 //     Apollo's header code;
-//   * the members of ApSolver that the limiter reaches through getParent():
-//     getSubSolver (the same lookup as apsolver.cc:160-169) over the boundary
-//     conditions this harness registered;
+//   * the members of ApSolver that the limiter reaches through getParent()
+//     (ref_harness.h): getSubSolver, the same lookup as apsolver.cc:160-169,
+//     over the boundary conditions this harness registered;
 //   * the PETSc vector norm that tuAliabadiLimiter's unused NaN check names.
 #include <cmath>
 #include <cstring>
@@ -39,21 +39,11 @@
 #include <vector>
 
 #include <wxcryptset.h>
-#include <wxexcept.h>
-#include <apsolver.h>
-#include <wxgridbc.h>
 #include <wxnodaldggeometry2d.h>
 #include <wxnodaldglimiter.h>
-#include "advection/wxgridfixedbc.h"
-#include "euler/wxeulerdirichletbc.h"
-#include "euler/wxeulerinflowbc.h"
-#include "euler/wxeulerwallbc.h"
-#include "euler/wxeulerzerogradientbc.h"
 #include "euler/wxhesthavenwarburtoneulerlimiter.h"
-#include "euler/wxisentropicvortexbc.h"
-#include "maxwell/wxmaxwelltranversemagneticbc.h"
-#include "maxwell/wxphmaxwellconductingwallbc.h"
 #include "multifluid/aptualiabadilimiter.h"
+#include "ref_harness.h"
 #include <wxcreator.h>
 #include "advection/wxadvectioneqn.h"
 #include "euler/wxeulereqn.h"
@@ -232,44 +222,6 @@ void wxNodalDGgeometry2D<REAL>::GeometricFactors2d(int k, REAL geom[]) {
 template class wxNodalDGgeometry2D<float>;
 template class wxNodalDGgeometry2D<double>;
 
-// --------------------------------------------------------------- solver ----
-// Boundary conditions created by this harness, handed to the solver by init().
-namespace {
-std::vector<std::pair<std::string, ApSubSolver<double>*> > g_pending;
-}
-
-template <typename REAL>
-ApSolver<REAL>::ApSolver(const std::string& name) : WxSolverBase<REAL>(name), tssolver(nullptr) {}
-template <typename REAL>
-ApSolver<REAL>::~ApSolver() {
-  for (typename SubSolverMap_t::iterator i = _subSolvers.begin(); i != _subSolvers.end(); ++i) delete i->second;
-}
-template <typename REAL>
-void ApSolver<REAL>::setup(const WxCryptSet&) {}
-template <typename REAL>
-void ApSolver<REAL>::init() {}
-template <>
-void ApSolver<double>::init() {
-  for (size_t i = 0; i < g_pending.size(); ++i) _subSolvers[g_pending[i].first] = g_pending[i].second;
-  g_pending.clear();
-}
-template <typename REAL>
-void ApSolver<REAL>::solve() {}
-template <typename REAL>
-WxStepperStatus<REAL> ApSolver<REAL>::step(REAL, REAL, Vec, Vec) {
-  return WxStepperStatus<REAL>();
-}
-template <typename REAL>
-ApSubSolver<REAL>* ApSolver<REAL>::getSubSolver(const std::string& name) {
-  typename SubSolverMap_t::iterator i = _subSolvers.find(name);
-  if (i != _subSolvers.end()) return i->second;
-  WxExcept wxe;
-  wxe << "WxSolver::getSubSolver : SubSolver " << name << " not found";
-  throw wxe;
-}
-template class ApSolver<float>;
-template class ApSolver<double>;
-
 // -------------------------------------------------------------- harness ----
 namespace {
 std::string g_err;
@@ -286,17 +238,6 @@ struct Harness {
   }
 };
 
-ApSubSolver<double>* make_bc(const std::string& kind) {
-  if (kind == "gridFixedBC") return new WxGridFixedBC<double>();
-  if (kind == "isentropicVortexBC") return new WxIsentropicVortexBC<double>();
-  if (kind == "eulerWallBC") return new WxEulerWallBC<double>();
-  if (kind == "eulerInflowBC") return new WxEulerInflowBC<double>();
-  if (kind == "eulerZeroGradientBC") return new WxEulerZeroGradientBC<double>();
-  if (kind == "eulerDirichletBC") return new WxEulerDirichletBC<double>();
-  if (kind == "maxwellTransverseMagneticBC") return new WxMaxwellTransverseMagnetic<double>();
-  if (kind == "phmConductingWallBC") return new WxPHMaxwellConductingWallBC<double>();
-  return nullptr;
-}
 }  // namespace
 
 extern "C" {

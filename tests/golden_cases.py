@@ -92,3 +92,18 @@ def boundary_after_interior(conn, N):
     from the last neighbour read): face 1 at order 2, face 2 at orders 3-4."""
     used = 1 if N == 2 else 2
     return int(sum(1 for c in conn if c[2 * used] < 0 and any(c[2 * j] >= 0 for j in range(used))))
+
+
+def one_tag_per_element(mesh):
+    """Give every boundary face of an element the tag of its first boundary
+    face.  Apollo stores one boundary tag per element (the last of its
+    boundary faces to be labelled writes all six connectivity slots,
+    wxnodaldggeometry2d.cc:348-356), this library one per face; on meshes
+    like this the two agree."""
+    ft = mesh.face_tag.copy()
+    for e in range(ft.shape[0]):
+        tags = [t for t in ft[e] if t > 0]
+        if len(set(tags)) > 1:
+            ft[e][ft[e] > 0] = tags[0]
+    mesh.face_tag = ft
+    return mesh
