@@ -107,3 +107,23 @@ def one_tag_per_element(mesh):
             ft[e][ft[e] > 0] = tags[0]
     mesh.face_tag = ft
     return mesh
+
+
+# Right-hand sides made by Apollo's own code (tests/golden/make_apollo_rhs.py)
+APOLLO_DIR = os.path.join(HERE, "apollo_rhs")
+APOLLO_NAMES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(APOLLO_DIR, "*.npz")))
+BC_KINDS = {v: k for k, v in BC_NAMES.items()}
+SRC_CODES = {"tranverseMagneticSrc": 1, "pointCurrentSrc": 2}
+
+
+def load_apollo(name):
+    z = np.load(os.path.join(APOLLO_DIR, name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    d["mesh"] = Mesh(vx=d["vx"], vy=d["vy"], etov=d["etov"], face_tag=d["face_tag"], vert_canon=d["vert_canon"],
+                     n=0, lo=(0, 0), hi=(1, 1), periodic=False)
+    d["equation"] = str(d["equation"])
+    d["numflux"] = str(d["numflux"])
+    d["bcs"] = tuple((str(n), tuple(p[:k])) for n, p, k in zip(d["bc_names"], d["bc_params"], d["bc_nparams"]))
+    d["sources"] = tuple((str(k), (2,), tuple(p[:n])) for k, p, n in
+                         zip(d["src_kinds"], d["src_params"], d["src_nparams"]))
+    return d

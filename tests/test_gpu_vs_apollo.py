@@ -1,0 +1,25 @@
+"""The B200 float64 right-hand side against right-hand sides made by Apollo's
+own code (tests/golden/apollo_rhs, written by tests/golden/make_apollo_rhs.py
+with Apollo's WxNodalDG2dMethod compiled unmodified): every Euler flux with
+the four Euler boundary conditions on elements listing their faces in every
+order, the isentropic-vortex example, the Maxwell TM cavity, the cleaned
+Maxwell form with both sources, advection.  Agreement to 1e-12 relative L2
+(1e-11 for the vortex, whose right-hand side is a small difference of O(1)
+flux terms); no restatement stands between the CUDA kernels and Apollo's code.
+"""
+import pytest
+
+from apollo_b200 import NodalDG2d
+from golden_cases import APOLLO_NAMES, load_apollo, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", APOLLO_NAMES)
+def test_rhs_matches_apollo(name):
+    g = load_apollo(name)
+    s = NodalDG2d(int(g["N"]), 0.5, g["equation"], tuple(g["eqp"]), g["mesh"], bcs=g["bcs"],
+                  numerical_flux=g["numflux"], sources=g["sources"])
+    got, sugg = s.step(float(g["t"]), float(g["dt"]), g["U"])
+    assert rel_l2(got, g["rhs"]) <= (1e-11 if "vortex" in name else 1e-12)
+    assert sugg == pytest.approx(float(g["sugg"]), rel=1e-13)

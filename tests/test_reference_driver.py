@@ -190,3 +190,21 @@ def test_limited_rhs_vs_reference(oracle_lib, kind, N):
         ro, _ = o.rhs(o.limit(U), 0.3, 0.01)
         assert o.error == 0
         assert rel_l2(rr, ro) <= 1e-12
+
+
+@pytest.mark.parametrize("name", __import__("golden_cases").APOLLO_NAMES)
+def test_oracle_reproduces_apollo_rhs_fixtures(oracle_lib, name):
+    """The committed right-hand sides made by Apollo's own code
+    (tests/golden/make_apollo_rhs.py) are reproduced by the oracle."""
+    from golden_cases import BC_KINDS, SRC_CODES, load_apollo
+    orc = oracle_lib
+    g = load_apollo(name)
+    eq = {"eulerEqn": orc.EQ_EULER, "phMaxwellEqn": orc.EQ_MAXWELL, "advectionEqn": orc.EQ_ADVECTION}[g["equation"]]
+    code = {"LF": orc.NF_LF, "HLL": orc.NF_HLL, "Roe": orc.NF_ROE, "Wave": orc.NF_WAVE}[g["numflux"]]
+    o = orc.Oracle(g["mesh"], int(g["N"]), eq, tuple(g["eqp"]) + (code,),
+                   bcs=tuple((BC_KINDS[n], p) for n, p in g["bcs"]), cfl=0.5)
+    for kind, out, params in g["sources"]:
+        o.add_source(SRC_CODES[kind], out[0], params)
+    rhs, sugg = o.rhs(g["U"], float(g["t"]), float(g["dt"]))
+    assert rel_l2(rhs, g["rhs"]) <= (1e-11 if "vortex" in name else 1e-12)
+    assert sugg == pytest.approx(float(g["sugg"]), rel=1e-14)
