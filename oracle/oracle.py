@@ -544,3 +544,52 @@ class RefDriver:
         s = C.c_double()
         self._check(self.lib.refdrv_rhs(self.h, t, dt, _p(u), _p(out), C.byref(s)))
         return out, s.value
+
+    def ssp_step(self, u, t0: float, dt: float):
+        """One SSPRK(5,2) step through Apollo's right-hand side: PETSc's TSSSP
+        `rks2` with 5 stages as documented (w = u; 4x w += dt/4 L(w) at
+        t0 + dt i/4; u = 4/5 w + dt/5 L(w) + 1/5 u), the arithmetic of the
+        oracle's orc_ssp_step.  Returns (u, suggested dt of the last stage)."""
+        w = np.array(u, dtype=np.float64, copy=True)
+        for i in range(4):
+            F, _ = self.rhs(w, t0 + dt * (i / 4.0), dt)
+            w += (dt / 4.0) * F
+        F, sugg = self.rhs(w, t0 + dt, dt)
+        return 0.8 * w + (dt / 5.0) * F + 0.2 * np.asarray(u), sugg
+
+    def run(self, u, nsteps: int, t: float, dt: float):
+        """nsteps steps with Apollo's dt policy (ApSolver::ComputeRHSforTS: the
+        next dt is the smaller of this one and the last stage's suggestion)."""
+        for _ in range(nsteps):
+            u, sugg = self.ssp_step(u, t, dt)
+            t += dt
+            dt = min(sugg, dt)
+        return u, t, dt
+
+
+# Apollo's isentropicVortex example input (examples/unstructuredDG/euler/
+# isentropicVortex/isentropicVortex.pin): the exprFunc program of its
+# initial state
+VORTEX_PROGN = ["r = sqrt((x-xo)*(x-xo)+(y-yo)*(y-yo))", "u = uo - beta*exp(1.-r*r)*(y-yo)/(2.*pi)",
+                "v = vo + beta*exp(1.-r*r)*(x-xo)/(2.*pi)",
+                "base = 1. - ( (gamma-1.)*beta*beta*exp(2.*(1.-r*r))/(16.*gamma*pi*pi) )",
+                "rho = base^(1./(gamma-1.))", "p   = rho^gamma", "en = p/(gamma-1.) + 0.5*rho*(u*u + v*v)",
+                "rhou = rho*u", "rhov = rho*v"]
+
+
+def apollo_vortex_driver(mesh, N: int, cfl: float, x0: float = 5.0, y0: float = 5.0, beta: float = 5.0,
+                         gamma: float = 1.4, u0: float = 1.0, v0: float = 0.0) -> RefDriver:
+    """Apollo's isentropicVortex example on `mesh` through Apollo's own
+    right-hand-side code: eulerEqn (Lax-Friedrichs), the exprFunc initial
+    state, isentropicVortexBC (the exact vortex) on every boundary face."""
+    r = RefDriver(mesh)
+    r.add_bc("allSides", "isentropicVortexBC", u0=u0, v0=v0, x0=x0, y0=y0, gas_gamma=gamma, beta=beta)
+    consts = "".join(f"  {k} = {v}\n" for k, v in (("xo", x0), ("yo", y0), ("beta", beta), ("gamma", gamma),
+                                                    ("uo", u0), ("vo", v0), ("pi", 3.141592653589793)))
+    progn = ", ".join(f'"{p}"' for p in VORTEX_PROGN)
+    r.setup(f"<hyperbolic>\n Kind = nodalDG2d\n Equations = [euler]\n boundaryConditions = [allSides]\n"
+            f" polynomialOrder = {N}\n cfl = {cfl!r}\n DataStructure = [0, dg, {5 * (N + 1) * (N + 2) // 2}]\n"
+            f" <InitialCondition>\n  Kind = exprFunc\n{consts}"
+            f'  exprList = ["rho", "rhou", "rhov", "0.0", "en"]\n  progn = [{progn}]\n </InitialCondition>\n'
+            f" <euler>\n  Kind = eulerEqn\n  gas_gamma = {gamma!r}\n </euler>\n</hyperbolic>\n")
+    return r

@@ -17,7 +17,8 @@
 //
 // What this file supplies in place of PETSc and MPI (declared in
 // solver_stub/petsc.h and solver_stub/mpi.h):
-//   * dense matrices with PETSc's calling conventions: products summed in
+//   * dense matrices with PETSc's calling conventions (and sparse ones for the
+//     face-to-vertex and face-to-face connectivity): products summed in
 //     index order, LU with partial pivoting and the triangular solves in the
 //     order of LAPACK's unblocked dgetf2/dgetrs (PETSc's dense LU calls
 //     LAPACK; which LAPACK Apollo links is not known, so results agree with
@@ -81,6 +82,11 @@ struct _p_Mat {
   std::vector<int> cols;    // 0 .. n-1, what MatGetRow hands out
   std::vector<double> lu;   // a factor: LU of the factored matrix, row-major
   std::vector<int> piv;     // and its row interchanges
+  // a sparse (AIJ) matrix: its rows, and the row MatGetRow last handed out
+  bool aij = false;
+  std::vector<std::map<int, double> > sp;
+  std::vector<int> rc;
+  std::vector<double> rv;
   void shape(int mm, int nn) {
     m = mm; n = nn;
     a.assign((size_t)m * n, 0.0);
@@ -98,20 +104,35 @@ PetscErrorCode MatCreateSeqDense(MPI_Comm, PetscInt m, PetscInt n, PetscScalar*,
   return 0;
 }
 PetscErrorCode MatCreateSeqAIJ(MPI_Comm, PetscInt m, PetscInt n, PetscInt, const PetscInt*, Mat* A) {
-  *A = new_mat(m, n);
+  *A = new _p_Mat();
+  (*A)->m = m;
+  (*A)->n = n;
+  (*A)->aij = true;
+  (*A)->sp.resize(m);
   return 0;
 }
 PetscErrorCode MatSetValue(Mat A, PetscInt i, PetscInt j, PetscScalar v, InsertMode mode) {
-  double& x = A->a[(size_t)i * A->n + j];
+  double& x = A->aij ? A->sp[i][j] : A->a[(size_t)i * A->n + j];
   x = mode == ADD_VALUES ? x + v : v;
   return 0;
 }
 PetscErrorCode MatAssemblyBegin(Mat, MatAssemblyType) { return 0; }
 PetscErrorCode MatAssemblyEnd(Mat, MatAssemblyType) { return 0; }
-// A dense row: every column, as PETSc's dense MatGetRow gives it (the
-// connectivity matrices Apollo builds as AIJ are searched for values of 2,
-// which the zeros never match).
+// A dense row: every column, as PETSc's dense MatGetRow gives it; a sparse
+// row: its stored entries in column order.
 PetscErrorCode MatGetRow(Mat A, PetscInt r, PetscInt* nc, const PetscInt** c, const PetscScalar** v) {
+  if (A->aij) {
+    A->rc.clear();
+    A->rv.clear();
+    for (std::map<int, double>::const_iterator it = A->sp[r].begin(); it != A->sp[r].end(); ++it) {
+      A->rc.push_back(it->first);
+      A->rv.push_back(it->second);
+    }
+    *nc = (PetscInt)A->rc.size();
+    if (c) *c = A->rc.data();
+    if (v) *v = A->rv.data();
+    return 0;
+  }
   *nc = A->n;
   if (c) *c = A->cols.data();
   if (v) *v = &A->a[(size_t)r * A->n];
@@ -131,6 +152,8 @@ PetscErrorCode MatDestroy(Mat* A) {
 PetscErrorCode MatView(Mat, PetscViewer) { return 0; }
 PetscErrorCode MatZeroEntries(Mat A) {
   std::fill(A->a.begin(), A->a.end(), 0.0);
+  for (size_t i = 0; i < A->sp.size(); ++i)
+    for (std::map<int, double>::iterator it = A->sp[i].begin(); it != A->sp[i].end(); ++it) it->second = 0.0;
   return 0;
 }
 PetscErrorCode MatTranspose(Mat A, MatReuse reuse, Mat* B) {
@@ -155,8 +178,22 @@ PetscErrorCode MatMatMult(Mat A, Mat B, MatReuse reuse, PetscReal, Mat* C) {
   matmul(A, B, false, reuse, C);
   return 0;
 }
+// Sparse A B^T (the face-to-face connectivity from face-to-vertex): the
+// pattern of every pair of rows sharing a column, as PETSc's AIJ product has it
 PetscErrorCode MatMatTransposeMult(Mat A, Mat B, MatReuse reuse, PetscReal, Mat* C) {
-  matmul(A, B, true, reuse, C);
+  if (!A->aij || !B->aij) {
+    matmul(A, B, true, reuse, C);
+    return 0;
+  }
+  std::vector<std::vector<std::pair<int, double> > > bcol(B->n);
+  for (int j = 0; j < B->m; ++j)
+    for (std::map<int, double>::const_iterator it = B->sp[j].begin(); it != B->sp[j].end(); ++it)
+      bcol[it->first].push_back(std::make_pair(j, it->second));
+  MatCreateSeqAIJ(MPI_COMM_SELF, A->m, B->m, 0, nullptr, C);
+  for (int i = 0; i < A->m; ++i)
+    for (std::map<int, double>::const_iterator it = A->sp[i].begin(); it != A->sp[i].end(); ++it)
+      for (size_t q = 0; q < bcol[it->first].size(); ++q)
+        (*C)->sp[i][bcol[it->first][q].first] += it->second * bcol[it->first][q].second;
   return 0;
 }
 PetscErrorCode MatDuplicate(Mat A, MatDuplicateOption op, Mat* B) {

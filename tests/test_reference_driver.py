@@ -208,3 +208,24 @@ def test_oracle_reproduces_apollo_rhs_fixtures(oracle_lib, name):
     rhs, sugg = o.rhs(g["U"], float(g["t"]), float(g["dt"]))
     assert rel_l2(rhs, g["rhs"]) <= (1e-11 if "vortex" in name else 1e-12)
     assert sugg == pytest.approx(float(g["sugg"]), rel=1e-14)
+
+
+def test_steps_through_apollo_rhs_match_oracle(oracle_lib):
+    """SSPRK(5,2) steps with Apollo's dt policy taken through Apollo's own
+    right-hand side (what `bench.py --impl reference` times) equal the
+    oracle's steps: the isentropicVortex example on a walled square."""
+    orc = oracle_lib
+    if not orc.RefDriver.available():
+        pytest.skip("Apollo's right-hand side is not built here")
+    mesh = jittered_square(10, (0.0, 0.0), (10.0, 10.0), seed=2, periodic=False, wall_tag=1)
+    r = orc.apollo_vortex_driver(mesh, 4, 0.5)
+    u0, dt0 = r.init(0.0)
+    o = orc.Oracle(mesh, 4, orc.EQ_EULER, (1.4, 0.0, 0.0), bcs=((orc.BC_VORTEX, (1.0, 0.0, 5.0, 5.0, 1.4, 5.0)),),
+                   cfl=0.5)
+    assert dt0 == pytest.approx(o.init_dt(u0), rel=1e-14)
+    uo = u0.copy()
+    n, to, dto = o.run(uo, 4, 0.0, dt0)
+    ur, tr, dtr = r.run(u0, 4, 0.0, dt0)
+    assert n == 4
+    assert rel_l2(ur, uo) <= 1e-12
+    assert tr == pytest.approx(to, rel=1e-14) and dtr == pytest.approx(dto, rel=1e-13)
