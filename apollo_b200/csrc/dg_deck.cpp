@@ -15,7 +15,8 @@
 // This file reads that text: blocks <name> ... </name>, "key = value" lines
 // (with '\' continuations and '#' comments), values that are numbers,
 // arithmetic over the preamble's names (+ - * / ** ^, parentheses), quoted or
-// bare strings, and [lists].  Keys keep Apollo's names and defaults.
+// bare strings, and [lists].  Keys keep Apollo's names and defaults; a key
+// written after a sub-block of its block is not read, as in Apollo.
 #include <cctype>
 #include <cmath>
 #include <cstring>
@@ -216,6 +217,11 @@ bool parse(const char* text, Deck& d) {
       double x;
       if (eval_number(v, d.defs, &x)) d.defs[k] = x;
     }
+    // Apollo's reader does not see a key written after a sub-block of the
+    // same block (each nested parse runs on its own copy of the lexer,
+    // WxCryptSet::_WxParser::wx_decl_value, src/lib/wxcryptset.cc:337-367):
+    // such a key is dropped here too, so a deck configures the same plugins
+    if (stack.size() > 1 && !stack.back()->sub.empty()) continue;
     stack.back()->kv.emplace_back(k, v);
   }
   if (stack.size() != 1) {

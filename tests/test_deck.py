@@ -127,3 +127,29 @@ def test_apollo_example_decks(deck, N, eq, flux, bcs, lim):
     assert (kind, params) == eq and nf == flux
     assert deck_bcs(text) == bcs
     assert deck_limiter(text) == lim
+
+
+def test_keys_after_a_sub_block_are_not_read_as_in_apollo(oracle_lib):
+    """Apollo's cryptset reader does not see a key written after a sub-block
+    of the same block: Numerical_Flux = HLL there leaves the Lax-Friedrichs
+    flux, and a required key there is missing.  The deck reader does the same,
+    checked against Apollo's own reader and eulerEqn plugin."""
+    import numpy as np
+    base = "<top>\n Equations = [eq]\n <eq>\n  Kind = eulerEqn\n  gas_gamma = 1.4\n{body} </eq>\n</top>\n"
+    after = base.format(body="  <sub>\n   a = 1\n  </sub>\n  Numerical_Flux = HLL\n")
+    before = base.format(body="  Numerical_Flux = HLL\n  <sub>\n   a = 1\n  </sub>\n")
+    assert deck_equation(after)[2] == "LF"
+    assert deck_equation(before)[2] == "HLL"
+    with pytest.raises(Exception, match="gas_gamma"):
+        deck_equation("<top>\n Equations = [eq]\n <eq>\n  Kind = eulerEqn\n  <sub>\n   a = 1\n  </sub>\n"
+                      "  gas_gamma = 1.4\n </eq>\n</top>\n")
+    orc = oracle_lib
+    if not orc.RefPlugins.available():
+        pytest.skip("Apollo's plugins are not built here")
+    ref = orc.RefPlugins()
+    qM, qP, n = np.array([1.0, 0.5, 0.2, 0.0, 2.5]), np.array([0.8, 0.1, -0.3, 0.0, 2.0]), np.array([0.6, 0.8])
+
+    def flux(text):
+        return ref.numflux(ref.lib.ref_eqn_create(text.encode()), n, qM.copy(), qP.copy())[0]
+    np.testing.assert_array_equal(flux(after), flux(base.format(body="")))
+    assert not np.array_equal(flux(before), flux(base.format(body="")))
