@@ -89,7 +89,9 @@ apollo_status apollo_dg_set_equation(apollo_dg* h, const char* kind, const doubl
  * Limiter naming blocks whose Kind and keys configure each plugin.  These
  * calls take that text (a whole deck, or one block) with Apollo's key names
  * and defaults; the deck's Python preamble of "NAME = expression" lines may be
- * included, and values may be arithmetic over those names.  With kind NULL
+ * included, and values may be arithmetic over those names.  As in Apollo's
+ * reader, a key written after a sub-block of its block is not read, and of a
+ * key written twice the first counts.  With kind NULL
  * the block is found through the list (or is the text's only block); with a
  * kind, the text's keys are that plugin's.  Errors: APOLLO_ERR_CONFIG with the
  * reason in err (host-only calls) or apollo_dg_last_error. */
