@@ -44,8 +44,14 @@ def deck(N, eq, bcs, meqn, exprs=None, keys="", consts="", progn=None, blocks=""
             + f"]\n{pg} </InitialCondition>\n{blocks} <eq>\n{eq}\n </eq>\n</hyperbolic>\n")
 
 
-def save(name, mesh, N, equation, eqp, flux, bcs, U, t, dt, r, sources=()):
+def save(name, mesh, N, equation, eqp, flux, bcs, U, t, dt, r, sources=(), steps=0):
+    """The right-hand side at (U, t, dt) and, with `steps`, that many
+    SSPRK(5,2) steps from (U, t = 0, dt) through the same code."""
     rhs, sugg = r.rhs(U, t, dt)
+    extra = {}
+    if steps:
+        U_end, t_end, dt_end = r.run(U, steps, 0.0, dt)
+        extra = dict(steps=steps, U_end=U_end, t_end=t_end, dt_end=dt_end)
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"), vx=mesh.vx, vy=mesh.vy, etov=mesh.etov, face_tag=mesh.face_tag,
         vert_canon=mesh.vert_canon, N=N, equation=equation, eqp=np.asarray(eqp, dtype=np.float64), numflux=flux,
@@ -55,7 +61,7 @@ def save(name, mesh, N, equation, eqp, flux, bcs, U, t, dt, r, sources=()):
         src_kinds=np.asarray([s[0] for s in sources]), src_params=np.asarray(
             [list(s[1]) + [0.0] * (9 - len(s[1])) for s in sources], dtype=np.float64).reshape(-1, 9),
         src_nparams=np.asarray([len(s[1]) for s in sources], dtype=np.int32),
-        U=U, t=t, dt=dt, rhs=rhs, sugg=sugg)
+        U=U, t=t, dt=dt, rhs=rhs, sugg=sugg, **extra)
     print(name, U.shape, float(np.abs(rhs).max()))
 
 
@@ -76,8 +82,12 @@ def main():
         r.setup(deck(N, f"  Kind = eulerEqn\n  gas_gamma = 1.4\n  Numerical_Flux = {flux}", names, 5))
         o = orc.Oracle(mesh, N, orc.EQ_EULER, (1.4, 0.0, 0.0))
         x, y = o.node_coords()
+        U = channel_state(x, y, rough=0.05, seed=N)
+        _, dt0 = r.rhs(U, 0.0, 0.0)  # Apollo's suggested dt at this state
+        # steps only with LF and HLL: Apollo's Roe and Wave fluxes turn the
+        # state non-physical within a step or two, where Apollo's driver exits
         save(f"euler_{flux.lower()}_channel_N{N}", mesh, N, "eulerEqn", (1.4, 0.0, 0.0), flux, EULER_BCS,
-             channel_state(x, y, rough=0.05, seed=N), 0.3, 0.01, r)
+             U, 0.3, dt0, r, steps=3 if flux in ("LF", "HLL") else 0)
     # Apollo's isentropicVortex example on a walled square
     N = 4
     mesh = jittered_square(7, (0.0, -5.0), (10.0, 5.0), seed=N, periodic=False, wall_tag=1)
@@ -87,8 +97,8 @@ def main():
                                                     ("uo", 1.0), ("vo", 0.0), ("pi", 3.141592653589793)))
     r.setup(deck(N, "  Kind = eulerEqn\n  gas_gamma = 1.4", names, 5, ["rho", "rhou", "rhov", "0.0", "en"],
                  consts=consts, progn=VORTEX))
-    u0, _ = r.init(0.0)
-    save("euler_vortex_N4", mesh, N, "eulerEqn", (1.4, 0.0, 0.0), "LF", bcs, u0, 0.3, 0.01, r)
+    u0, dt0 = r.init(0.0)
+    save("euler_vortex_N4", mesh, N, "eulerEqn", (1.4, 0.0, 0.0), "LF", bcs, u0, 0.3, dt0, r, steps=5)
     rng = np.random.default_rng(11)
     # Maxwell TM cavity, order 5
     N = 5

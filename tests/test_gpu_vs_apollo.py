@@ -1,9 +1,11 @@
-"""The B200 float64 right-hand side against right-hand sides made by Apollo's
+"""The B200 float64 right-hand side and stepper against results made by Apollo's
 own code (tests/golden/apollo_rhs, written by tests/golden/make_apollo_rhs.py
 with Apollo's WxNodalDG2dMethod compiled unmodified): every Euler flux with
 the four Euler boundary conditions on elements listing their faces in every
 order, the isentropic-vortex example, the Maxwell TM cavity, the cleaned
-Maxwell form with both sources, advection.  Agreement to 1e-12 relative L2
+Maxwell form with both sources, advection; and for the LF, HLL and vortex
+cases a few SSPRK(5,2) steps taken through Apollo's right-hand side (the stage
+arithmetic as PETSc's TSSSP documents it).  Agreement to 1e-12 relative L2
 (1e-11 for the vortex, whose right-hand side is a small difference of O(1)
 flux terms); no restatement stands between the CUDA kernels and Apollo's code.
 """
@@ -23,3 +25,9 @@ def test_rhs_matches_apollo(name):
     got, sugg = s.step(float(g["t"]), float(g["dt"]), g["U"])
     assert rel_l2(got, g["rhs"]) <= (1e-11 if "vortex" in name else 1e-12)
     assert sugg == pytest.approx(float(g["sugg"]), rel=1e-13)
+    if "steps" in g:  # SSPRK(5,2) steps with Apollo's dt policy through Apollo's right-hand side
+        s.set_state(g["U"])
+        t, dt = s.advance(int(g["steps"]), 0.0, float(g["dt"]))
+        assert rel_l2(s.get_state(), g["U_end"]) <= 1e-12
+        assert t == pytest.approx(float(g["t_end"]), rel=1e-13)
+        assert dt == pytest.approx(float(g["dt_end"]), rel=1e-13)

@@ -208,6 +208,13 @@ def test_oracle_reproduces_apollo_rhs_fixtures(oracle_lib, name):
     rhs, sugg = o.rhs(g["U"], float(g["t"]), float(g["dt"]))
     assert rel_l2(rhs, g["rhs"]) <= (1e-11 if "vortex" in name else 1e-12)
     assert sugg == pytest.approx(float(g["sugg"]), rel=1e-14)
+    if "steps" in g:  # SSPRK(5,2) steps through Apollo's right-hand side
+        U = g["U"].copy()
+        n, t, dt = o.run(U, int(g["steps"]), 0.0, float(g["dt"]))
+        assert n == int(g["steps"])
+        assert rel_l2(U, g["U_end"]) <= 1e-12
+        assert t == pytest.approx(float(g["t_end"]), rel=1e-14)
+        assert dt == pytest.approx(float(g["dt_end"]), rel=1e-13)
 
 
 def test_steps_through_apollo_rhs_match_oracle(oracle_lib):
