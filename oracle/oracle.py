@@ -539,10 +539,17 @@ class RefDriver:
         return u, dt.value
 
     def rhs(self, u, t: float = 0.0, dt: float = 0.0):
-        u = np.ascontiguousarray(u, dtype=np.float64)
-        out = np.zeros_like(u)
+        """(right-hand side, suggested dt) at u; u itself is left as it is."""
+        return self.rhs_stage(np.array(u, dtype=np.float64, order="C", copy=True), t, dt)
+
+    def rhs_stage(self, w, t: float = 0.0, dt: float = 0.0):
+        """The right-hand side at the stage vector w (float64, C-contiguous),
+        which a limiter in the method's Limiter list rewrites in place, as
+        Apollo's step does to PETSc's stage vector."""
+        assert w.dtype == np.float64 and w.flags.c_contiguous
+        out = np.zeros_like(w)
         s = C.c_double()
-        self._check(self.lib.refdrv_rhs(self.h, t, dt, _p(u), _p(out), C.byref(s)))
+        self._check(self.lib.refdrv_rhs(self.h, t, dt, _p(w), _p(out), C.byref(s)))
         return out, s.value
 
     def ssp_step(self, u, t0: float, dt: float):
@@ -550,11 +557,11 @@ class RefDriver:
         `rks2` with 5 stages as documented (w = u; 4x w += dt/4 L(w) at
         t0 + dt i/4; u = 4/5 w + dt/5 L(w) + 1/5 u), the arithmetic of the
         oracle's orc_ssp_step.  Returns (u, suggested dt of the last stage)."""
-        w = np.array(u, dtype=np.float64, copy=True)
+        w = np.array(u, dtype=np.float64, order="C", copy=True)
         for i in range(4):
-            F, _ = self.rhs(w, t0 + dt * (i / 4.0), dt)
+            F, _ = self.rhs_stage(w, t0 + dt * (i / 4.0), dt)
             w += (dt / 4.0) * F
-        F, sugg = self.rhs(w, t0 + dt, dt)
+        F, sugg = self.rhs_stage(w, t0 + dt, dt)
         return 0.8 * w + (dt / 5.0) * F + 0.2 * np.asarray(u), sugg
 
     def run(self, u, nsteps: int, t: float, dt: float):

@@ -568,8 +568,9 @@ int refdrv_init(void* p, double t, double* u0, double* dt0) {
 }
 
 // WxNodalDG2dMethod::step(t, dt, u, rhs): the right-hand side and the
-// suggested dt.
-int refdrv_rhs(void* p, double t, double dt, const double* u, double* rhs, double* sugg) {
+// suggested dt.  With a limiter the method limits its input vector in place,
+// as it does PETSc's stage vector; that limited input is written back to u.
+int refdrv_rhs(void* p, double t, double dt, double* u, double* rhs, double* sugg) {
   Driver* d = (Driver*)p;
   _p_Vec in, out;
   in.a.assign(u, u + (size_t)d->dm.K * d->dm.dof);
@@ -584,6 +585,7 @@ int refdrv_rhs(void* p, double t, double dt, const double* u, double* rhs, doubl
     return -1;
   }
   std::memcpy(rhs, out.a.data(), out.a.size() * sizeof(double));
+  std::memcpy(u, in.a.data(), in.a.size() * sizeof(double));
   return 0;
 }
 }  // extern "C"

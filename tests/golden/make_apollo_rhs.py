@@ -1,7 +1,9 @@
 """Golden right-hand sides made by Apollo's own code.
 
 Each fixture holds a mesh, a state and the right-hand side and suggested dt
-that Apollo's WxNodalDG2dMethod computes for it, run compiled unmodified
+that Apollo's WxNodalDG2dMethod computes for it (with a limiter in its
+Limiter list where the fixture names one), and for some a few SSPRK(5,2)
+steps taken through it, run compiled unmodified
 through oracle/ref_driver.cpp (`make -C oracle refdrv`, which needs Apollo's
 source tree).  The B200 tests compare the CUDA path with these directly.
 Run from the repository root: python tests/golden/make_apollo_rhs.py
@@ -44,7 +46,7 @@ def deck(N, eq, bcs, meqn, exprs=None, keys="", consts="", progn=None, blocks=""
             + f"]\n{pg} </InitialCondition>\n{blocks} <eq>\n{eq}\n </eq>\n</hyperbolic>\n")
 
 
-def save(name, mesh, N, equation, eqp, flux, bcs, U, t, dt, r, sources=(), steps=0):
+def save(name, mesh, N, equation, eqp, flux, bcs, U, t, dt, r, sources=(), steps=0, limiter=None):
     """The right-hand side at (U, t, dt) and, with `steps`, that many
     SSPRK(5,2) steps from (U, t = 0, dt) through the same code."""
     rhs, sugg = r.rhs(U, t, dt)
@@ -61,7 +63,9 @@ def save(name, mesh, N, equation, eqp, flux, bcs, U, t, dt, r, sources=(), steps
         src_kinds=np.asarray([s[0] for s in sources]), src_params=np.asarray(
             [list(s[1]) + [0.0] * (9 - len(s[1])) for s in sources], dtype=np.float64).reshape(-1, 9),
         src_nparams=np.asarray([len(s[1]) for s in sources], dtype=np.int32),
-        U=U, t=t, dt=dt, rhs=rhs, sugg=sugg, **extra)
+        U=U, t=t, dt=dt, rhs=rhs, sugg=sugg, **extra,
+        **({} if limiter is None else dict(limiter_kind=limiter[0],
+                                           limiter=np.asarray(limiter[1], dtype=np.float64))))
     print(name, U.shape, float(np.abs(rhs).max()))
 
 
@@ -88,6 +92,27 @@ def main():
         # state non-physical within a step or two, where Apollo's driver exits
         save(f"euler_{flux.lower()}_channel_N{N}", mesh, N, "eulerEqn", (1.4, 0.0, 0.0), flux, EULER_BCS,
              U, 0.3, dt0, r, steps=3 if flux in ("LF", "HLL") else 0)
+    # each limiter in the method's Limiter list (the limiter acts on every
+    # stage input), HLL flux, the channel's four conditions
+    for kind, N in (("eulerLimiterHW", 3), ("tuAliabadiLimiter", 4)):
+        mesh = one_tag_per_element(channel_mesh(5, seed=N + 20, rotate_seed=N + 20))
+        r, names = driver(mesh, EULER_BCS)
+        eq = "  Kind = eulerEqn\n  gas_gamma = 1.4\n  Numerical_Flux = HLL"
+        if kind == "eulerLimiterHW":
+            r.add_limiter("lim", kind, names, gas_gamma=1.4, min_pressure=1e-6, min_density=1e-6)
+            eqp, lim = (1.4, 0.0, 0.0), (kind, (1.4, 1e-6, 1e-6))
+        else:
+            r.add_limiter("lim", kind, names, equation="eulerEqn", gas_gamma=1.4, minPressure=1e-6,
+                          minDensity=1e-6)
+            eq += "\n  minPressure = 1e-6\n  minDensity = 1e-6"
+            eqp, lim = (1.4, 1e-6, 1e-6), (kind, ())
+        r.setup(deck(N, eq, names, 5, keys=" Limiter = [lim]\n"))
+        o = orc.Oracle(mesh, N, orc.EQ_EULER, (1.4, 0.0, 0.0))
+        x, y = o.node_coords()
+        U = channel_state(x, y, rough=0.15, seed=N)
+        _, dt0 = r.rhs(U, 0.0, 0.0)
+        save(f"euler_hll_{'hw' if kind == 'eulerLimiterHW' else 'ta'}limiter_channel_N{N}", mesh, N, "eulerEqn",
+             eqp, "HLL", EULER_BCS, U, 0.3, dt0, r, steps=3, limiter=lim)
     # Apollo's isentropicVortex example on a walled square
     N = 4
     mesh = jittered_square(7, (0.0, -5.0), (10.0, 5.0), seed=N, periodic=False, wall_tag=1)

@@ -3,9 +3,10 @@ own code (tests/golden/apollo_rhs, written by tests/golden/make_apollo_rhs.py
 with Apollo's WxNodalDG2dMethod compiled unmodified): every Euler flux with
 the four Euler boundary conditions on elements listing their faces in every
 order, the isentropic-vortex example, the Maxwell TM cavity, the cleaned
-Maxwell form with both sources, advection; and for the LF, HLL and vortex
-cases a few SSPRK(5,2) steps taken through Apollo's right-hand side (the stage
-arithmetic as PETSc's TSSSP documents it).  Agreement to 1e-12 relative L2
+Maxwell form with both sources, advection, each of Apollo's Euler limiters
+acting on the input; and for the LF, HLL, limiter and vortex cases a few
+SSPRK(5,2) steps taken through Apollo's right-hand side (the stage arithmetic
+as PETSc's TSSSP documents it, the limiter rewriting each stage vector).  Agreement to 1e-12 relative L2
 (1e-11 for the vortex, whose right-hand side is a small difference of O(1)
 flux terms); no restatement stands between the CUDA kernels and Apollo's code.
 """
@@ -22,6 +23,8 @@ def test_rhs_matches_apollo(name):
     g = load_apollo(name)
     s = NodalDG2d(int(g["N"]), 0.5, g["equation"], tuple(g["eqp"]), g["mesh"], bcs=g["bcs"],
                   numerical_flux=g["numflux"], sources=g["sources"])
+    if "limiter_kind" in g:  # Apollo's limiter in the method's Limiter list
+        s.set_limiter(str(g["limiter_kind"]), tuple(g["limiter"]))
     got, sugg = s.step(float(g["t"]), float(g["dt"]), g["U"])
     assert rel_l2(got, g["rhs"]) <= (1e-11 if "vortex" in name else 1e-12)
     assert sugg == pytest.approx(float(g["sugg"]), rel=1e-13)
