@@ -535,8 +535,10 @@ int refdrv_setup(void* p, const char* text) {
     d->dm.section.dof = d->dm.dof;
     delete d->method;
     d->method = m;
-  } catch (WxExcept& e) {
-    g_err = std::string("setup failed: ") + e.what();
+  } catch (WxExcept&) {
+    // (WxExcept::what() hands out a pointer into a temporary string,
+    // wxexcept.cc:46-49, so its text is not read here)
+    g_err = "setup failed: Apollo raised WxExcept (a missing or malformed key, or an unknown Kind)";
     return -1;
   } catch (...) {
     g_err = "setup failed";
