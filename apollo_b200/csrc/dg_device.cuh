@@ -157,7 +157,10 @@ struct StageArgs {
   int phase;
 };
 
-enum { PHASE_ALL = 0, PHASE_VOLUME = 1, PHASE_FACE = 2 };
+// PHASE_FACE_ONLY and PHASE_LIFT split PHASE_FACE into the face kernel and
+// the lift (a partitioned stage runs its interior faces while the halo is in
+// flight, then the cut faces and the lift).
+enum { PHASE_ALL = 0, PHASE_VOLUME = 1, PHASE_FACE = 2, PHASE_FACE_ONLY = 3, PHASE_LIFT = 4 };
 
 template <int N> struct Sizes {
   static constexpr int NP = (N + 1) * (N + 2) / 2;

@@ -859,7 +859,7 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
   int per_sm = vol_res < 1 ? 1 : (vol_res > 8 ? 8 : vol_res);
   int gv = sms * per_sm;
   if (gv > vt) gv = vt;
-  if (a.phase != PHASE_FACE) {
+  if (a.phase == PHASE_ALL || a.phase == PHASE_VOLUME) {
     if (ev) cudaEventRecord(ev[0], s);
     k_volume<EQ, N><<<gv, kThreads, VT::BYTES, s>>>(d, a);
     // sources enter the volume term (wxcubature2d.cc:297-325: VT (w J S))
@@ -870,12 +870,16 @@ cudaError_t launch_rhs_t(const DgDev& d, const StageArgs& a, cudaStream_t s, cud
     if (ev) cudaEventRecord(ev[1], s);
   }
   if (a.phase == PHASE_VOLUME) return cudaGetLastError();
-  const int fthreads = d.nfaces * Sizes<N>::NG;
-  int gf = (fthreads + kThreads - 1) / kThreads;
-  if (gf > sms * 8) gf = sms * 8;
-  if (gf < 1) gf = 1;
-  k_face<EQ, N><<<gf, kThreads, 0, s>>>(d, a);
-  if (ev) cudaEventRecord(ev[2], s);
+  if (a.phase != PHASE_LIFT) {
+    // the faces d.faces[0, d.nfaces): all of them, or a range of them
+    const int fthreads = d.nfaces * Sizes<N>::NG;
+    int gf = (fthreads + kThreads - 1) / kThreads;
+    if (gf > sms * 8) gf = sms * 8;
+    if (gf < 1) gf = 1;
+    if (fthreads > 0) k_face<EQ, N><<<gf, kThreads, 0, s>>>(d, a);
+    if (ev) cudaEventRecord(ev[2], s);
+  }
+  if (a.phase == PHASE_FACE_ONLY) return cudaGetLastError();
   const int lt = (d.K + LT::E - 1) / LT::E;
   int lper = lift_res < 1 ? 1 : (lift_res > 8 ? 8 : lift_res);
   int gl = sms * lper;

@@ -95,6 +95,12 @@ struct apollo_dg {
   int *halo_src_d = nullptr, *halo_dst_d = nullptr;
   void *hsend = nullptr, *hrecv = nullptr, *hlam = nullptr;
   size_t hsend_bytes = 0, hrecv_bytes = 0;
+  // the face list holds the faces between local elements first (nface_int of
+  // them), then the cut faces that touch ghost slots; a float64 stage runs the
+  // first group on side_stream while the caller's exchange is in flight
+  int nface_int = 0;
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_packed = nullptr, ev_interior = nullptr;
   // Euler limiter (apollo_dg_set_limiter): applied to every stage input
   bool lim_on = false;
   LimArgs lim{};
@@ -176,6 +182,10 @@ void free_mesh(apollo_dg* h) {
   h->have_state = false;
   h->ninst = 1;
   dfree(h->halo_src_d); dfree(h->halo_dst_d);
+  if (h->ev_packed) { cudaEventDestroy(h->ev_packed); h->ev_packed = nullptr; }
+  if (h->ev_interior) { cudaEventDestroy(h->ev_interior); h->ev_interior = nullptr; }
+  if (h->side_stream) { cudaStreamDestroy(h->side_stream); h->side_stream = nullptr; }
+  h->nface_int = 0;
   h->partitioned = false;
   h->KG = 0;
   h->peers.clear(); h->send_count.clear(); h->recv_count.clear();
@@ -721,6 +731,14 @@ apollo_status set_mesh_body(apollo_dg* h, int nverts, const double* vx, const do
   h->nbound = 0;
   for (const FaceRec& fr : h->faces_h)
     if (fr.k2 < 0) ++h->nbound;
+  // interior and boundary faces of the local elements first, the cut faces
+  // (one side a ghost slot) last; each face is computed on its own, so the
+  // order changes no result
+  std::stable_partition(h->faces_h.begin(), h->faces_h.end(),
+                        [K](const FaceRec& fr) { return fr.k1 < K && fr.k2 < K; });
+  h->nface_int = 0;
+  for (const FaceRec& fr : h->faces_h)
+    if (fr.k1 < K && fr.k2 < K) ++h->nface_int;
   // device buffers: state-sized ones for the local elements, geometry and
   // trace/flux scratch with the ghost slots
   const size_t nU = (size_t)K * Np * M, nT = (size_t)(K + G) * o.Nf * M;
@@ -1815,6 +1833,23 @@ apollo_status apollo_dg_stage_begin(apollo_dg* h, int stage, apollo_precision pr
     CK(launch_rhs_fp64(h->eq, d, a, h->stream), "volume launch");
     const int blk = h->ops.Ng * h->M * (int)sizeof(double);
     CK(launch_halo_blocks(h->trace_d, h->hsend, h->halo_src_d, h->n_send, blk, false, h->stream), "halo pack");
+    if (!h->peers.empty() && h->nface_int > 0) {
+      // the faces between local elements need no remote trace: they run on
+      // the side stream while the caller's exchange (enqueued on the handle's
+      // stream after this call) is in flight; apollo_dg_stage_end joins them
+      if (!h->side_stream) {
+        CK(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking), "side stream");
+        CK(cudaEventCreateWithFlags(&h->ev_packed, cudaEventDisableTiming), "stage event");
+        CK(cudaEventCreateWithFlags(&h->ev_interior, cudaEventDisableTiming), "stage event");
+      }
+      CK(cudaEventRecord(h->ev_packed, h->stream), "stage event");
+      CK(cudaStreamWaitEvent(h->side_stream, h->ev_packed, 0), "stage event");
+      DgDev di = d;
+      di.nfaces = h->nface_int;
+      a.phase = PHASE_FACE_ONLY;
+      CK(launch_rhs_fp64(h->eq, di, a, h->side_stream), "interior face launch");
+      CK(cudaEventRecord(h->ev_interior, h->side_stream), "stage event");
+    }
   }
   return APOLLO_OK;
 }
@@ -1834,8 +1869,21 @@ apollo_status apollo_dg_stage_end(apollo_dg* h, int stage, apollo_precision prec
   } else {
     const int blk = h->ops.Ng * h->M * (int)sizeof(double);
     CK(launch_halo_blocks(h->hrecv, h->trace_d, h->halo_dst_d, h->n_recv, blk, true, h->stream), "halo unpack");
-    a.phase = PHASE_FACE;
-    CK(launch_rhs_fp64(h->eq, d, a, h->stream), "face launch");
+    if (!h->peers.empty() && h->nface_int > 0) {
+      // the interior faces ran on the side stream since apollo_dg_stage_begin;
+      // the cut faces now, then the lift over all of them
+      CK(cudaStreamWaitEvent(h->stream, h->ev_interior, 0), "stage event");
+      DgDev dc = d;
+      dc.faces = d.faces + h->nface_int;
+      dc.nfaces = d.nfaces - h->nface_int;
+      a.phase = PHASE_FACE_ONLY;
+      CK(launch_rhs_fp64(h->eq, dc, a, h->stream), "cut face launch");
+      a.phase = PHASE_LIFT;
+      CK(launch_rhs_fp64(h->eq, d, a, h->stream), "lift launch");
+    } else {
+      a.phase = PHASE_FACE;
+      CK(launch_rhs_fp64(h->eq, d, a, h->stream), "face launch");
+    }
   }
   if (stage == 4 && h->hlam)
     CK(cudaMemcpyAsync(h->hlam, &h->st_d->lam_bits, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, h->stream),
