@@ -132,8 +132,9 @@ def main():
     r, names = driver(mesh, bcs)
     r.setup(deck(N, "  Kind = phMaxwellEqn\n  c0 = 1.0", names, 8))
     Np = (N + 1) * (N + 2) // 2
-    save("maxwell_tm_N5", mesh, N, "phMaxwellEqn", (1.0, 0.0, 0.0), "LF", bcs,
-         rng.standard_normal((mesh.K, Np, 8)), 0.3, 0.01, r)
+    U = rng.standard_normal((mesh.K, Np, 8))
+    save("maxwell_tm_N5", mesh, N, "phMaxwellEqn", (1.0, 0.0, 0.0), "LF", bcs, U, 0.3, r.rhs(U, 0.0, 0.0)[1], r,
+         steps=3)
     # cleaned Maxwell, conducting walls, TM2DwithSource.pin's source and a point current
     N = 3
     mesh = jittered_square(5, seed=N, periodic=False, wall_tag=1)
@@ -146,16 +147,17 @@ def main():
     r.setup(deck(N, "  Kind = phMaxwellEqn\n  c0 = 1.0\n  chi = 1.0\n  gamma = 1.0", names, 8,
                  keys=" Sources = [current, wire]\n", blocks=blocks))
     Np = (N + 1) * (N + 2) // 2
-    save("maxwell_src_N3", mesh, N, "phMaxwellEqn", (1.0, 1.0, 1.0), "LF", bcs,
-         rng.standard_normal((mesh.K, Np, 8)), 0.7, 0.01, r,
-         sources=(("tranverseMagneticSrc", ()), ("pointCurrentSrc", pc)))
+    U = rng.standard_normal((mesh.K, Np, 8))
+    save("maxwell_src_N3", mesh, N, "phMaxwellEqn", (1.0, 1.0, 1.0), "LF", bcs, U, 0.7, r.rhs(U, 0.0, 0.0)[1], r,
+         sources=(("tranverseMagneticSrc", ()), ("pointCurrentSrc", pc)), steps=3)
     # advection with a fixed inflow value
     mesh = jittered_square(6, seed=13, periodic=False, wall_tag=1)
     bcs = (("gridFixedBC", (0.75,)),)
     r, names = driver(mesh, bcs)
     r.setup(deck(N, "  Kind = advectionEqn\n  ux = 1.0\n  uy = 0.5", names, 1))
-    save("advection_N3", mesh, N, "advectionEqn", (1.0, 0.5, 0.0), "LF", bcs,
-         rng.standard_normal((mesh.K, Np, 1)), 0.3, 0.01, r)
+    U = rng.standard_normal((mesh.K, Np, 1))
+    save("advection_N3", mesh, N, "advectionEqn", (1.0, 0.5, 0.0), "LF", bcs, U, 0.3, r.rhs(U, 0.0, 0.0)[1], r,
+         steps=3)
 
 
 if __name__ == "__main__":

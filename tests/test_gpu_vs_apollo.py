@@ -4,7 +4,7 @@ with Apollo's WxNodalDG2dMethod compiled unmodified): every Euler flux with
 the four Euler boundary conditions on elements listing their faces in every
 order, the isentropic-vortex example, the Maxwell TM cavity, the cleaned
 Maxwell form with both sources, advection, each of Apollo's Euler limiters
-acting on the input; and for the LF, HLL, limiter and vortex cases a few
+acting on the input; and for all but the Roe and Wave cases a few
 SSPRK(5,2) steps taken through Apollo's right-hand side (the stage arithmetic
 as PETSc's TSSSP documents it, the limiter rewriting each stage vector).  Agreement to 1e-12 relative L2
 (1e-11 for the vortex, whose right-hand side is a small difference of O(1)
