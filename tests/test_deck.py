@@ -153,3 +153,21 @@ def test_keys_after_a_sub_block_are_not_read_as_in_apollo(oracle_lib):
         return ref.numflux(ref.lib.ref_eqn_create(text.encode()), n, qM.copy(), qP.copy())[0]
     np.testing.assert_array_equal(flux(after), flux(base.format(body="")))
     assert not np.array_equal(flux(before), flux(base.format(body="")))
+
+
+def test_a_key_written_twice_takes_the_first_as_in_apollo(oracle_lib):
+    """Of a key written twice in one block the first value counts, in the deck
+    reader and in Apollo's own reader (checked through its eulerEqn flux)."""
+    import numpy as np
+    base = "<top>\n Equations = [eq]\n <eq>\n  Kind = eulerEqn\n{body} </eq>\n</top>\n"
+    twice = base.format(body="  gas_gamma = 1.2\n  gas_gamma = 1.4\n")
+    assert deck_equation(twice)[1][0] == 1.2
+    orc = oracle_lib
+    if not orc.RefPlugins.available():
+        pytest.skip("Apollo's plugins are not built here")
+    ref = orc.RefPlugins()
+    qM, qP, n = np.array([1.0, 0.5, 0.2, 0.0, 2.5]), np.array([0.8, 0.1, -0.3, 0.0, 2.0]), np.array([0.6, 0.8])
+
+    def flux(text):
+        return ref.numflux(ref.lib.ref_eqn_create(text.encode()), n, qM.copy(), qP.copy())[0]
+    np.testing.assert_array_equal(flux(twice), flux(base.format(body="  gas_gamma = 1.2\n")))
