@@ -404,6 +404,32 @@ def maxwell_measure(args, device: int, cpu: bool):
     return out
 
 
+def apollo_cpu_extra(procs: int | None = None):
+    """Apollo's own code (where it is built) on the other configurations'
+    problems, bounded samples: the TM cavity at N = 5 and a walled Gaussian
+    advection at N = 3 on every host core, one process per core, and the
+    vortex at N = 4 on one core.  DOF counts the physical fields (3, 1, 4)."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+    if not orc.RefDriver.available():
+        return None
+    import multiprocessing as mp
+    procs = procs or _host_cores()
+    res = {}
+    for key, case, n, m, steps, pp in (("maxwell_tm_N5", "tm", 24, 3, 2, procs),
+                                       ("advection_N3", "advection", 32, 1, 4, procs),
+                                       ("euler_vortex_N4_1_core", "vortex", APOLLO_SAMPLE_N, 4, 2, 1)):
+        with mp.get_context("spawn").Pool(pp) as pool:
+            out = pool.map(_apollo_steps, [(n, steps, 1, case)] * pp)
+        el = max(o[0] for o in out)
+        K, Np = out[0][1], out[0][2]
+        res[key] = {"value": pp * K * Np * m * steps / el, "cores": pp, "K_per_process": K, "steps": steps,
+                    "seconds": el, "kind": "reference",
+                    "sample": f"{steps} SSPRK(5,2) steps per process through Apollo's own right-hand-side code "
+                              f"on a {n}x{n} vertex grid (K={K}), {pp} process(es)"}
+    return res
+
+
 def cpu_extra(threads: int):
     """CPU oracle rates the single-GPU line reports beside its own numbers: the
     Euler vortex at N = 4 on one thread (one step of a 64 x 64 grid), and the
@@ -449,15 +475,24 @@ def _host_cores() -> int:
 
 def _apollo_steps(job):
     """One process of the reference arm: Apollo's own right-hand-side code
-    (compiled unmodified into oracle/_ref) stepping its isentropicVortex
-    example on an n x n vertex grid of [0, 10]^2 at order 4; returns the
-    seconds of the timed steps, the elements and the nodes per element."""
-    n, steps, warmup = job
+    (compiled unmodified into oracle/_ref) stepping one of its example
+    problems on an n x n vertex grid: the isentropicVortex example on
+    [0, 10]^2 at order 4 (case "vortex"), the transverseMagnetic cavity on
+    [0, 1]^2 at order 5 ("tm"), or a Gaussian advected on [0, 1]^2 at order 3
+    ("advection"); returns the seconds of the timed steps, the elements and
+    the nodes per element."""
+    n, steps, warmup = job[:3]
+    case = job[3] if len(job) > 3 else "vortex"
     sys.path.insert(0, ROOT)
     from apollo_b200.mesh import jittered_square
     from oracle import oracle as orc
-    mesh = jittered_square(n, (0.0, 0.0), (10.0, 10.0), seed=0, periodic=False, wall_tag=1)
-    r = orc.apollo_vortex_driver(mesh, 4, 0.5)
+    if case == "vortex":
+        mesh = jittered_square(n, (0.0, 0.0), (10.0, 10.0), seed=0, periodic=False, wall_tag=1)
+        r = orc.apollo_vortex_driver(mesh, 4, 0.5)
+    else:
+        mesh = jittered_square(n, seed=0, periodic=False, wall_tag=1)
+        r = (orc.apollo_tm_driver if case == "tm" else orc.apollo_advection_driver)(mesh, 5 if case == "tm" else 3,
+                                                                                     0.5)
     u, dt = r.init(0.0)
     u, t, dt = r.run(u, warmup, 0.0, dt)
     t0 = time.perf_counter()
@@ -1151,6 +1186,12 @@ def ours_arm(args):
                 extra["cpu_extra"] = cpu_extra(os.cpu_count() or 1)
             except Exception as exc:
                 extra["cpu_extra"] = {"error": str(exc)}
+            try:
+                ref_extra = apollo_cpu_extra()
+                if ref_extra is not None:
+                    extra["apollo_cpu"] = ref_extra
+            except Exception as exc:
+                extra["apollo_cpu"] = {"error": str(exc)}
 
     if rank == 0:
         # our kernels per step: float64 5 x (volume, face, lift) + finalize;

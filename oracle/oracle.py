@@ -600,3 +600,32 @@ def apollo_vortex_driver(mesh, N: int, cfl: float, x0: float = 5.0, y0: float = 
             f'  exprList = ["rho", "rhou", "rhov", "0.0", "en"]\n  progn = [{progn}]\n </InitialCondition>\n'
             f" <euler>\n  Kind = eulerEqn\n  gas_gamma = {gamma!r}\n </euler>\n</hyperbolic>\n")
     return r
+
+
+def _apollo_deck(N: int, cfl: float, eq: str, bcs, meqn: int, exprs, consts: str = "") -> str:
+    return (f"<hyperbolic>\n Kind = nodalDG2d\n Equations = [eq]\n boundaryConditions = [{', '.join(bcs)}]\n"
+            f" polynomialOrder = {N}\n cfl = {cfl!r}\n DataStructure = [0, dg, {meqn * (N + 1) * (N + 2) // 2}]\n"
+            f" <InitialCondition>\n  Kind = exprFunc\n{consts}  exprList = ["
+            + ", ".join(f'"{e}"' for e in exprs) + f"]\n </InitialCondition>\n <eq>\n{eq}\n </eq>\n</hyperbolic>\n")
+
+
+def apollo_tm_driver(mesh, N: int, cfl: float) -> RefDriver:
+    """Apollo's transverseMagnetic example on `mesh` through Apollo's own
+    right-hand-side code: phMaxwellEqn (c0 = 1), Ez = sin(pi x) sin(pi y),
+    maxwellTransverseMagneticBC on every boundary face."""
+    r = RefDriver(mesh)
+    r.add_bc("walls", "maxwellTransverseMagneticBC")
+    r.setup(_apollo_deck(N, cfl, "  Kind = phMaxwellEqn\n  c0 = 1.0", ["walls"], 8,
+                         ["0.0", "0.0", "sin(pi*x)*sin(pi*y)"] + ["0.0"] * 5, "  pi = 3.141592653589793\n"))
+    return r
+
+
+def apollo_advection_driver(mesh, N: int, cfl: float) -> RefDriver:
+    """Advection of a Gaussian through Apollo's own right-hand-side code:
+    advectionEqn (ux = 1, uy = 0.5), exp(-r^2/0.01) about (0.5, 0.5), a fixed
+    zero value on every boundary face (gridFixedBC)."""
+    r = RefDriver(mesh)
+    r.add_bc("fixed", "gridFixedBC", value=0.0)
+    r.setup(_apollo_deck(N, cfl, "  Kind = advectionEqn\n  ux = 1.0\n  uy = 0.5", ["fixed"], 1,
+                         ["exp(-((x-0.5)*(x-0.5)+(y-0.5)*(y-0.5))/0.01)"]))
+    return r

@@ -243,3 +243,26 @@ def test_steps_through_apollo_rhs_match_oracle(oracle_lib):
     assert n == 4
     assert rel_l2(ur, uo) <= 1e-12
     assert tr == pytest.approx(to, rel=1e-14) and dtr == pytest.approx(dto, rel=1e-13)
+
+
+@pytest.mark.parametrize("case", ["tm", "advection"])
+def test_example_drivers_step_like_the_oracle(oracle_lib, case):
+    """The TM cavity and walled advection problems the bench times through
+    Apollo's own code (apollo_tm_driver, apollo_advection_driver) step like
+    the oracle on the same problem."""
+    orc = oracle_lib
+    if not orc.RefDriver.available():
+        pytest.skip("Apollo's right-hand side is not built here")
+    mesh = jittered_square(8, seed=1, periodic=False, wall_tag=1)
+    if case == "tm":
+        N, r = 5, orc.apollo_tm_driver(mesh, 5, 0.5)
+        o = orc.Oracle(mesh, N, orc.EQ_MAXWELL, (1.0, 0.0, 0.0), bcs=((orc.BC_TM, ()),), cfl=0.5)
+    else:
+        N, r = 3, orc.apollo_advection_driver(mesh, 3, 0.5)
+        o = orc.Oracle(mesh, N, orc.EQ_ADVECTION, (1.0, 0.5, 0.0), bcs=((orc.BC_FIXED, (0.0,)),), cfl=0.5)
+    u0, dt0 = r.init(0.0)
+    assert dt0 == pytest.approx(o.init_dt(u0), rel=1e-14)
+    uo = u0.copy()
+    o.run(uo, 3, 0.0, dt0)
+    ur, _, _ = r.run(u0, 3, 0.0, dt0)
+    assert rel_l2(ur, uo) <= 1e-12
